@@ -1,0 +1,320 @@
+"""ctypes binding of libfwt (include/fwt.h).
+
+The method names mirror the reference's Fortran routines so that a caller of the reference
+finds the same steps:
+
+=====================  ==========================================  =========================
+method                 reference                                    C entry point
+=====================  ==========================================  =========================
+``load_inputs``        tube.f90:168-223, 341-379                    fwt_load_inputs
+``set_centerlines``    tube.f90:353-379 (after the broadcasts)      fwt_set_centerlines
+``deposit``            tube.f90:392-946                             fwt_deposit
+``filter_spec``        subroutine.f90:1225-1277                     fwt_filter
+``biot_savart``        tube.f90:972-1023                            fwt_biot_savart
+``cal_helicity``       tube.f90:1026-1044                           fwt_normalize
+``spectrum``           subroutine.f90:1604-1638                     fwt_spectrum
+``export_pdf``         subroutine.f90:1-62                          fwt_pdf
+``Sp_calculate``       subroutine.f90:64-129                        fwt_sp
+``output_v``           tube.f90:1055-1071, subroutine.f90:1342      fwt_field_wh
+``run``                tube.f90:392-1188                            fwt_run
+``write_outputs``      the output tree of tube.f90                  fwt_write_outputs
+=====================  ==========================================  =========================
+
+Errors raise :class:`FwtError` with the library's message, as the reference would abort.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libfwt.so")
+_lib = None
+
+
+class FwtError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libfwt error {code}: {msg}")
+        self.code = code
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [
+        ("N", ctypes.c_int), ("N_downsample", ctypes.c_int), ("line_s", ctypes.c_int), ("line_e", ctypes.c_int),
+        ("sigma_ratio", ctypes.c_double), ("eta_t", ctypes.c_double), ("ntf_times", ctypes.c_int),
+        ("ntf_pre", ctypes.c_int), ("Rtube_ratio", ctypes.c_double), ("dzeta_sup", ctypes.c_double),
+        ("precision", ctypes.c_int), ("deposit_mode", ctypes.c_int), ("device", ctypes.c_int),
+        ("stream", ctypes.c_void_p), ("if_pdf", ctypes.c_int), ("if_Sp", ctypes.c_int), ("Sp_order", ctypes.c_int),
+        ("pdf_bins", ctypes.c_int), ("vorticity_output", ctypes.c_int), ("mem_cap", ctypes.c_size_t),
+    ]
+
+
+EXPORTS = [
+    "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_set_centerlines",
+    "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
+    "fwt_pdf", "fwt_sp", "fwt_field_wh", "fwt_copy_field", "fwt_write_outputs", "fwt_run_dir", "fwt_run",
+    "fwt_timings", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
+]
+
+
+def library(path: str | None = None):
+    """Load libfwt.so (built in-tree by fastweavturb_b200.build); raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or _LIB_PATH
+    if not os.path.exists(p):
+        raise FwtError(-2, f"{p} is missing: build it with `python -m fastweavturb_b200.build` "
+                           "(there is no CPU fallback)")
+    L = ctypes.CDLL(p)
+    vp, ip, dp = ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double)
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    sig = {
+        "fwt_default_params": [ctypes.POINTER(_Params)],
+        "fwt_create": [ctypes.POINTER(_Params), ctypes.POINTER(vp)],
+        "fwt_destroy": [vp],
+        "fwt_load_inputs": [vp, ctypes.c_char_p, ctypes.c_char_p],
+        "fwt_set_centerlines": [vp, ip, i64p, dp, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+        "fwt_set_centerlines_device": [vp, ip, i64p, vp, vp, vp, dp, dp, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)],
+        "fwt_deposit": [vp, ip, ip],
+        "fwt_filter": [vp, ctypes.c_double],
+        "fwt_biot_savart": [vp],
+        "fwt_normalize": [vp, dp, dp, dp],
+        "fwt_spectrum": [vp, ip, dp, ip],
+        "fwt_pdf": [vp, ip, ip, ip, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                    ctypes.POINTER(ctypes.c_uint64)],
+        "fwt_sp": [vp, ip, ctypes.POINTER(ctypes.c_int), ip, dp],
+        "fwt_field_wh": [vp, ctypes.POINTER(ctypes.c_float)],
+        "fwt_copy_field": [vp, ip, ip, dp],
+        "fwt_write_outputs": [vp, ctypes.c_char_p],
+        "fwt_run_dir": [ctypes.c_char_p, ctypes.POINTER(_Params)],
+        "fwt_run": [vp],
+        "fwt_timings": [vp, dp, ip],
+        "fwt_counters": [vp, i64p, ip],
+        "fwt_last_error": [ctypes.c_char_p, ip],
+        "fwt_fbb_generate": [vp, ctypes.c_uint64, ip, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), dp,
+                             dp, vp, vp, vp],
+        "fwt_fbb_signs": [ctypes.c_uint64, ip, ctypes.POINTER(ctypes.c_int)],
+    }
+    for name, args in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _err():
+    buf = ctypes.create_string_buffer(1024)
+    library().fwt_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def _check(rc):
+    if rc != 0:
+        raise FwtError(rc, _err())
+    return rc
+
+
+def _ptr(a, ct):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+@dataclass
+class Params:
+    """parameters_input.dat scalars plus the reference's compile-time switches."""
+    N: int = 64
+    N_downsample: int = 64
+    line_s: int = 1
+    line_e: int = 1
+    sigma_ratio: float = 4.0
+    eta_t: float = 0.0
+    ntf_times: int = 50
+    ntf_pre: int = 1000
+    Rtube_ratio: float = 3.0
+    dzeta_sup: float = 1e-4
+    precision: int = 32
+    deposit_mode: int = 0
+    device: int = 0
+    stream: int = 0
+    if_pdf: int = 1
+    if_Sp: int = 1
+    Sp_order: int = 10
+    pdf_bins: int = 1000
+    vorticity_output: int = 1
+    mem_cap: int = 0
+
+    def to_c(self):
+        p = _Params()
+        for f, _ in _Params._fields_:
+            v = getattr(self, f)
+            setattr(p, f, v if f != "stream" else (v or None))
+        return p
+
+
+def sp_separations(N):
+    """r_m = floor(sqrt(2.0)**m + 0.5), m = 0..2*floor(log2 N + 0.01), REAL(4) (subroutine.f90:78,98)."""
+    f32 = np.float32
+    lg2L = int(np.floor(f32(np.log(f32(N)) / np.log(f32(2.0))) + f32(0.01)))
+    s2 = f32(np.sqrt(f32(2.0)))
+    out = []
+    for m in range(2 * lg2L + 1):
+        p, base, e = f32(1.0), s2, m
+        while e:
+            if e & 1:
+                p = f32(p * base)
+            base = f32(base * base)
+            e >>= 1
+        out.append(int(np.floor(f32(p + f32(0.5)))))
+    return np.array(out, dtype=np.int32)
+
+
+class Context:
+    """One libfwt context (device buffers, FFT plans, stream) for one field."""
+
+    def __init__(self, params: Params | None = None, **kw):
+        self.params = params or Params(**kw)
+        L = library()
+        self._h = ctypes.c_void_p()
+        self._p = self.params.to_c()
+        _check(L.fwt_create(ctypes.byref(self._p), ctypes.byref(self._h)))
+        self.N = self.params.N
+
+    # ------------------------------------------------------------------ life cycle
+    def close(self):
+        if self._h:
+            library().fwt_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------------ inputs
+    def load_inputs(self, centerline_path, params_path):
+        _check(library().fwt_load_inputs(self._h, str(centerline_path).encode(), str(params_path).encode()))
+
+    def set_centerlines(self, npoint, xyz, sigma, Gamma, n_T, if_filter=None):
+        npoint = np.ascontiguousarray(npoint, dtype=np.int64)
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        nl = len(npoint)
+        sigma = np.ascontiguousarray(sigma, dtype=np.float64)
+        Gamma = np.ascontiguousarray(Gamma, dtype=np.float64)
+        n_T = np.ascontiguousarray(n_T, dtype=np.int32)
+        filt = np.ascontiguousarray(np.zeros(nl) if if_filter is None else if_filter, dtype=np.int32)
+        _check(library().fwt_set_centerlines(self._h, nl, _ptr(npoint, ctypes.c_int64), _ptr(xyz, ctypes.c_double),
+                                             _ptr(sigma, ctypes.c_double), _ptr(Gamma, ctypes.c_double),
+                                             _ptr(n_T, ctypes.c_int), _ptr(filt, ctypes.c_int)))
+
+    def set_centerlines_device(self, npoint, dx, dy, dz, sigma, Gamma, n_T, if_filter=None):
+        """dx, dy, dz: device pointers (int) to FP64 node coordinates on this context's GPU."""
+        npoint = np.ascontiguousarray(npoint, dtype=np.int64)
+        nl = len(npoint)
+        sigma = np.ascontiguousarray(sigma, dtype=np.float64)
+        Gamma = np.ascontiguousarray(Gamma, dtype=np.float64)
+        n_T = np.ascontiguousarray(n_T, dtype=np.int32)
+        filt = np.ascontiguousarray(np.zeros(nl) if if_filter is None else if_filter, dtype=np.int32)
+        self._keep = (npoint, sigma, Gamma, n_T, filt)
+        _check(library().fwt_set_centerlines_device(self._h, nl, _ptr(npoint, ctypes.c_int64), dx, dy, dz,
+                                                    _ptr(sigma, ctypes.c_double), _ptr(Gamma, ctypes.c_double),
+                                                    _ptr(n_T, ctypes.c_int), _ptr(filt, ctypes.c_int)))
+
+    # ------------------------------------------------------------------ phases
+    def deposit(self, line_s=None, line_e=None):
+        _check(library().fwt_deposit(self._h, line_s or self.params.line_s, line_e or self.params.line_e))
+
+    def filter_spec(self, k_c):
+        _check(library().fwt_filter(self._h, float(k_c)))
+
+    def biot_savart(self):
+        _check(library().fwt_biot_savart(self._h))
+
+    def cal_helicity(self):
+        """Normalisation by u' (tube.f90:1026-1044); returns dict(up, Etot, Enstrophy)."""
+        up, E, en = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(library().fwt_normalize(self._h, ctypes.byref(up), ctypes.byref(E), ctypes.byref(en)))
+        return {"up": up.value, "Etot": E.value, "Enstrophy": en.value}
+
+    def spectrum(self, which=1):
+        out = np.zeros(self.N // 2)
+        _check(library().fwt_spectrum(self._h, which, _ptr(out, ctypes.c_double), len(out)))
+        return out
+
+    def export_pdf(self, which=0, component=-1, nbins=1000):
+        val = np.zeros(nbins, dtype=np.float32)
+        pdf = np.zeros(nbins, dtype=np.float32)
+        cnt = np.zeros(nbins, dtype=np.uint64)
+        _check(library().fwt_pdf(self._h, which, component, nbins, _ptr(val, ctypes.c_float),
+                                 _ptr(pdf, ctypes.c_float), _ptr(cnt, ctypes.c_uint64)))
+        return val, pdf, cnt
+
+    def Sp_calculate(self, pmax=10, r=None):
+        r = sp_separations(self.N) if r is None else np.ascontiguousarray(r, dtype=np.int32)
+        out = np.zeros(pmax * len(r))
+        _check(library().fwt_sp(self._h, pmax, _ptr(r, ctypes.c_int), len(r), _ptr(out, ctypes.c_double)))
+        return r, out.reshape(pmax, len(r))
+
+    def output_v(self):
+        nd = self.params.N_downsample
+        out = np.zeros(2 * nd ** 3, dtype=np.float32)
+        _check(library().fwt_field_wh(self._h, _ptr(out, ctypes.c_float)))
+        return out.reshape(2, nd, nd, nd)
+
+    def copy_field(self, which, component):
+        """which 0: omega, 1: u; normalised once cal_helicity ran.  Array [k, j, i]."""
+        out = np.zeros(self.N ** 3)
+        _check(library().fwt_copy_field(self._h, which, component, _ptr(out, ctypes.c_double)))
+        return out.reshape(self.N, self.N, self.N)
+
+    def field(self, which):
+        return np.stack([self.copy_field(which, c) for c in range(3)])
+
+    def run(self):
+        _check(library().fwt_run(self._h))
+
+    def write_outputs(self, outdir):
+        _check(library().fwt_write_outputs(self._h, str(outdir).encode()))
+
+    def timings(self):
+        t = np.zeros(5)
+        library().fwt_timings(self._h, _ptr(t, ctypes.c_double), 5)
+        return {"setup_ms": t[0], "deposit_ms": t[1], "spectral_ms": t[2], "stats_ms": t[3], "total_ms": t[4]}
+
+    def counters(self):
+        v = np.zeros(5, dtype=np.int64)
+        library().fwt_counters(self._h, _ptr(v, ctypes.c_int64), 5)
+        return {"lines": int(v[0]), "sections": int(v[1]), "subsegments": int(v[2]), "pairs": int(v[3]),
+                "launches": int(v[4])}
+
+    def fbb_generate(self, seed, tubes, nodes, H, dB, dx, dy, dz):
+        tubes = np.ascontiguousarray(tubes, dtype=np.int32)
+        nodes = np.ascontiguousarray(nodes, dtype=np.int32)
+        H = np.ascontiguousarray(H, dtype=np.float64)
+        dB = np.ascontiguousarray(dB, dtype=np.float64)
+        _check(library().fwt_fbb_generate(self._h, ctypes.c_uint64(seed), len(tubes), _ptr(tubes, ctypes.c_int),
+                                          _ptr(nodes, ctypes.c_int), _ptr(H, ctypes.c_double),
+                                          _ptr(dB, ctypes.c_double), dx, dy, dz))
+
+
+def run_dir(rundir, params: Params | None = None):
+    """The whole program in `rundir` (reads both input files, writes rundir/output)."""
+    p = (params or Params()).to_c()
+    _check(library().fwt_run_dir(str(rundir).encode(), ctypes.byref(p)))
+
+
+def fbb_signs(seed, ntubes):
+    out = np.zeros(ntubes, dtype=np.int32)
+    _check(library().fwt_fbb_signs(ctypes.c_uint64(seed), ntubes, _ptr(out, ctypes.c_int)))
+    return out

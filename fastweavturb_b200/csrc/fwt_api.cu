@@ -1,0 +1,514 @@
+// fwt_api.cu -- the C-ABI of libfwt (include/fwt.h): context life cycle, inputs, the phase
+// entry points and the whole-program driver.
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "k_centerline.cuh"
+
+namespace fwt {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+int buf_reserve(Ctx *c, DevBuf &b, size_t bytes)
+{
+    if (bytes <= b.bytes && b.p) return 0;
+    if (b.p) {
+        cudaFree(b.p);
+        c->mem_held -= b.bytes;
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    if (bytes == 0) bytes = 16;
+    if (c->p.mem_cap && c->mem_held + bytes > c->p.mem_cap)
+        return fail(FWT_E_NOMEM, "device allocation of " + std::to_string(bytes) + " bytes exceeds the memory cap");
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        cudaGetLastError();
+        return fail(FWT_E_NOMEM, "cudaMalloc(" + std::to_string(bytes) + "): " + cudaGetErrorString(e));
+    }
+    b.bytes = bytes;
+    c->mem_held += bytes;
+    return 0;
+}
+
+void buf_free(Ctx *c, DevBuf &b)
+{
+    if (b.p) {
+        cudaFree(b.p);
+        c->mem_held -= b.bytes;
+    }
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+static int validate(const fwt_params &p)
+{
+    if (p.N < 4 || p.N > 2048 || (p.N & 1)) return fail(FWT_E_ARG, "N must be even and in 4..2048");
+    if (p.N_downsample < 1 || p.N % p.N_downsample) return fail(FWT_E_ARG, "N_downsample must divide N");
+    if (p.precision != 32 && p.precision != 64) return fail(FWT_E_ARG, "precision must be 32 or 64");
+    if (p.ntf_times < 0 || p.ntf_pre < 1) return fail(FWT_E_ARG, "ntf_times >= 0 and ntf_pre >= 1 required");
+    if (!(p.Rtube_ratio > 0) || !(p.dzeta_sup > 0) || !(p.sigma_ratio > 0))
+        return fail(FWT_E_ARG, "Rtube_ratio, dzeta_sup and sigma_ratio must be positive");
+    if (p.pdf_bins < 1 || p.pdf_bins > 8192) return fail(FWT_E_ARG, "pdf_bins must be 1..8192");
+    if (p.Sp_order < 1 || p.Sp_order > 10) return fail(FWT_E_ARG, "Sp_order must be 1..10");
+    return 0;
+}
+
+static void reset_state(Ctx *c)
+{
+    c->have_w = c->have_u = c->normalised = false;
+    c->w_written = c->wmm_valid = c->umm_valid = false;
+}
+
+struct PhaseTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaStream_t s;
+    explicit PhaseTimer(cudaStream_t st) : s(st)
+    {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, s);
+    }
+    double stop()
+    {
+        float ms = 0;
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    }
+    ~PhaseTimer()
+    {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
+}  // namespace fwt
+
+using namespace fwt;
+
+extern "C" {
+
+int fwt_last_error(char *buf, int len)
+{
+    if (!buf || len <= 0) return FWT_E_ARG;
+    std::strncpy(buf, g_err.c_str(), (size_t)len - 1);
+    buf[len - 1] = 0;
+    return 0;
+}
+
+int fwt_default_params(fwt_params *p)
+{
+    if (!p) return fail(FWT_E_ARG, "null params");
+    std::memset(p, 0, sizeof(*p));
+    p->N = 256;
+    p->N_downsample = 256;
+    p->line_s = 1;
+    p->line_e = 1;
+    p->sigma_ratio = 4.0;
+    p->eta_t = 0.0;
+    p->ntf_times = 50;
+    p->ntf_pre = 1000;
+    p->Rtube_ratio = 3.0;
+    p->dzeta_sup = 1e-4;
+    p->precision = 32;
+    p->deposit_mode = 0;
+    p->device = 0;
+    p->stream = nullptr;
+    p->if_pdf = 1;
+    p->if_Sp = 1;
+    p->Sp_order = 10;
+    p->pdf_bins = 1000;
+    p->vorticity_output = 1;
+    p->mem_cap = 0;
+    return 0;
+}
+
+int fwt_create(const fwt_params *p, fwt_ctx **out)
+{
+    if (!p || !out) return fail(FWT_E_ARG, "null argument");
+    FWT_TRY(validate(*p));
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(FWT_E_CUDA, "no CUDA device: the woven-field library has no CPU path");
+    }
+    if (p->device < 0 || p->device >= ndev) return fail(FWT_E_ARG, "device ordinal out of range");
+    Ctx *c = new Ctx();
+    c->p = *p;
+    c->dev = p->device;
+    cudaError_t e = cudaSetDevice(c->dev);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(FWT_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    }
+    if (p->stream) {
+        c->stream = (cudaStream_t)p->stream;
+    } else {
+        e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete c;
+            return fail(FWT_E_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+        }
+        c->own_stream = true;
+    }
+    *out = (fwt_ctx *)c;
+    return 0;
+}
+
+int fwt_destroy(fwt_ctx *h)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return 0;
+    cudaSetDevice(c->dev);
+    cudaStreamSynchronize(c->stream);
+    if (c->plans) {
+        cufftDestroy(c->plan_r2c);
+        cufftDestroy(c->plan_c2r);
+    }
+    buf_free(c, c->b_nodes);
+    buf_free(c, c->b_w);
+    buf_free(c, c->b_u);
+    buf_free(c, c->b_spec);
+    buf_free(c, c->b_fftws);
+    for (auto &b : c->scratch) buf_free(c, b);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return 0;
+}
+
+static int set_lines_common(Ctx *c, int nline, const int64_t *npoint, const double *sigma, const double *Gamma,
+                            const int *n_T, const int *if_filter)
+{
+    if (nline < 1 || !npoint || !sigma || !Gamma || !n_T) return fail(FWT_E_ARG, "bad centerline arguments");
+    c->nline = nline;
+    c->npoint.assign(npoint, npoint + nline);
+    c->node_off.assign(nline + 1, 0);
+    for (int l = 0; l < nline; ++l) {
+        if (npoint[l] < 2) return fail(FWT_E_ARG, "every line needs at least 2 nodes");
+        if (npoint[l] > (1 << 30)) return fail(FWT_E_RANGE, "line too long");
+        if (!(sigma[l] > 0)) return fail(FWT_E_ARG, "sigma must be positive");
+        c->node_off[l + 1] = c->node_off[l] + npoint[l];
+    }
+    c->sigma.assign(sigma, sigma + nline);
+    c->Gamma.assign(Gamma, Gamma + nline);
+    c->n_T.assign(n_T, n_T + nline);
+    if (if_filter) c->if_filter.assign(if_filter, if_filter + nline);
+    else c->if_filter.assign(nline, 0);
+    c->have_lines = true;
+    reset_state(c);
+    return 0;
+}
+
+int fwt_set_centerlines(fwt_ctx *h, int nline, const int64_t *npoint, const double *xyz, const double *sigma,
+                        const double *Gamma, const int *n_T, const int *if_filter)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !xyz) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    FWT_TRY(set_lines_common(c, nline, npoint, sigma, Gamma, n_T, if_filter));
+    const int64_t n = c->node_off[nline];
+    c->xyz_host.assign(xyz, xyz + 3 * n);
+    FWT_TRY(buf_reserve(c, c->b_nodes, sizeof(double) * 3 * (size_t)n));
+    // SoA on the device: x[], y[], z[]
+    std::vector<double> soa((size_t)(3 * n));
+    for (int64_t i = 0; i < n; ++i) {
+        soa[i] = xyz[3 * i];
+        soa[n + i] = xyz[3 * i + 1];
+        soa[2 * n + i] = xyz[3 * i + 2];
+    }
+    double *d = (double *)c->b_nodes.p;
+    FWT_CUDA(cudaMemcpyAsync(d, soa.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    c->d_x = d;
+    c->d_y = d + n;
+    c->d_z = d + 2 * n;
+    return 0;
+}
+
+int fwt_set_centerlines_device(fwt_ctx *h, int nline, const int64_t *npoint, const double *d_x, const double *d_y,
+                               const double *d_z, const double *sigma, const double *Gamma, const int *n_T,
+                               const int *if_filter)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !d_x || !d_y || !d_z) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    FWT_TRY(set_lines_common(c, nline, npoint, sigma, Gamma, n_T, if_filter));
+    c->xyz_host.clear();
+    c->d_x = d_x;
+    c->d_y = d_y;
+    c->d_z = d_z;
+    return 0;
+}
+
+int fwt_load_inputs(fwt_ctx *h, const char *cpath, const char *ppath)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !cpath || !ppath) return fail(FWT_E_ARG, "null argument");
+    std::vector<int64_t> np;
+    std::vector<double> xyz, sig, gam;
+    std::vector<int> nT, filt;
+    FWT_TRY(io_read_centerlines(cpath, np, xyz));
+    fwt_params p = c->p;
+    FWT_TRY(io_read_params(ppath, (int)np.size(), p, sig, gam, nT, filt));
+    FWT_TRY(validate(p));
+    if (p.N != c->p.N || p.precision != c->p.precision) {
+        // the grid size fixes the FFT plans and field buffers: rebuild them
+        if (c->plans) {
+            cufftDestroy(c->plan_r2c);
+            cufftDestroy(c->plan_c2r);
+            c->plans = false;
+        }
+    }
+    c->p = p;
+    return fwt_set_centerlines(h, (int)np.size(), np.data(), xyz.data(), sig.data(), gam.data(), nT.data(), filt.data());
+}
+
+int fwt_deposit(fwt_ctx *h, int line_s, int line_e)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    cudaSetDevice(c->dev);
+    PhaseTimer t(c->stream);
+    const int rc = deposit_lines(c, line_s, line_e);
+    c->t_ms[1] = t.stop();
+    return rc;
+}
+
+int fwt_filter(fwt_ctx *h, double k_c)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    cudaSetDevice(c->dev);
+    return spectral_filter(c, k_c);
+}
+
+int fwt_biot_savart(fwt_ctx *h)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    cudaSetDevice(c->dev);
+    PhaseTimer t(c->stream);
+    const int rc = spectral_biot_savart(c);
+    c->t_ms[2] = t.stop();
+    return rc;
+}
+
+int fwt_normalize(fwt_ctx *h, double *up, double *Etot, double *enstrophy)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    FWT_TRY(stats_normalise(c));
+    if (up) *up = c->up;
+    if (Etot) *Etot = c->Etot;
+    if (enstrophy) *enstrophy = c->enstrophy;
+    return 0;
+}
+
+int fwt_spectrum(fwt_ctx *h, int which, double *Ek, int nshell)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !Ek) return fail(FWT_E_ARG, "null argument");
+    if (!c->have_u) return fail(FWT_E_STATE, "spectrum before Biot-Savart");
+    if (which == 1 && !c->normalised) return fail(FWT_E_STATE, "velocity spectrum before normalisation");
+    const std::vector<double> &s = which ? c->spec_u : c->spec_w;
+    const double sc = which ? 1.0 / (c->up * c->up) : 1.0;
+    for (int i = 0; i < nshell; ++i) Ek[i] = i < (int)s.size() ? s[i] * sc : 0.0;
+    return 0;
+}
+
+int fwt_pdf(fwt_ctx *h, int which, int component, int nbins, float *val, float *pdf, uint64_t *counts)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    cudaSetDevice(c->dev);
+    return stats_pdf(c, which, component, nbins, val, pdf, counts);
+}
+
+int fwt_sp(fwt_ctx *h, int pmax, const int *r, int nr, double *Sp)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !r || !Sp) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    return stats_sp(c, pmax, r, nr, Sp);
+}
+
+int fwt_field_wh(fwt_ctx *h, float *host_out)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    cudaSetDevice(c->dev);
+    return stats_field_wh(c, host_out);
+}
+
+int fwt_copy_field(fwt_ctx *h, int which, int component, double *host)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !host) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    return stats_copy_field(c, which, component, host);
+}
+
+// r_m = floor(sqrt(2.0)**m + 0.5), m = 0..2*lg2L in REAL(4) (subroutine.f90:78,97-98)
+static std::vector<int> sp_separations(int N)
+{
+    const float l2 = std::log((float)N) / std::log(2.0f);
+    const int lg2L = (int)std::floor(l2 + 0.01f);
+    const float s2 = std::sqrt(2.0f);
+    std::vector<int> r;
+    for (int m = 0; m <= 2 * lg2L; ++m) {
+        float p = 1.0f, base = s2;
+        int e = m;
+        while (e) {
+            if (e & 1) p = p * base;
+            base = base * base;
+            e >>= 1;
+        }
+        r.push_back((int)std::floor(p + 0.5f));
+    }
+    return r;
+}
+
+int fwt_run(fwt_ctx *h)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    if (!c->have_lines) return fail(FWT_E_STATE, "no centerlines set");
+    cudaSetDevice(c->dev);
+    const int64_t l0 = c->launches;
+    reset_state(c);
+    PhaseTimer total(c->stream);
+    {
+        PhaseTimer t(c->stream);
+        FWT_TRY(deposit_lines(c, c->p.line_s, c->p.line_e));
+        c->t_ms[1] = t.stop();
+    }
+    {
+        PhaseTimer t(c->stream);
+        FWT_TRY(spectral_biot_savart(c));
+        FWT_TRY(stats_normalise(c));
+        c->t_ms[2] = t.stop();
+    }
+    {
+        PhaseTimer t(c->stream);
+        const int nb = c->p.pdf_bins;
+        if (c->p.if_pdf) {
+            c->pdf_u_val.resize(nb);
+            c->pdf_u.resize(nb);
+            c->pdf_w_val.resize(nb);
+            c->pdf_w.resize(nb);
+            FWT_TRY(stats_pdf(c, 0, -1, nb, c->pdf_u_val.data(), c->pdf_u.data(), nullptr));
+            FWT_TRY(stats_pdf(c, 1, -1, nb, c->pdf_w_val.data(), c->pdf_w.data(), nullptr));
+        }
+        if (c->p.if_Sp) {
+            c->sp_r = sp_separations(c->p.N);
+            c->sp.assign((size_t)c->p.Sp_order * c->sp_r.size(), 0.0);
+            FWT_TRY(stats_sp(c, c->p.Sp_order, c->sp_r.data(), (int)c->sp_r.size(), c->sp.data()));
+        }
+        if (c->p.vorticity_output) {
+            const size_t nd = (size_t)c->p.N_downsample;
+            c->field_wh.resize(2 * nd * nd * nd);
+            FWT_TRY(stats_field_wh(c, c->field_wh.data()));
+        }
+        c->t_ms[3] = t.stop();
+    }
+    c->t_ms[4] = total.stop();
+    c->counters[4] = c->launches - l0;
+    // total length of every line (tube.f90:501-502): Len_Disc * 2pi
+    c->lengthtot = 0.0;
+    for (int l = 0; l < c->nline; ++l) {
+        double L = (l < (int)c->line_len.size()) ? c->line_len[l] : 0.0;
+        if (L == 0.0 && !c->xyz_host.empty()) {
+            // lines outside line_s..line_e: periodic polygon length on the host
+            const double *x = c->xyz_host.data() + 3 * c->node_off[l];
+            const int64_t n = c->npoint[l];
+            for (int64_t i = 0; i < n; ++i) {
+                const int64_t j = (i + 1) % n;
+                double s2 = 0;
+                for (int d = 0; d < 3; ++d) {
+                    double v = std::fabs(x[3 * j + d] - x[3 * i + d]);
+                    if (v > kPi) v -= kPi2;
+                    s2 += v * v;
+                }
+                L += std::sqrt(s2);
+            }
+        }
+        c->lengthtot += L;
+    }
+    // per-line times: the batch times apportioned by section count
+    c->timing_line.assign(2 * (size_t)c->nline, 0.0);
+    int64_t secs = 0;
+    for (int l = c->p.line_s - 1; l < c->p.line_e; ++l) secs += c->npoint[l];
+    for (int l = c->p.line_s - 1; l < c->p.line_e; ++l) {
+        const double f = secs ? (double)c->npoint[l] / secs : 0.0;
+        c->timing_line[2 * l] = c->t_ms[0] * 1e-3 * f;
+        c->timing_line[2 * l + 1] = c->t_ms[1] * 1e-3 * f;
+    }
+    return 0;
+}
+
+int fwt_write_outputs(fwt_ctx *h, const char *outdir)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !outdir) return fail(FWT_E_ARG, "null argument");
+    if (!c->normalised) return fail(FWT_E_STATE, "write_outputs before the statistics were built");
+    return io_write_outputs(c, outdir);
+}
+
+int fwt_run_dir(const char *rundir, const fwt_params *p0)
+{
+    if (!rundir) return fail(FWT_E_ARG, "null run directory");
+    fwt_params p;
+    if (p0) p = *p0;
+    else fwt_default_params(&p);
+    fwt_ctx *h = nullptr;
+    FWT_TRY(fwt_create(&p, &h));
+    const std::string d = rundir;
+    int rc = fwt_load_inputs(h, (d + "/centerline_input.dat").c_str(), (d + "/parameters_input.dat").c_str());
+    if (rc == 0) rc = fwt_run(h);
+    if (rc == 0) rc = fwt_write_outputs(h, (d + "/output").c_str());
+    std::string keep = g_err;
+    fwt_destroy(h);
+    if (rc) g_err = keep;
+    return rc;
+}
+
+int fwt_timings(fwt_ctx *h, double *t, int n)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !t) return fail(FWT_E_ARG, "null argument");
+    int k = 0;
+    for (; k < n && k < 5; ++k) t[k] = c->t_ms[k];
+    return k;
+}
+
+int fwt_counters(fwt_ctx *h, int64_t *v, int n)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !v) return fail(FWT_E_ARG, "null argument");
+    int k = 0;
+    for (; k < n && k < 5; ++k) v[k] = c->counters[k];
+    return k;
+}
+
+int fwt_fbb_generate(fwt_ctx *h, uint64_t seed, int nlev, const int *tubes, const int *nodes, const double *H,
+                     const double *dB, double *d_x, double *d_y, double *d_z)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || nlev < 1 || !tubes || !nodes || !H || !dB || !d_x || !d_y || !d_z)
+        return fail(FWT_E_ARG, "bad generator arguments");
+    cudaSetDevice(c->dev);
+    return fbb_generate(c, seed, nlev, tubes, nodes, H, dB, d_x, d_y, d_z);
+}
+
+}  // extern "C"

@@ -1,0 +1,166 @@
+// fwt_internal.h -- shared declarations of libfwt (not part of the public C-ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/fwt.h"
+
+namespace fwt {
+
+constexpr double kPi = 3.141592653589793115997963468544185161590576171875;   // 4*datan(1d0)
+constexpr double kPi2 = 6.28318530717958623199592693708837032318115234375;   // 8*datan(1d0)
+
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+
+#define FWT_CUDA(call)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return ::fwt::fail(FWT_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+#define FWT_CUFFT(call)                                                                    \
+    do {                                                                                   \
+        cufftResult r_ = (call);                                                           \
+        if (r_ != CUFFT_SUCCESS)                                                           \
+            return ::fwt::fail(FWT_E_CUDA, std::string(#call) + ": cufft error " + std::to_string((int)r_)); \
+    } while (0)
+#define FWT_TRY(call)                                                                      \
+    do {                                                                                   \
+        int rc_ = (call);                                                                  \
+        if (rc_ != 0) return rc_;                                                          \
+    } while (0)
+
+// A device buffer that grows on demand and is freed with the context.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+// Per-line set-up parameters on the device.
+struct LineParam {
+    double sigma_min, sigma_max, Gamma, length, Len;
+    int n_T;
+    int n_sec;          // nodes of the line
+    int64_t node_off;   // first node of the line in the node arrays
+    int64_t slot_off;   // first section slot of the line (n_sec + 1 slots per line)
+};
+
+// Sub-segment record (FP64), one per (section, t_j), t_j < ntf (tube.f90:767-798).
+struct SubSeg {
+    double ci0[3];   // unwrapped start (mark1, tube.f90:779-785)
+    double ci1[3];   // unwrapped end
+    double tci0[3], tci1[3];
+    double s0, s1, ndci0;
+    double ssec;     // s_list2(t_i, 1): zeta of the section start
+    double zs0;      // s0 - ssec: section-local zeta of the start
+    double Rt;       // truncation radius Rtube_ratio * max(sigma(s0), sigma(s1))
+    int slot;        // global section slot
+    int line;        // line index (0-based)
+    int box_lo[3];   // 1-based unwrapped box (tube.f90:793-798)
+    int box_hi[3];
+};
+
+struct Timers {
+    cudaEvent_t ev[8];
+    bool made = false;
+};
+
+struct Ctx {
+    fwt_params p{};
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+
+    // inputs (host)
+    int nline = 0;
+    std::vector<int64_t> npoint, node_off;
+    std::vector<double> sigma, Gamma;
+    std::vector<int> n_T, if_filter;
+    std::vector<double> xyz_host;   // only when set from host / files (for centerline_output)
+    bool have_lines = false;
+
+    // node coordinates on the device (SoA)
+    const double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr;
+    DevBuf b_nodes;   // owned copy when set from host
+
+    // fields
+    DevBuf b_w;       // omega, 3 N^3 (float or double)
+    DevBuf b_u;       // u, 3 N^3
+    DevBuf b_spec;    // spectral buffer, 3 N^2 (N/2+1) complex
+    DevBuf b_fftws;   // cuFFT work area
+    cufftHandle plan_r2c = 0, plan_c2r = 0;
+    bool plans = false;
+    size_t fft_ws_bytes = 0;
+
+    // scratch (centerline set-up, deposition, statistics)
+    DevBuf scratch[24];
+
+    // state
+    bool have_w = false, have_u = false, normalised = false;
+    bool w_written = false;   // omega holds deposited data (later batches accumulate)
+    bool wmm_valid = false;   // wmin/wmax hold the raw omega component range
+    double up = 1.0, Etot = 0.0, Etot_raw = 0.0, enstrophy = 0.0, enstrophy_raw = 0.0, lengthtot = 0.0;
+    bool umm_valid = false;   // umin/umax hold the raw u component range
+    std::vector<double> spec_w, spec_u;   // shells 1..N/2
+    std::vector<int64_t> line_ntf_sum, line_ntf_max;  // per deposited line
+    std::vector<int> line_nsec;
+    std::vector<double> line_len;
+    std::vector<float> wmin, wmax, umin, umax;   // per component, raw (unnormalised) fields
+
+    // statistics kept for file output
+    std::vector<float> pdf_u_val, pdf_u, pdf_w_val, pdf_w;
+    std::vector<int> sp_r;
+    std::vector<double> sp;
+    std::vector<float> field_wh;
+
+    // timers / counters
+    Timers tm;
+    double t_ms[5] = {0, 0, 0, 0, 0};
+    double t_deposit_wall_init = 0;
+    int64_t counters[5] = {0, 0, 0, 0, 0};
+    int64_t launches = 0;
+    size_t mem_held = 0;
+
+    std::vector<double> timing_line;   // per line: set-up ms, construction ms
+};
+
+// device memory helpers
+int buf_reserve(Ctx *c, DevBuf &b, size_t bytes);
+void buf_free(Ctx *c, DevBuf &b);
+
+// centerline set-up + deposition (k_centerline.cu, k_deposit.cu)
+int deposit_lines(Ctx *c, int line_s, int line_e);
+
+// spectral (k_spectral.cu)
+int spectral_init(Ctx *c);
+int spectral_filter(Ctx *c, double k_c);
+int spectral_biot_savart(Ctx *c);
+
+// statistics (k_stats.cu)
+int stats_minmax(Ctx *c, int which);
+int stats_normalise(Ctx *c);
+int stats_pdf(Ctx *c, int which, int comp, int nbins, float *val, float *pdf, uint64_t *counts);
+int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp);
+int stats_field_wh(Ctx *c, float *host_out);
+int stats_copy_field(Ctx *c, int which, int comp, double *host);
+
+// host I/O (fwt_io.cpp)
+int io_read_centerlines(const char *path, std::vector<int64_t> &npoint, std::vector<double> &xyz);
+int io_read_params(const char *path, int nline, fwt_params &p, std::vector<double> &sigma,
+                   std::vector<double> &Gamma, std::vector<int> &n_T, std::vector<int> &if_filter);
+int io_write_outputs(Ctx *c, const char *outdir);
+
+// generator (k_fbb.cu)
+int fbb_generate(Ctx *c, uint64_t seed, int nlev, const int *tubes, const int *nodes, const double *H,
+                 const double *dB, double *d_x, double *d_y, double *d_z);
+
+inline size_t field_elems(const Ctx *c) { return (size_t)c->p.N * c->p.N * c->p.N; }
+inline size_t real_bytes(const Ctx *c) { return c->p.precision == 64 ? 8 : 4; }
+
+}  // namespace fwt

@@ -1,0 +1,260 @@
+// k_deposit.cu -- Burgers vortex-tube deposition (tube.f90:762-904).
+//
+// Two kernels share the per-point arithmetic:
+//   * deposit_walk_kernel  -- the reference's box walk, one warp per sub-segment, global
+//     atomics.  Templated on FP64 (the plain FP64 GPU path, statement-for-statement the
+//     reference arithmetic) and FP32.
+//   * deposit_tile_kernel  -- (k_deposit_tile.cu) tile-owned: sub-segments binned into
+//     integer cell lists, each CTA owns a grid tile, accumulates in shared memory and writes
+//     the tile once with coalesced vector stores.
+//
+// FP32 arithmetic is done in a frame local to the sub-segment start ci0: grid-point offsets
+// x - ci0, and the spline re-expanded around the start, c(z0 + W) - c(z0) = sum_k b_k W^k
+// (Taylor shift of the quintic in FP64), so no FP32 quantity carries the absolute position.
+#include "k_deposit.cuh"
+
+namespace fwt {
+
+// ---------------------------------------------------------------------------- FP64 walk
+// Statement-for-statement the reference's inner body (tube.f90:806-892) at grid index
+// (ip, jp, kp) (1-based, unwrapped).  Returns true and the contribution if accepted.
+__device__ __forceinline__ bool point_ref_f64(const SubSeg &S, const LineParam &P, const double *coe, double dtf,
+                                              double dzeta_sup, double eta, double dx, int ip, int jp, int kp,
+                                              double out[3])
+{
+    const double xstart = -dev_pi();
+    const double m0 = dadd(dmul((double)ip - 1.0, dx), xstart);
+    const double m1 = dadd(dmul((double)jp - 1.0, dx), xstart);
+    const double m2 = dadd(dmul((double)kp - 1.0, dx), xstart);
+    const double a0 = dsub(m0, S.ci0[0]), a1 = dsub(m1, S.ci0[1]), a2 = dsub(m2, S.ci0[2]);
+    const double t0 = dadd(dadd(dmul(a0, S.tci0[0]), dmul(a1, S.tci0[1])), dmul(a2, S.tci0[2]));
+    if (!(t0 >= 0.0)) return false;
+    const double e0 = dsub(m0, S.ci1[0]), e1 = dsub(m1, S.ci1[1]), e2 = dsub(m2, S.ci1[2]);
+    double t1 = dadd(dadd(dmul(e0, S.tci1[0]), dmul(e1, S.tci1[1])), dmul(e2, S.tci1[2]));
+    if (!(t1 < 0.0)) return false;
+    double rho = sqrt(dsub(dadd(dadd(dmul(a0, a0), dmul(a1, a1)), dmul(a2, a2)), dmul(t0, t0)));
+    if (!(rho < S.Rt)) return false;
+    t1 = dadd(dadd(dmul(e0, S.tci0[0]), dmul(e1, S.tci0[1])), dmul(e2, S.tci0[2]));
+    const double zeta = (S.s1 * t0 - S.s0 * t1) / S.ndci0;
+    const double zsec = zeta - S.ssec;
+    const double L = P.Len;
+    double cz[3], dc[3], ddc[3];
+    spl_pos(coe, zsec * L, cz);
+    const double dzeta = fmin(dzeta_sup, 1.0 * dtf);
+    spl_d1(coe, zsec * L, dc);
+    const double ndc = sqrt(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]);
+    double T[3] = {dc[0] / ndc, dc[1] / ndc, dc[2] / ndc};
+    spl_d2(coe, zsec * L, ddc);
+    double X[3] = {dc[1] * ddc[2] - dc[2] * ddc[1], dc[2] * ddc[0] - dc[0] * ddc[2], dc[0] * ddc[1] - dc[1] * ddc[0]};
+    const double nX = sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+    double xc[3];
+    const double m[3] = {m0, m1, m2};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double v = m[d] - cz[d];
+        if (v > dev_pi()) v = v - dev_pi2();
+        if (v < -dev_pi()) v = v + dev_pi2();
+        xc[d] = v;
+    }
+    const double nxc = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
+    rho = nxc;
+    const double sigma = sigma_func(zeta, P.length, P.sigma_max, P.sigma_min, P.n_T);
+    const double s2 = sigma * sigma;
+    double tp = exp(-(rho * rho) / 2.0 / s2) / (dev_pi2() * s2);
+    const double ftd = -exp(-(S.Rt * S.Rt) / 2.0 / s2) / (dev_pi2() * s2);
+    tp = tp + ftd;
+    const double sl = sigma_func(zeta - dzeta, P.length, P.sigma_max, P.sigma_min, P.n_T);
+    const double sr = sigma_func(zeta + dzeta, P.length, P.sigma_max, P.sigma_min, P.n_T);
+    double dsds = (sr - sl) / (2.0 * dzeta);
+    dsds = dsds / ndc / L;
+    const double G = P.Gamma;
+    if (nX < 1.0e-8) {
+        double er[3], eth[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) er[d] = xc[d] / (nxc + 1.0e-15);
+        eth[0] = er[1] * T[2] - er[2] * T[1];
+        eth[1] = er[2] * T[0] - er[0] * T[2];
+        eth[2] = er[0] * T[1] - er[1] * T[0];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) out[d] = tp * G * (T[d] + eta * rho * eth[d] + (rho * dsds / sigma) * er[d]);
+    } else {
+        double B[3], Nv[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) B[d] = X[d] / nX;
+        Nv[0] = B[1] * T[2] - B[2] * T[1];
+        Nv[1] = B[2] * T[0] - B[0] * T[2];
+        Nv[2] = B[0] * T[1] - B[1] * T[0];
+        const double kap = nX / (ndc * ndc * ndc);
+        const double costh = (xc[0] * Nv[0] + xc[1] * Nv[1] + xc[2] * Nv[2]) / (nxc + 1.0e-15);
+        const double sinth = (xc[0] * B[0] + xc[1] * B[1] + xc[2] * B[2]) / (nxc + 1.0e-15);
+        const double den = 1.0 - kap * rho * costh;
+        const double t5 = -(sinth * rho) / den;
+        const double t6 = costh * rho / den;
+        const double t7 = costh * rho * dsds / sigma / den;
+        const double t8 = sinth * rho * dsds / sigma / den;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            out[d] = tp * G * (T[d] + eta * (t5 * Nv[d] + t6 * B[d]) + (t7 * Nv[d] + t8 * B[d]));
+    }
+    return true;
+}
+
+// Reference box walk: one warp per sub-segment; lanes stride the box points in the
+// reference's loop order (k outer, i inner); contributions added with global atomics.
+template <typename Real, bool General>
+__global__ void __launch_bounds__(256) deposit_walk_kernel(const SubSeg *__restrict__ seg, int64_t nsub,
+                                                           const LineParam *__restrict__ lp, int line_base,
+                                                           const double *__restrict__ coe,
+                                                           const double *__restrict__ dtf, int N, double dzeta_sup,
+                                                           double eta, Real *__restrict__ wx, Real *__restrict__ wy,
+                                                           Real *__restrict__ wz, unsigned long long *accepted)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long acc = 0;
+    for (int64_t q = w0; q < nsub; q += nw) {
+        const SubSeg S = seg[q];
+        const LineParam P = lp[S.line - line_base];
+        const int nx = S.box_hi[0] - S.box_lo[0] + 1, ny = S.box_hi[1] - S.box_lo[1] + 1,
+                  nz = S.box_hi[2] - S.box_lo[2] + 1;
+        const int64_t total = (int64_t)nx * ny * nz;
+        const double dt = dtf[S.slot];
+        if constexpr (sizeof(Real) == 8) {
+            const double dx = dev_pi2() / N;
+            const double *cf = coe + 18 * (size_t)S.slot;
+            for (int64_t idx = lane; idx < total; idx += 32) {
+                const int ii = (int)(idx % nx);
+                const int64_t r = idx / nx;
+                const int jj = (int)(r % ny), kk = (int)(r / ny);
+                const int ip = S.box_lo[0] + ii, jp = S.box_lo[1] + jj, kp = S.box_lo[2] + kk;
+                double o[3];
+                if (!point_ref_f64(S, P, cf, dt, dzeta_sup, eta, dx, ip, jp, kp, o)) continue;
+                const size_t id = (size_t)wrap_idx(ip - 1, N) +
+                                  (size_t)N * ((size_t)wrap_idx(jp - 1, N) + (size_t)N * (size_t)wrap_idx(kp - 1, N));
+                atomicAdd((double *)wx + id, o[0]);
+                atomicAdd((double *)wy + id, o[1]);
+                atomicAdd((double *)wz + id, o[2]);
+                ++acc;
+            }
+        } else {
+            SegF G;
+            seg_setup_f32(S, P, coe, dt, dzeta_sup, eta, N, S.box_lo[0], S.box_lo[1], S.box_lo[2], G);
+            for (int64_t idx = lane; idx < total; idx += 32) {
+                const int ii = (int)(idx % nx);
+                const int64_t r = idx / nx;
+                const int jj = (int)(r % ny), kk = (int)(r / ny);
+                float o[3];
+                if (!point_f32<General>(G, ii, jj, kk, o)) continue;
+                const int ip = S.box_lo[0] + ii, jp = S.box_lo[1] + jj, kp = S.box_lo[2] + kk;
+                const size_t id = (size_t)wrap_idx(ip - 1, N) +
+                                  (size_t)N * ((size_t)wrap_idx(jp - 1, N) + (size_t)N * (size_t)wrap_idx(kp - 1, N));
+                atomicAdd((float *)wx + id, o[0]);
+                atomicAdd((float *)wy + id, o[1]);
+                atomicAdd((float *)wz + id, o[2]);
+                ++acc;
+            }
+        }
+    }
+    acc = warp_sum(acc);
+    if (lane == 0 && accepted) atomicAdd(accepted, acc);
+}
+
+// ---------------------------------------------------------------------------- driver
+int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc)
+{
+    if (B.nsub == 0) return 0;
+    const int N = c->p.N;
+    const size_t n3 = field_elems(c);
+    const bool general = !(c->p.sigma_ratio == 1.0 && c->p.eta_t == 0.0);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+    const int64_t want = (B.nsub * 32 + 255) / 256;
+    const unsigned blocks = (unsigned)std::min<int64_t>(want, (int64_t)sms * 64);
+    if (c->p.precision == 64) {
+        double *w = (double *)c->b_w.p;
+        deposit_walk_kernel<double, true><<<blocks, 256, 0, c->stream>>>(
+            B.seg, B.nsub, B.lp, B.la, B.coe, B.dtf, N, c->p.dzeta_sup, c->p.eta_t, w, w + n3, w + 2 * n3, d_acc);
+    } else {
+        float *w = (float *)c->b_w.p;
+        if (general)
+            deposit_walk_kernel<float, true><<<blocks, 256, 0, c->stream>>>(
+                B.seg, B.nsub, B.lp, B.la, B.coe, B.dtf, N, c->p.dzeta_sup, c->p.eta_t, w, w + n3, w + 2 * n3, d_acc);
+        else
+            deposit_walk_kernel<float, false><<<blocks, 256, 0, c->stream>>>(
+                B.seg, B.nsub, B.lp, B.la, B.coe, B.dtf, N, c->p.dzeta_sup, c->p.eta_t, w, w + n3, w + 2 * n3, d_acc);
+    }
+    c->launches += 1;
+    FWT_CUDA(cudaGetLastError());
+    return 0;
+}
+
+static int64_t batch_node_cap(const Ctx *c)
+{
+    // sub-segment records are ~200 B and there are ~10-50 per node: keep a batch's
+    // set-up arrays within a few GB
+    return (int64_t)1 << 22;
+}
+
+int deposit_lines(Ctx *c, int line_s, int line_e)
+{
+    if (!c->have_lines) return fail(FWT_E_STATE, "no centerlines set");
+    if (line_s < 1 || line_e > c->nline || line_s > line_e)
+        return fail(FWT_E_ARG, "line range outside 1..nline");
+    const size_t n3 = field_elems(c);
+    FWT_TRY(buf_reserve(c, c->b_w, 3 * n3 * real_bytes(c)));
+    if (!c->have_w) {
+        FWT_CUDA(cudaMemsetAsync(c->b_w.p, 0, 3 * n3 * real_bytes(c), c->stream));
+        c->have_w = true;
+        c->line_ntf_sum.assign(c->nline, 0);
+        c->line_ntf_max.assign(c->nline, 0);
+        c->line_len.assign(c->nline, 0.0);
+    }
+    c->have_u = false;
+    c->normalised = false;
+    FWT_TRY(buf_reserve(c, c->scratch[19], 64));
+    unsigned long long *d_acc = (unsigned long long *)c->scratch[19].p;
+    FWT_CUDA(cudaMemsetAsync(d_acc, 0, sizeof(unsigned long long), c->stream));
+    int64_t sections = 0, subsegs = 0, pairs = 0;
+    const int64_t cap = batch_node_cap(c);
+    int la = line_s - 1;
+    while (la < line_e) {
+        // batch: consecutive lines up to the node cap, ending after a filtered line
+        int lb = la;
+        int64_t nodes = 0;
+        while (lb < line_e) {
+            nodes += c->npoint[lb];
+            ++lb;
+            if (c->if_filter[lb - 1]) break;
+            if (lb < line_e && nodes + c->npoint[lb] > cap) break;
+        }
+        CenterlineBatch B;
+        FWT_TRY(centerline_setup(c, la, lb, B));
+        for (int i = 0; i < B.nl; ++i) {
+            c->line_ntf_sum[la + i] = B.line_ntf_sum[2 * i];
+            c->line_ntf_max[la + i] = B.line_ntf_sum[2 * i + 1];
+            c->line_len[la + i] = B.Lens[i] * kPi2;
+        }
+        sections += B.nslots - B.nl;
+        subsegs += B.nsub;
+        if (c->p.deposit_mode == 1 || c->p.precision == 64) {
+            FWT_TRY(launch_walk(c, B, d_acc));
+        } else {
+            int64_t np_ = 0;
+            FWT_TRY(launch_tile(c, B, &np_));
+            pairs += np_;
+        }
+        if (c->if_filter[lb - 1]) {
+            const double kc = std::ceil(4.0 / c->sigma[lb - 1]);
+            FWT_TRY(spectral_filter(c, kc));
+        }
+        la = lb;
+    }
+    c->counters[0] = line_e - line_s + 1;
+    c->counters[1] = sections;
+    c->counters[2] = subsegs;
+    c->counters[3] = pairs;
+    return 0;
+}
+
+}  // namespace fwt

@@ -1,0 +1,184 @@
+// k_deposit.cuh -- per-point Burgers-tube arithmetic shared by the deposition kernels.
+#pragma once
+
+#include "k_centerline.cuh"
+
+namespace fwt {
+
+// FP32 view of one sub-segment, local to its start point ci0 and to a grid-index origin.
+struct SegF {
+    float off[3];     // mesh point at the origin index minus ci0
+    float dx;
+    float tc0[3], tc1[3], dci[3];
+    float g;          // W = t0 * g is the spline argument measured from the start, times Len
+    float b[3][5];    // c(z0 + W) - c(z0) = sum_k b[k-1] W^k
+    float R2, Rt;
+    float smin, A, ph0, om, q;   // sigma = smin + A (sin(ph0 + om W) + 1); dsigma/dzeta = q cos(.)
+    float Gamma, Linv, eta;
+    // periodic bookkeeping of the reference's two single wraps (coo_curve_spline_5th wraps
+    // c(zeta) once into [-pi,pi), cminus wraps x - c once): x - c(z) = (d0 - P) + 2 pi n with
+    // n = kq + (P >= thi) - (P < tlo), then one cminus wrap
+    int kq[3];        // (ci0 - poly(z0)) / 2pi
+    float thi[3];     // pi - poly(z0): poly(z) >= pi  <=>  P >= thi
+    float tlo[3];     // -pi - poly(z0): poly(z) < -pi <=>  P < tlo
+};
+
+// ---------------------------------------------------------------------------- FP32 set-up
+__device__ __forceinline__ void seg_setup_f32(const SubSeg &S, const LineParam &P, const double *__restrict__ coe_all,
+                              double dtf, double dzeta_sup, double eta0, int N, int i0, int j0, int k0, SegF &G)
+{
+    const double dx = dev_pi2() / N, xstart = -dev_pi();
+    const double *coe = coe_all + 18 * (size_t)S.slot;
+    const double L = P.Len;
+    const int org[3] = {i0, j0, k0};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        // mesh coordinate of the 1-based unwrapped index org[d]: (i_plus - 1)*dx + xstart
+        const double X0 = dadd(dmul((double)org[d] - 1.0, dx), xstart);
+        G.off[d] = (float)(X0 - S.ci0[d]);
+        G.tc0[d] = (float)S.tci0[d];
+        G.tc1[d] = (float)S.tci1[d];
+        G.dci[d] = (float)(S.ci1[d] - S.ci0[d]);
+    }
+    G.dx = (float)dx;
+    G.g = (float)((S.s1 - S.s0) * L / S.ndci0);
+    // Taylor shift of the quintic around z0 = zs0 * Len: b_k = sum_{m>=k} C(m,k) a_m z0^(m-k)
+    const double z0 = S.zs0 * L;
+    double zp[6];
+    zp[0] = 1.0;
+    for (int m = 1; m < 6; ++m) zp[m] = zp[m - 1] * z0;
+    const double C[6][6] = {{1, 0, 0, 0, 0, 0},  {1, 1, 0, 0, 0, 0},  {1, 2, 1, 0, 0, 0},
+                            {1, 3, 3, 1, 0, 0},  {1, 4, 6, 4, 1, 0},  {1, 5, 10, 10, 5, 1}};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double *a = coe + 6 * d;
+        for (int k = 1; k <= 5; ++k) {
+            double b = 0.0;
+            for (int m = k; m <= 5; ++m) b += C[m][k] * a[m] * zp[m - k];
+            G.b[d][k - 1] = (float)b;
+        }
+        // unwrapped polynomial value at the start, as spl_pos evaluates it before its wrap
+        double c0 = dmul(a[5], zp[5]);
+        c0 = dadd(c0, dmul(a[4], zp[4]));
+        c0 = dadd(c0, dmul(a[3], zp[3]));
+        c0 = dadd(c0, dmul(a[2], zp[2]));
+        c0 = dadd(c0, dmul(a[1], z0));
+        c0 = dadd(c0, a[0]);
+        G.kq[d] = (int)rint((S.ci0[d] - c0) / dev_pi2());
+        G.thi[d] = (float)(dev_pi() - c0);
+        G.tlo[d] = (float)(-dev_pi() - c0);
+    }
+    G.R2 = (float)(S.Rt * S.Rt);
+    G.Rt = (float)S.Rt;
+    // core size sigma(zeta) = smin + A (sin(omega zeta) + 1), zeta = s0 + W/Len
+    const double omega = floor(P.length / dev_pi() + 0.5) * (double)P.n_T;
+    const double A = (P.sigma_max - P.sigma_min) / 2.0;
+    G.smin = (float)P.sigma_min;
+    G.A = (float)A;
+    double ph = fmod(omega * S.s0, dev_pi2());
+    G.ph0 = (float)ph;
+    G.om = (float)(omega / L);
+    // central difference of dsigmadzeta (subroutine.f90:748-761) in closed form:
+    // (sigma(z+h) - sigma(z-h)) / (2h) = A cos(omega z) sin(omega h) / h
+    const double h = fmin(dzeta_sup, 1.0 * dtf);
+    G.q = (float)(A * sin(omega * h) / h);
+    G.Gamma = (float)P.Gamma;
+    G.Linv = (float)(1.0 / L);
+    G.eta = (float)eta0;
+}
+
+
+// Contribution of sub-segment G at grid offset (ii, jj, kk) from G's origin index
+// (tube.f90:806-892 in the local frame).  General=false is the exact specialisation for a
+// constant core (sigma_ratio = 1) and no twist (eta = 0), where the reference's vorticity
+// reduces to tp * Gamma * T.
+template <bool General>
+__device__ __forceinline__ bool point_f32(const SegF &G, int ii, int jj, int kk, float out[3])
+{
+    const float d0x = fmaf((float)ii, G.dx, G.off[0]);
+    const float d0y = fmaf((float)jj, G.dx, G.off[1]);
+    const float d0z = fmaf((float)kk, G.dx, G.off[2]);
+    const float t0 = d0x * G.tc0[0] + d0y * G.tc0[1] + d0z * G.tc0[2];
+    if (!(t0 >= 0.0f)) return false;
+    const float ex = d0x - G.dci[0], ey = d0y - G.dci[1], ez = d0z - G.dci[2];
+    const float t1 = ex * G.tc1[0] + ey * G.tc1[1] + ez * G.tc1[2];
+    if (!(t1 < 0.0f)) return false;
+    const float r2 = d0x * d0x + d0y * d0y + d0z * d0z - t0 * t0;
+    if (!(r2 < G.R2)) return false;
+    const float W = t0 * G.g;
+    float P[3], c1[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float *b = G.b[d];
+        P[d] = W * fmaf(W, fmaf(W, fmaf(W, fmaf(W, b[4], b[3]), b[2]), b[1]), b[0]);
+        c1[d] = fmaf(W, fmaf(W, fmaf(W, fmaf(W, 5.0f * b[4], 4.0f * b[3]), 3.0f * b[2]), 2.0f * b[1]), b[0]);
+    }
+    float xc[3] = {d0x - P[0], d0y - P[1], d0z - P[2]};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        // x - wrap(c(z)) of the reference, then its cminus wrap (see SegF::kq)
+        int n = G.kq[d] + (P[d] >= G.thi[d] ? 1 : 0) - (P[d] < G.tlo[d] ? 1 : 0);
+        const float v = n ? fmaf(6.28318530717958647692f, (float)n, xc[d]) : xc[d];
+        if (v > 3.14159265358979f) n -= 1;
+        else if (v < -3.14159265358979f) n += 1;
+        if (n) xc[d] = fmaf(6.28318530717958647692f, (float)n, xc[d]);
+    }
+    const float rho2 = xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2];
+    const float n1 = sqrtf(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+    const float in1 = 1.0f / n1;
+    const float T[3] = {c1[0] * in1, c1[1] * in1, c1[2] * in1};
+    if constexpr (!General) {
+        const float s2 = G.smin * G.smin;
+        const float inv2s2 = 0.5f / s2;
+        const float tp = (expf(-rho2 * inv2s2) - expf(-G.R2 * inv2s2)) * (0.159154943f / s2) * G.Gamma;
+        out[0] = tp * T[0];
+        out[1] = tp * T[1];
+        out[2] = tp * T[2];
+        return true;
+    } else {
+        float c2[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const float *b = G.b[d];
+            c2[d] = fmaf(W, fmaf(W, fmaf(W, 20.0f * b[4], 12.0f * b[3]), 6.0f * b[2]), 2.0f * b[1]);
+        }
+        const float ph = fmaf(G.om, W, G.ph0);
+        float sn, cs;
+        sincosf(ph, &sn, &cs);
+        const float sigma = fmaf(G.A, sn + 1.0f, G.smin);
+        const float s2 = sigma * sigma;
+        const float inv2s2 = 0.5f / s2;
+        const float tp = (expf(-rho2 * inv2s2) - expf(-G.R2 * inv2s2)) * (0.159154943f / s2) * G.Gamma;
+        const float dsds = G.q * cs * in1 * G.Linv;
+        const float rho = sqrtf(rho2);
+        const float X[3] = {c1[1] * c2[2] - c1[2] * c2[1], c1[2] * c2[0] - c1[0] * c2[2], c1[0] * c2[1] - c1[1] * c2[0]};
+        const float nX = sqrtf(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+        const float inr = 1.0f / (rho + 1.0e-15f);
+        if (nX < 1.0e-8f) {
+            const float er[3] = {xc[0] * inr, xc[1] * inr, xc[2] * inr};
+            const float eth[3] = {er[1] * T[2] - er[2] * T[1], er[2] * T[0] - er[0] * T[2], er[0] * T[1] - er[1] * T[0]};
+            const float a = G.eta * rho, bq = rho * dsds / sigma;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) out[d] = tp * (T[d] + a * eth[d] + bq * er[d]);
+        } else {
+            const float inX = 1.0f / nX;
+            const float B[3] = {X[0] * inX, X[1] * inX, X[2] * inX};
+            const float Nv[3] = {B[1] * T[2] - B[2] * T[1], B[2] * T[0] - B[0] * T[2], B[0] * T[1] - B[1] * T[0]};
+            const float kap = nX * in1 * in1 * in1;
+            const float costh = (xc[0] * Nv[0] + xc[1] * Nv[1] + xc[2] * Nv[2]) * inr;
+            const float sinth = (xc[0] * B[0] + xc[1] * B[1] + xc[2] * B[2]) * inr;
+            const float iden = 1.0f / (1.0f - kap * rho * costh);
+            const float t5 = -sinth * rho * iden, t6 = costh * rho * iden;
+            const float t7 = costh * rho * dsds / sigma * iden, t8 = sinth * rho * dsds / sigma * iden;
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                out[d] = tp * (T[d] + G.eta * (t5 * Nv[d] + t6 * B[d]) + (t7 * Nv[d] + t8 * B[d]));
+        }
+        return true;
+    }
+}
+
+int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc);
+int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out);
+
+}  // namespace fwt

@@ -1,0 +1,151 @@
+/*
+ * fwt.h -- C-ABI of the B200 woven-field construction library (libfwt.so).
+ *
+ * The reference (FastWeavTurb, program `Weav_ver5_8_2`) is one Fortran/MPI program whose
+ * seams are implicit-interface subroutines and two input files.  Each entry point below
+ * replaces one of those seams; the citation names the reference code it stands in for.
+ * Plain C types only: pointers, sizes, doubles.  Every function returns 0 on success and
+ * a negative FWT_E_* code on error; fwt_last_error() gives the message (thread-local).
+ *
+ * Host arrays are caller-owned.  A 3-D field crossing this boundary is column-major
+ * (x fastest), i.e. Fortran `field(nx, ny, nz)`.  Device memory is owned by the context.
+ * One context per host thread; no internal locking.
+ */
+#ifndef FWT_H
+#define FWT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FWT_OK 0
+#define FWT_E_ARG (-1)      /* invalid argument */
+#define FWT_E_CUDA (-2)     /* CUDA runtime / cuFFT failure */
+#define FWT_E_IO (-3)       /* file missing, unreadable or malformed */
+#define FWT_E_STATE (-4)    /* call out of order (e.g. statistics before velocity) */
+#define FWT_E_NOMEM (-5)    /* device allocation failed or exceeds the cap */
+#define FWT_E_TIMEOUT (-6)  /* a bounded device-side wait ran out */
+#define FWT_E_RANGE (-7)    /* value outside the supported range */
+
+typedef struct fwt_ctx fwt_ctx;
+
+/* Run parameters: the scalar block of parameters_input.dat (tube.f90:190-217) plus the
+ * compile-time switches of tube.f90:53-59,129 as runtime fields. */
+typedef struct {
+    int N;              /* grid points per side, nx = ny = nz (tube.f90:193,200-201) */
+    int N_downsample;   /* field output points per side (tube.f90:195,1056) */
+    int line_s, line_e; /* 1-based inclusive range of lines to deposit (tube.f90:197-199,528) */
+    double sigma_ratio; /* sigma_max / sigma_min (tube.f90:203,538) */
+    double eta_t;       /* twist rate eta0 (tube.f90:206) */
+    int ntf_times;      /* sub-segments per 2pi of turning (tube.f90:210,641) */
+    int ntf_pre;        /* presamples per section (tube.f90:212,627) */
+    double Rtube_ratio; /* truncation radius / sigma (tube.f90:214,790) */
+    double dzeta_sup;   /* upper bound of the sigma difference step (tube.f90:217,826) */
+    int precision;      /* 32: FP32 bulk arithmetic; 64: FP64 throughout */
+    int deposit_mode;   /* 0: tile-owned cell-list kernel (default); 1: reference box walk */
+    int device;         /* CUDA device ordinal */
+    void *stream;       /* cudaStream_t to launch on, or NULL for a context-owned stream */
+    int if_pdf;         /* tube.f90:57 (default 1) */
+    int if_Sp;          /* tube.f90:58 (default 1) */
+    int Sp_order;       /* tube.f90:58 (default 10) */
+    int pdf_bins;       /* tube.f90:129 bin_num (default 1000) */
+    int vorticity_output; /* tube.f90:55 (default 1) */
+    size_t mem_cap;     /* bytes of device memory the context may hold (0 = no cap) */
+} fwt_params;
+
+/* Fill *p with the reference defaults (the values of FBB_with_parameters.m:205-225 and
+ * the switches of tube.f90:53-59). */
+int fwt_default_params(fwt_params *p);
+
+/* Replaces MPI_Init + set_fft_plans + wavenumber (tube.f90:161-163,306-307;
+ * subroutine.f90:860-919). */
+int fwt_create(const fwt_params *p, fwt_ctx **out);
+/* Replaces destroy_fft_plans + the deallocations + MPI_Finalize (tube.f90:1213-1238). */
+int fwt_destroy(fwt_ctx *ctx);
+
+/* Reads both input files; the scalar block of params_path overrides N..dzeta_sup of the
+ * context (tube.f90:168-223, 341-379).  Writes nothing. */
+int fwt_load_inputs(fwt_ctx *ctx, const char *centerline_path, const char *params_path);
+
+/* Array form of the same inputs (tube.f90:353-379 after the broadcasts): nline lines,
+ * npoint[l] nodes each, xyz row-major (npointall x 3) host doubles in [-pi,pi), and the
+ * per-line columns of parameters_input.dat (tube.f90:221-223). */
+int fwt_set_centerlines(fwt_ctx *ctx, int nline, const int64_t *npoint, const double *xyz,
+                        const double *sigma, const double *Gamma, const int *n_T,
+                        const int *if_filter);
+/* Same, with the node coordinates already on this context's device (x, y, z: npointall
+ * doubles each).  The device arrays must stay valid until fwt_deposit returns. */
+int fwt_set_centerlines_device(fwt_ctx *ctx, int nline, const int64_t *npoint, const double *d_x,
+                               const double *d_y, const double *d_z, const double *sigma,
+                               const double *Gamma, const int *n_T, const int *if_filter);
+
+/* Deposit lines line_s..line_e (1-based inclusive) into omega, applying each flagged
+ * line's spectral filter after it (tube.f90:392-946: centerline preprocessing, quintic
+ * splines, adaptive sub-segmentation, Burgers-tube deposition, filter_spec). */
+int fwt_deposit(fwt_ctx *ctx, int line_s, int line_e);
+/* Sharp spectral low-pass |k|^2 > k_c^2 on omega (subroutine.f90:1225-1277). */
+int fwt_filter(fwt_ctx *ctx, double k_c);
+/* E(k) of omega, then spectral Biot-Savart omega -> u with the energy reduction fused
+ * (tube.f90:972-1023: spectrum + fourier_forward x3 + i k x w / |k|^2 + fourier_backward x3). */
+int fwt_biot_savart(fwt_ctx *ctx);
+/* E, u' = sqrt(2E/3), and the scaling of omega and u by 1/u'; enstrophy after scaling
+ * (tube.f90:1026-1044, cal_helicity subroutine.f90:1550-1569). */
+int fwt_normalize(fwt_ctx *ctx, double *up, double *Etot, double *enstrophy);
+/* Shell spectrum, nshell = N/2 values for shells 1..N/2 (subroutine.f90:1604-1638).
+ * which = 0: omega before normalisation; 1: u after normalisation. */
+int fwt_spectrum(fwt_ctx *ctx, int which, double *Ek, int nshell);
+/* PDF with the reference's REAL(4) bin layout (subroutine.f90:1-62).  which = 0: u,
+ * 1: omega; component = -1 pools the three components (tube.f90:1169-1177), 0/1/2 picks one.
+ * val, pdf: nbins floats; counts (may be NULL): nbins uint64. */
+int fwt_pdf(fwt_ctx *ctx, int which, int component, int nbins, float *val, float *pdf,
+            uint64_t *counts);
+/* Longitudinal structure functions S_p(r), p = 1..pmax, at nr separations r (grid units)
+ * (subroutine.f90:64-129).  Sp: pmax x nr doubles, Sp[(p-1)*nr + m]. */
+int fwt_sp(fwt_ctx *ctx, int pmax, const int *r, int nr, double *Sp);
+/* Downsampled |omega| and omega.u (normalised) as float32, Fortran order
+ * (n_d, n_d, n_d, 2) (tube.f90:1055-1071). */
+int fwt_field_wh(fwt_ctx *ctx, float *host_out);
+/* Copy a normalised (after fwt_normalize) or raw field to the host as doubles,
+ * column-major.  which = 0: omega, 1: u; component 0..2. */
+int fwt_copy_field(fwt_ctx *ctx, int which, int component, double *host_colmajor);
+/* Write the reference's output tree under outdir: parameters_output.dat,
+ * centerline_output.dat, info.dat, test_data.dat, field_wh.dat, stat/spectrum_vor_temp.dat,
+ * stat/spectrum.dat, stat/pdf_um.dat, stat/pdf_wm.dat, stat/Sp.dat (tube.f90:171,226-258,
+ * 519-526,623,1055-1188). */
+int fwt_write_outputs(fwt_ctx *ctx, const char *outdir);
+/* The whole program Weav_ver5_8_2 run in `rundir` (inputs read from it, outputs written to
+ * rundir/output), equivalent to `mpirun ./tube` there (tube.f90:30-1240). */
+int fwt_run_dir(const char *rundir, const fwt_params *p);
+/* The path from centerlines already set on the context to all statistics on the device
+ * (tube.f90:392-1188 without file output).  Host copies of the statistics are made. */
+int fwt_run(fwt_ctx *ctx);
+
+/* Per-phase device times in milliseconds of the last fwt_run / phase calls:
+ * t[0] centerline set-up, t[1] deposition, t[2] Biot-Savart + spectra, t[3] statistics,
+ * t[4] total.  Returns the number of values written (<= n). */
+int fwt_timings(fwt_ctx *ctx, double *t, int n);
+/* Counters of the last deposition: c[0] lines, c[1] sections, c[2] sub-segments,
+ * c[3] candidate (tile, sub-segment) pairs, c[4] kernel launches of the last fwt_run. */
+int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
+
+/* Message of the last error on this thread. */
+int fwt_last_error(char *buf, int len);
+
+/* ------------------------------------------------------------------ fBb generator
+ * Fractional-Brownian-bridge centerlines on the device (FBB_with_parameters.m:76-126).
+ * levels: nlev entries of (tubes, nodes per tube, H, dB).  Output xyz device arrays
+ * sized sum(tubes*nodes); d_x/d_y/d_z must be device pointers of this context's device.
+ * Tube t (global index over levels) draws from Philox stream (seed, t).  FP64 prefix sums. */
+int fwt_fbb_generate(fwt_ctx *ctx, uint64_t seed, int nlev, const int *tubes, const int *nodes,
+                     const double *H, const double *dB, double *d_x, double *d_y, double *d_z);
+/* Circulation signs (+1/-1) of tubes [0, ntubes) for the same seed. */
+int fwt_fbb_signs(uint64_t seed, int ntubes, int *signs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FWT_H */

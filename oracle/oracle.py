@@ -1,0 +1,504 @@
+"""FP64 CPU ORACLE for the woven-field construction path -- test infrastructure only.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference
+leg may import this module, and only as the checker.  The product path (the CUDA
+library ``fastweavturb_b200``) never calls it.
+
+It restates the reference program ``Weav_ver5_8_2`` (tube.f90 + subroutine.f90):
+
+* deposition (tube.f90:392-904) -> C restatement in ``fwt_oracle.c`` (OpenMP over z-slabs)
+* per-line spectral filter        -> :func:`filter_spec`   (subroutine.f90:1225-1277)
+* 3-D FFT with 1/N per axis        -> :func:`fourier_forward` / :func:`fourier_backward`
+                                      (subroutine.f90:983-1084, mathematically identical
+                                      c2c transform via numpy's pocketfft)
+* Biot-Savart                      -> :func:`biot_savart` (tube.f90:994-1007)
+* energy normalisation             -> :func:`normalise` (tube.f90:1026-1044)
+* spectrum                         -> :func:`spectrum` (subroutine.f90:1604-1638)
+* PDF                              -> :func:`pdf` (subroutine.f90:1-62)
+* structure functions              -> :func:`structure_functions` (subroutine.f90:64-129)
+* field output                     -> :func:`field_wh` (tube.f90:1055-1073)
+
+Parity status: UNPINNED against the reference binary (Fortran + MPI + FFTW; no Fortran
+compiler exists in this image and the reference ships no golden outputs).  The oracle is
+pinned by analytic known-answer tests instead (tests/test_oracle_kat.py).
+
+Array convention: a field is a numpy array of shape (N, N, N) indexed [k, j, i] in C
+order, i.e. the same memory order as the reference's column-major ``vor(i, j, k)``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liborc.so")
+_lib = None
+
+PI = 3.141592653589793  # 4*datan(1d0)
+PI2 = 2.0 * PI
+
+
+def build() -> str:
+    """Compile the C part of the oracle into oracle/_build/liborc.so."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.orc_line_prep.argtypes = [ctypes.c_int, dp, dp, dp, dp, dp, dp, dp]
+        L.orc_line_ntf.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ctypes.c_int, ip, dp, dp, dp]
+        L.orc_line_ntf.restype = ctypes.c_int
+        L.orc_line_subsegs.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ctypes.c_int, dp]
+        L.orc_line_subsegs.restype = ctypes.c_long
+        L.orc_deposit_line.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_int, dp, dp, dp, ctypes.c_int, dp]
+        L.orc_deposit_line.restype = ctypes.c_long
+        L.orc_sp.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ip, ctypes.c_int, dp, ctypes.c_int]
+        L.orc_philox.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                 ctypes.POINTER(ctypes.c_uint32)]
+        L.orc_fbb_gauss.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, dp, dp]
+        L.orc_fbb_shift.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
+        L.orc_fbb_shift.restype = ctypes.c_double
+        L.orc_fbb_sign.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
+        L.orc_fbb_sign.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class _Grid(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("sigma_ratio", ctypes.c_double), ("eta0", ctypes.c_double),
+                ("ntf_times", ctypes.c_int), ("ntf_pre", ctypes.c_int),
+                ("Rtube_ratio", ctypes.c_double), ("dzeta_sup", ctypes.c_double)]
+
+
+# ----------------------------------------------------------------------------- inputs
+
+@dataclass
+class Params:
+    """Contents of parameters_input.dat (tube.f90:190-223)."""
+    N: int = 64
+    N_downsample: int = 64
+    line_s: int = 1
+    line_e: int = 1
+    sigma_ratio: float = 1.0
+    eta_t: float = 0.0
+    ntf_times: int = 50
+    ntf_pre: int = 1000
+    Rtube_ratio: float = 3.0
+    dzeta_sup: float = 1e-4
+    sigma: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    Gamma: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    n_T: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int32))
+    if_filter: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int32))
+
+
+@dataclass
+class Centerlines:
+    """Contents of centerline_input.dat: nline, npoint per line, then x y z per node."""
+    npoint: np.ndarray
+    xyz: np.ndarray  # (npointall, 3)
+
+    def line(self, i):
+        off = int(np.sum(self.npoint[:i]))
+        n = int(self.npoint[i])
+        return self.xyz[off:off + n]
+
+
+def read_centerlines(path) -> Centerlines:
+    tok = open(path).read().split()
+    nline = int(float(tok[0]))
+    npoint = np.array([int(float(t)) for t in tok[1:1 + nline]], dtype=np.int64)
+    vals = np.array([float(t) for t in tok[1 + nline:1 + nline + 3 * int(npoint.sum())]], dtype=np.float64)
+    return Centerlines(npoint=npoint, xyz=vals.reshape(-1, 3))
+
+
+def read_parameters(path, nline) -> Params:
+    lines = [ln for ln in open(path).read().splitlines()]
+    # label / value pairs in the order of tube.f90:192-217, then a header row and nline rows
+    vals = [ln.split() for ln in lines]
+    p = Params()
+    p.N = int(vals[1][0])
+    p.N_downsample = int(vals[3][0])
+    p.line_s = int(vals[5][0])
+    p.line_e = int(vals[7][0])
+    p.sigma_ratio = float(vals[9][0])
+    p.eta_t = float(vals[11][0])
+    p.ntf_times = int(vals[14][0])
+    p.ntf_pre = int(vals[16][0])
+    p.Rtube_ratio = float(vals[18][0])
+    p.dzeta_sup = float(vals[20][0])
+    rows = [v for v in vals[23:23 + nline]]
+    sig = np.zeros(nline)
+    gam = np.zeros(nline)
+    nT = np.zeros(nline, dtype=np.int32)
+    filt = np.zeros(nline, dtype=np.int32)
+    for r in rows:
+        i = int(r[0]) - 1
+        sig[i] = float(r[1]); gam[i] = float(r[2]); nT[i] = int(r[3]); filt[i] = int(r[4])
+    p.sigma, p.Gamma, p.n_T, p.if_filter = sig, gam, nT, filt
+    return p
+
+
+# ----------------------------------------------------------------------------- construction
+
+def line_ntf(xyz, ntf_times=50, ntf_pre=1000):
+    """Per-section ntf (n_sec+1 entries), dtf and spline coefficients (tube.f90:598-657)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    n = xyz.shape[0]
+    cx, cy, cz = (np.ascontiguousarray(xyz[:, d]) for d in range(3))
+    ntf = np.zeros(n + 1, dtype=np.int32)
+    dtf = np.zeros(n + 1)
+    coe = np.zeros((n + 1) * 18)
+    L = ctypes.c_double()
+    rc = lib().orc_line_ntf(n, _dp(cx), _dp(cy), _dp(cz), ntf_times, ntf_pre, _ip(ntf), _dp(dtf), _dp(coe),
+                            ctypes.byref(L))
+    if rc != 0:
+        raise ValueError("line needs at least 2 nodes")
+    return ntf, dtf, coe.reshape(n + 1, 3, 6), L.value
+
+
+def line_prep(xyz):
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    n = xyz.shape[0]
+    cx, cy, cz = (np.ascontiguousarray(xyz[:, d]) for d in range(3))
+    cze = np.zeros(n); ck = np.zeros(3 * n); ckk = np.zeros(3 * n)
+    L = ctypes.c_double()
+    lib().orc_line_prep(n, _dp(cx), _dp(cy), _dp(cz), _dp(cze), _dp(ck), _dp(ckk), ctypes.byref(L))
+    return cze, ck.reshape(3, n), ckk.reshape(3, n), L.value
+
+
+def line_subsegs(xyz, ntf_times=50, ntf_pre=1000):
+    """(nsub, 15) table: s0, s1, ci0[3], ci1[3], tci0[3], tci1[3], ndci0 (tube.f90:762-777)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    n = xyz.shape[0]
+    cx, cy, cz = (np.ascontiguousarray(xyz[:, d]) for d in range(3))
+    cnt = lib().orc_line_subsegs(n, _dp(cx), _dp(cy), _dp(cz), ntf_times, ntf_pre, None)
+    out = np.zeros(max(cnt, 1) * 15)
+    lib().orc_line_subsegs(n, _dp(cx), _dp(cy), _dp(cz), ntf_times, ntf_pre, _dp(out))
+    return out[:cnt * 15].reshape(cnt, 15)
+
+
+def deposit(params: Params, cl: Centerlines, nthreads=None, line_s=None, line_e=None, vor=None):
+    """Deposit lines line_s..line_e (1-based, inclusive) into vor (3,N,N,N); applies the
+    per-line spectral filter of lines flagged if_filter (tube.f90:528-946)."""
+    N = params.N
+    if vor is None:
+        vor = np.zeros((3, N, N, N))
+    if nthreads is None:
+        nthreads = os.cpu_count() or 1
+    g = _Grid(N, params.sigma_ratio, params.eta_t, params.ntf_times, params.ntf_pre,
+              params.Rtube_ratio, params.dzeta_sup)
+    ls = params.line_s if line_s is None else line_s
+    le = params.line_e if line_e is None else line_e
+    stats = np.zeros(3)
+    info = []
+    vx, vy, vz = vor[0], vor[1], vor[2]
+    for il in range(ls, le + 1):
+        xyz = np.ascontiguousarray(cl.line(il - 1), dtype=np.float64)
+        cx, cy, cz = (np.ascontiguousarray(xyz[:, d]) for d in range(3))
+        nsub = lib().orc_deposit_line(ctypes.byref(g), xyz.shape[0], _dp(cx), _dp(cy), _dp(cz),
+                                      float(params.sigma[il - 1]), float(params.Gamma[il - 1]),
+                                      int(params.n_T[il - 1]), _dp(vx), _dp(vy), _dp(vz), nthreads,
+                                      _dp(stats))
+        if nsub < 0:
+            raise ValueError(f"line {il}: needs at least 2 nodes")
+        info.append((il, xyz.shape[0], int(stats[0]) // (xyz.shape[0] + 1), int(stats[1]), int(stats[2])))
+        if params.if_filter[il - 1]:
+            k_c = int(np.ceil(4.0 / params.sigma[il - 1]))
+            filter_spec(k_c, vor)
+    return vor, info
+
+
+# ----------------------------------------------------------------------------- spectral
+
+def wavenumbers(N):
+    """kx(i) = (mod(i-1+N/2, N) - N/2) * (2pi/lx) with lx = 2pi (subroutine.f90:888-919)."""
+    i = np.arange(N)
+    return ((i + N // 2) % N - N // 2).astype(np.float64)
+
+
+def k2_grid(N):
+    k = wavenumbers(N)
+    return k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2  # [kz, ky, kx]
+
+
+def fourier_forward(phy):
+    """3-D forward transform scaled by 1/N per axis (subroutine.f90:983-1024)."""
+    N = phy.shape[0]
+    return np.fft.fftn(phy) / float(N) ** 3
+
+
+def fourier_backward(spec):
+    """Unscaled backward transform, real part (subroutine.f90:1037-1084)."""
+    N = spec.shape[0]
+    return np.real(np.fft.ifftn(spec)) * float(N) ** 3
+
+
+def filter_spec(k_c, vor):
+    """Sharp spectral cutoff |k|^2 > k_c^2 on each component (subroutine.f90:1225-1277)."""
+    N = vor.shape[1]
+    mask = k2_grid(N) > k_c ** 2
+    for c in range(3):
+        s = fourier_forward(vor[c])
+        s[mask] = 0.0
+        vor[c] = fourier_backward(s)
+    return vor
+
+
+def biot_savart(vor):
+    """u = curl^-1 omega spectrally: u^ = i k x w^ / |k|^2, u^(0)=0 (tube.f90:991-1017)."""
+    N = vor.shape[1]
+    k = wavenumbers(N)
+    kz, ky, kx = k[:, None, None], k[None, :, None], k[None, None, :]
+    k2 = kx ** 2 + ky ** 2 + kz ** 2
+    k2s = k2.copy()
+    k2s[0, 0, 0] = 1.0
+    wx, wy, wz = (fourier_forward(vor[c]) for c in range(3))
+    ux = 1j * (ky * wz - kz * wy) / k2s
+    uy = 1j * (kz * wx - kx * wz) / k2s
+    uz = 1j * (kx * wy - ky * wx) / k2s
+    for s in (ux, uy, uz):
+        s[0, 0, 0] = 0.0
+    return np.stack([fourier_backward(ux), fourier_backward(uy), fourier_backward(uz)])
+
+
+def cal_helicity(a, b, dv):
+    """sum a.b * dv in the reference's serial order (subroutine.f90:1550-1569)."""
+    return float(np.sum(a[0] * b[0] + a[1] * b[1] + a[2] * b[2], dtype=np.float64)) * dv
+
+
+def normalise(vor, vel):
+    """Scale omega and u by u' = sqrt(2E/3) (tube.f90:1026-1044).  Returns dict of scalars."""
+    N = vor.shape[1]
+    dx = PI2 / N
+    dv = dx * dx * dx
+    Etot = cal_helicity(vel, vel, dv)
+    Etot = Etot / 2.0 / PI2 / PI2 / PI2
+    up = np.sqrt(2 * Etot / 3)
+    vor /= up
+    vel /= up
+    diss = cal_helicity(vor, vor, dv)
+    enstrophy = diss / 2.0 / PI2 / PI2 / PI2
+    return {"Etot": Etot, "up": up, "Enstrophy": enstrophy}
+
+
+def spectrum(f, faithful=False):
+    """Shell spectrum E(k) = sum_{nint|k|=i} 1/2 |f^|^2, i=1..nek (subroutine.f90:1604-1638).
+
+    faithful=True reproduces the reference's REAL(4) per-mode values and REAL(4) shell sums
+    (summation order within a shell is the memory order); otherwise FP64 throughout."""
+    N = f.shape[1]
+    nek = int(np.sqrt(np.float32((N * N * 3) / 12.0)))
+    ik2 = (np.sqrt(k2_grid(N) + 0.00000001) + 0.5).astype(np.int64)
+    if faithful:
+        spec = np.zeros((N, N, N), dtype=np.float32)
+        for c in range(3):
+            s = fourier_forward(f[c])
+            spec = (spec.astype(np.float64) + np.real(s * np.conj(s)) / 2.0).astype(np.float32)
+        out = np.zeros(nek, dtype=np.float32)
+        flat_i = ik2.ravel()
+        flat_s = spec.ravel()
+        for i in range(1, nek + 1):
+            acc = np.float32(0.0)
+            sel = flat_s[flat_i == i]
+            for v in sel:  # serial float32 accumulation
+                acc = np.float32(acc + v)
+            out[i - 1] = acc
+        return out
+    e = np.zeros((N, N, N))
+    for c in range(3):
+        s = fourier_forward(f[c])
+        e += 0.5 * (s.real ** 2 + s.imag ** 2)
+    return np.bincount(ik2.ravel(), weights=e.ravel(), minlength=nek + 1)[1:nek + 1]
+
+
+# ----------------------------------------------------------------------------- statistics
+
+def pdf_edges(vmin, vmax, nbins):
+    """Bin centres and edges in the reference's REAL(4) arithmetic (subroutine.f90:12-20,27)."""
+    f32 = np.float32
+    vmin, vmax = f32(vmin), f32(vmax)
+    bsz = f32(f32(vmax - vmin) / f32(nbins))
+    l = np.arange(nbins)
+    # val(l) = min + 0.5d0*bin_size + real(l-1)*bin_size : the first sum is REAL(8), the
+    # product real(l-1)*bin_size is REAL(4); the result is stored in REAL(4)
+    val = (np.float64(vmin) + 0.5 * np.float64(bsz) + (l.astype(f32) * bsz).astype(np.float64)).astype(f32)
+    half = f32(f32(0.5) * bsz)
+    lo = (val - half).astype(f32)
+    hi = (val + half).astype(f32)
+    return val, lo, hi, bsz
+
+
+def pdf_counts(data_f32, vmin, vmax, nbins):
+    """Integer counts with the reference's first-match bin search (subroutine.f90:22-34):
+    a value goes to the first l with lo(l) <= v < hi(l), or nowhere."""
+    val, lo, hi, bsz = pdf_edges(vmin, vmax, nbins)
+    v = np.asarray(data_f32, dtype=np.float32).ravel()
+    # hi is non-decreasing: the first l with v < hi(l)
+    l = np.searchsorted(hi, v, side="right")
+    ok = l < nbins
+    lc = np.minimum(l, nbins - 1)
+    ok &= lo[lc] <= v
+    counts = np.bincount(lc[ok], minlength=nbins).astype(np.int64)
+    return val, counts, bsz
+
+
+def pdf(data_f32, nbins=1000):
+    """PDF of REAL(4) data: (val, pdf) as REAL(4) (subroutine.f90:1-40)."""
+    d = np.asarray(data_f32, dtype=np.float32)
+    vmin, vmax = d.min(), d.max()
+    val, counts, bsz = pdf_counts(d, vmin, vmax, nbins)
+    n = d.size
+    # pdf_v(l)/(bin_size*nx*ny*nzp*nproc) evaluated left to right in REAL(4)
+    shape = d.shape if d.ndim == 3 else (n, 1, 1)
+    den = np.float32(bsz)
+    for s in shape:
+        den = np.float32(den * np.float32(s))
+    p = (counts.astype(np.float32) / den).astype(np.float32)
+    return val, p, counts
+
+
+def sp_separations(N):
+    """r_m = floor(sqrt(2.0)**m + 0.5), m = 0..2*lg2L, in REAL(4) (subroutine.f90:78,97-98)."""
+    lg2L = int(np.floor(np.float32(np.log(np.float32(N)) / np.log(np.float32(2.0))) + np.float32(0.01)))
+    s2 = np.float32(np.sqrt(np.float32(2.0)))
+    rs = []
+    for m in range(0, 2 * lg2L + 1):
+        p = np.float32(1.0)
+        # integer power by repeated squaring, as compilers lower x**n
+        base, e = s2, m
+        while e:
+            if e & 1:
+                p = np.float32(p * base)
+            base = np.float32(base * base)
+            e >>= 1
+        rs.append(int(np.floor(np.float32(p + np.float32(0.5)))))
+    return np.array(rs, dtype=np.int32)
+
+
+def structure_functions(vel, pmax=10, r=None, nthreads=None):
+    """S_p(r) = <du_x^p + du_y^p + du_z^p>/3 with longitudinal increments (subroutine.f90:64-129).
+    Returns (r, Sp[pmax, nr])."""
+    N = vel.shape[1]
+    if r is None:
+        r = sp_separations(N)
+    r = np.ascontiguousarray(r, dtype=np.int32)
+    out = np.zeros(pmax * len(r))
+    ux, uy, uz = (np.ascontiguousarray(vel[c], dtype=np.float64) for c in range(3))
+    lib().orc_sp(N, _dp(ux), _dp(uy), _dp(uz), pmax, _ip(r), len(r), _dp(out), nthreads or (os.cpu_count() or 1))
+    return r, out.reshape(pmax, len(r))
+
+
+def structure_functions_np(vel, pmax=10, r=None):
+    """Vectorised FP64 restatement of the same sums (for speed on larger grids)."""
+    N = vel.shape[1]
+    if r is None:
+        r = sp_separations(N)
+    Sp = np.zeros((pmax, len(r)))
+    for m, rr in enumerate(r):
+        dux = np.roll(vel[0], -rr, axis=2) - vel[0]
+        duy = np.roll(vel[1], -rr, axis=1) - vel[1]
+        duz = np.roll(vel[2], -rr, axis=0) - vel[2]
+        px = np.ones_like(dux); py = np.ones_like(duy); pz = np.ones_like(duz)
+        for p in range(1, pmax + 1):
+            px *= dux; py *= duy; pz *= duz
+            Sp[p - 1, m] = np.sum(px + py + pz) / N / N / N / 3.0
+    return np.asarray(r), Sp
+
+
+def field_wh(vor, vel, n_d):
+    """Downsampled |omega| and omega.u as REAL(4), Fortran order (tube.f90:1055-1071)."""
+    N = vor.shape[1]
+    r_d = N // n_d
+    s = slice(r_d - 1, N, r_d)
+    w = vor[:, s, s, s]
+    u = vel[:, s, s, s]
+    wm = np.sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]).astype(np.float32)
+    h = (w[0] * u[0] + w[1] * u[1] + w[2] * u[2]).astype(np.float32)
+    return np.stack([wm, h])  # (2, nz, ny, nx) == Fortran (nx, ny, nz, 2)
+
+
+# ----------------------------------------------------------------------------- pipeline
+
+def run(params: Params, cl: Centerlines, nthreads=None, faithful_spectrum=False, sp_pmax=10):
+    """The whole field-construction path of tube.f90:392-1188 in FP64.  Returns a dict."""
+    vor, info = deposit(params, cl, nthreads=nthreads)
+    out = {"line_info": info}
+    out["spectrum_vor"] = spectrum(vor, faithful=faithful_spectrum)
+    vel = biot_savart(vor)
+    out.update(normalise(vor, vel))
+    out["vor"] = vor
+    out["vel"] = vel
+    out["spectrum"] = spectrum(vel, faithful=faithful_spectrum)
+    out["pdf_u"] = pdf(vel.astype(np.float32).reshape(-1))
+    out["pdf_w"] = pdf(vor.astype(np.float32).reshape(-1))
+    out["Sp_r"], out["Sp"] = structure_functions(vel, pmax=sp_pmax, nthreads=nthreads)
+    out["field_wh"] = field_wh(vor, vel, params.N_downsample)
+    return out
+
+
+# ----------------------------------------------------------------------------- fBb generator
+
+def fbb_circulant_eigs(n, H):
+    """Eigenvalues of the 2n circulant embedding of the fGn covariance (Davies-Harte)."""
+    k = np.arange(n + 1, dtype=np.float64)
+    g = 0.5 * (np.abs(k + 1) ** (2 * H) - 2 * np.abs(k) ** (2 * H) + np.abs(k - 1) ** (2 * H))
+    c = np.concatenate([g, g[n - 1:0:-1]])
+    lam = np.real(np.fft.fft(c))
+    return np.maximum(lam, 0.0)
+
+
+def fbb_tube(seed, tube, Np, H, dB):
+    """One closed fBb centerline (FBB_with_parameters.m:76-120) -> (Np, 3) in [-pi, pi).
+
+    fBm: Davies-Harte circulant embedding (published method, in place of MATLAB's closed
+    wfbm) with Philox Gaussians; FP64 prefix sum; bridge f(j); rms-step normalisation to
+    dB; uniform random shift; wrap mod 2pi - pi."""
+    L = lib()
+    M = 128 if Np < 128 else Np
+    lam = fbb_circulant_eigs(M, H)
+    n2 = 2 * M
+    fbm = np.zeros((3, M))
+    za = np.zeros(n2); zb = np.zeros(n2)
+    for co in range(3):
+        L.orc_fbb_gauss(ctypes.c_uint64(seed), tube, co, n2, _dp(za), _dp(zb))
+        w = np.fft.fft(np.sqrt(lam / n2) * (za + 1j * zb))
+        x = np.real(w[:M])
+        fbm[co] = np.cumsum(x)
+    if Np < 128:
+        r_t = 128 // Np
+        idx = np.ceil(np.arange(1, Np + 1) * r_t).astype(np.int64) - 1
+        fbm = fbm[:, idx]
+    j = np.arange(1, Np + 1, dtype=np.float64)
+    f = 0.5 * ((j / Np) ** (2.0 * H) + 1 - (1.0 - j / Np) ** (2.0 * H))
+    bb = fbm - f[None, :] * fbm[:, Np - 1:Np]
+    d = np.diff(bb, axis=1)
+    rms = float(np.sum(d * d / (Np - 1)))
+    bb = bb * dB / np.sqrt(rms)
+    for co in range(3):
+        bb[co] = bb[co] + (L.orc_fbb_shift(ctypes.c_uint64(seed), tube, co) - 0.5) * 2 * PI
+    bbp = np.mod(bb, 2 * PI) - PI
+    return bbp.T.copy()
+
+
+def fbb_sign(seed, tube):
+    return lib().orc_fbb_sign(ctypes.c_uint64(seed), tube)
