@@ -56,7 +56,7 @@ EXPORTS = [
     "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_set_centerlines",
     "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
     "fwt_pdf", "fwt_sp", "fwt_field_wh", "fwt_copy_field", "fwt_write_outputs", "fwt_run_dir", "fwt_run",
-    "fwt_timings", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
+    "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
 ]
 
 
@@ -94,6 +94,7 @@ def library(path: str | None = None):
         "fwt_run_dir": [ctypes.c_char_p, ctypes.POINTER(_Params)],
         "fwt_run": [vp],
         "fwt_timings": [vp, dp, ip],
+        "fwt_kernel_times": [vp, dp, i64p, ip],
         "fwt_counters": [vp, i64p, ip],
         "fwt_last_error": [ctypes.c_char_p, ip],
         "fwt_fbb_generate": [vp, ctypes.c_uint64, ip, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), dp,
@@ -291,6 +292,16 @@ class Context:
         t = np.zeros(5)
         library().fwt_timings(self._h, _ptr(t, ctypes.c_double), 5)
         return {"setup_ms": t[0], "deposit_ms": t[1], "spectral_ms": t[2], "stats_ms": t[3], "total_ms": t[4]}
+
+    KERNEL_CATEGORIES = ("section_presample", "centerline_setup", "binning", "deposit", "biot_savart", "cufft",
+                         "statistics", "generator")
+
+    def kernel_times(self):
+        """Per-category device ms and launch counts of the last run()."""
+        ms = np.zeros(8)
+        n = np.zeros(8, dtype=np.int64)
+        library().fwt_kernel_times(self._h, _ptr(ms, ctypes.c_double), _ptr(n, ctypes.c_int64), 8)
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_CATEGORIES)}
 
     def counters(self):
         v = np.zeros(5, dtype=np.int64)

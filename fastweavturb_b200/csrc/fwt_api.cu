@@ -50,6 +50,60 @@ void buf_free(Ctx *c, DevBuf &b)
     b.bytes = 0;
 }
 
+int kt_begin(Ctx *c, int cat)
+{
+    if (c->ev_used + 2 > c->ev_pool.size()) {
+        for (int i = 0; i < 64; ++i) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            c->ev_pool.push_back(e);
+        }
+    }
+    const int id = (int)c->ev_used;
+    c->ev_used += 2;
+    cudaEventRecord(c->ev_pool[id], c->stream);
+    c->ev_marks.push_back({cat, id});
+    return id;
+}
+
+void kt_end(Ctx *c, int mark) { cudaEventRecord(c->ev_pool[mark + 1], c->stream); }
+
+void kt_reset(Ctx *c)
+{
+    c->ev_used = 0;
+    c->ev_marks.clear();
+    for (int i = 0; i < 8; ++i) {
+        c->ktime[i] = 0;
+        c->kcount[i] = 0;
+        c->kbytes[i] = 0;
+    }
+}
+
+int kt_collect(Ctx *c)
+{
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    for (auto &m : c->ev_marks) {
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, c->ev_pool[m.second], c->ev_pool[m.second + 1]) == cudaSuccess) {
+            c->ktime[m.first] += ms;
+            c->kcount[m.first] += 1;
+        }
+    }
+    c->ev_marks.clear();
+    c->ev_used = 0;
+    return 0;
+}
+
+// de-interleave row-major xyz (n x 3) into SoA x[], y[], z[]
+__global__ void deinterleave_kernel(const double *__restrict__ aos, int64_t n, double *__restrict__ soa)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        soa[i] = aos[3 * i];
+        soa[n + i] = aos[3 * i + 1];
+        soa[2 * n + i] = aos[3 * i + 2];
+    }
+}
+
 static int validate(const fwt_params &p)
 {
     if (p.N < 4 || p.N > 2048 || (p.N & 1)) return fail(FWT_E_ARG, "N must be even and in 4..2048");
@@ -218,17 +272,14 @@ int fwt_set_centerlines(fwt_ctx *h, int nline, const int64_t *npoint, const doub
     cudaSetDevice(c->dev);
     FWT_TRY(set_lines_common(c, nline, npoint, sigma, Gamma, n_T, if_filter));
     const int64_t n = c->node_off[nline];
-    c->xyz_host.assign(xyz, xyz + 3 * n);
-    FWT_TRY(buf_reserve(c, c->b_nodes, sizeof(double) * 3 * (size_t)n));
-    // SoA on the device: x[], y[], z[]
-    std::vector<double> soa((size_t)(3 * n));
-    for (int64_t i = 0; i < n; ++i) {
-        soa[i] = xyz[3 * i];
-        soa[n + i] = xyz[3 * i + 1];
-        soa[2 * n + i] = xyz[3 * i + 2];
-    }
+    // one copy of the caller's row-major array (fast when it is pinned), then SoA on the device
+    FWT_TRY(buf_reserve(c, c->b_nodes, sizeof(double) * 6 * (size_t)n));
     double *d = (double *)c->b_nodes.p;
-    FWT_CUDA(cudaMemcpyAsync(d, soa.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    double *stage = d + 3 * n;
+    FWT_CUDA(cudaMemcpyAsync(stage, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+    deinterleave_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(stage, n, d);
+    c->launches += 1;
+    FWT_CUDA(cudaGetLastError());
     FWT_CUDA(cudaStreamSynchronize(c->stream));
     c->d_x = d;
     c->d_y = d + n;
@@ -244,7 +295,6 @@ int fwt_set_centerlines_device(fwt_ctx *h, int nline, const int64_t *npoint, con
     if (!c || !d_x || !d_y || !d_z) return fail(FWT_E_ARG, "null argument");
     cudaSetDevice(c->dev);
     FWT_TRY(set_lines_common(c, nline, npoint, sigma, Gamma, n_T, if_filter));
-    c->xyz_host.clear();
     c->d_x = d_x;
     c->d_y = d_y;
     c->d_z = d_z;
@@ -279,9 +329,13 @@ int fwt_deposit(fwt_ctx *h, int line_s, int line_e)
     Ctx *c = (Ctx *)h;
     if (!c) return fail(FWT_E_ARG, "null context");
     cudaSetDevice(c->dev);
+    kt_reset(c);
+    c->t_setup_acc = 0;
     PhaseTimer t(c->stream);
     const int rc = deposit_lines(c, line_s, line_e);
     c->t_ms[1] = t.stop();
+    c->t_ms[0] = c->t_setup_acc;
+    if (rc == 0) FWT_TRY(kt_collect(c));
     return rc;
 }
 
@@ -387,6 +441,8 @@ int fwt_run(fwt_ctx *h)
     cudaSetDevice(c->dev);
     const int64_t l0 = c->launches;
     reset_state(c);
+    kt_reset(c);
+    c->t_setup_acc = 0;
     PhaseTimer total(c->stream);
     {
         PhaseTimer t(c->stream);
@@ -416,35 +472,16 @@ int fwt_run(fwt_ctx *h)
             FWT_TRY(stats_sp(c, c->p.Sp_order, c->sp_r.data(), (int)c->sp_r.size(), c->sp.data()));
         }
         if (c->p.vorticity_output) {
-            const size_t nd = (size_t)c->p.N_downsample;
-            c->field_wh.resize(2 * nd * nd * nd);
-            FWT_TRY(stats_field_wh(c, c->field_wh.data()));
+            // built on the device here; copied to the host by fwt_field_wh / fwt_write_outputs
+            FWT_TRY(stats_field_wh(c, nullptr));
+            c->field_wh.clear();
         }
         c->t_ms[3] = t.stop();
     }
     c->t_ms[4] = total.stop();
+    c->t_ms[0] = c->t_setup_acc;
     c->counters[4] = c->launches - l0;
-    // total length of every line (tube.f90:501-502): Len_Disc * 2pi
-    c->lengthtot = 0.0;
-    for (int l = 0; l < c->nline; ++l) {
-        double L = (l < (int)c->line_len.size()) ? c->line_len[l] : 0.0;
-        if (L == 0.0 && !c->xyz_host.empty()) {
-            // lines outside line_s..line_e: periodic polygon length on the host
-            const double *x = c->xyz_host.data() + 3 * c->node_off[l];
-            const int64_t n = c->npoint[l];
-            for (int64_t i = 0; i < n; ++i) {
-                const int64_t j = (i + 1) % n;
-                double s2 = 0;
-                for (int d = 0; d < 3; ++d) {
-                    double v = std::fabs(x[3 * j + d] - x[3 * i + d]);
-                    if (v > kPi) v -= kPi2;
-                    s2 += v * v;
-                }
-                L += std::sqrt(s2);
-            }
-        }
-        c->lengthtot += L;
-    }
+    FWT_TRY(kt_collect(c));
     // per-line times: the batch times apportioned by section count
     c->timing_line.assign(2 * (size_t)c->nline, 0.0);
     int64_t secs = 0;
@@ -462,6 +499,11 @@ int fwt_write_outputs(fwt_ctx *h, const char *outdir)
     Ctx *c = (Ctx *)h;
     if (!c || !outdir) return fail(FWT_E_ARG, "null argument");
     if (!c->normalised) return fail(FWT_E_STATE, "write_outputs before the statistics were built");
+    if (c->p.vorticity_output && c->field_wh.empty()) {
+        const size_t nd = (size_t)c->p.N_downsample;
+        c->field_wh.resize(2 * nd * nd * nd);
+        FWT_TRY(stats_field_wh(c, c->field_wh.data()));
+    }
     return io_write_outputs(c, outdir);
 }
 
@@ -489,6 +531,18 @@ int fwt_timings(fwt_ctx *h, double *t, int n)
     if (!c || !t) return fail(FWT_E_ARG, "null argument");
     int k = 0;
     for (; k < n && k < 5; ++k) t[k] = c->t_ms[k];
+    return k;
+}
+
+int fwt_kernel_times(fwt_ctx *h, double *ms, int64_t *launches, int n)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !ms) return fail(FWT_E_ARG, "null argument");
+    int k = 0;
+    for (; k < n && k < 8; ++k) {
+        ms[k] = c->ktime[k];
+        if (launches) launches[k] = c->kcount[k];
+    }
     return k;
 }
 

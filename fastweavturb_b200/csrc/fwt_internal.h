@@ -82,7 +82,6 @@ struct Ctx {
     std::vector<int64_t> npoint, node_off;
     std::vector<double> sigma, Gamma;
     std::vector<int> n_T, if_filter;
-    std::vector<double> xyz_host;   // only when set from host / files (for centerline_output)
     bool have_lines = false;
 
     // node coordinates on the device (SoA)
@@ -128,7 +127,24 @@ struct Ctx {
     size_t mem_held = 0;
 
     std::vector<double> timing_line;   // per line: set-up ms, construction ms
+
+    // per-kernel device times of the last fwt_run (CUDA events on the context's stream)
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, int>> ev_marks;   // (category, index of the start event)
+    size_t ev_used = 0;
+    double ktime[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t kcount[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t kbytes[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // algorithmic bytes moved by the category
+    double t_setup_acc = 0;
 };
+
+// kernel time categories
+enum { KT_SECTION = 0, KT_CENTERLINE = 1, KT_BINNING = 2, KT_DEPOSIT = 3, KT_SPECTRAL = 4, KT_FFT = 5, KT_STATS = 6,
+       KT_GEN = 7 };
+int kt_begin(Ctx *c, int cat);            // records a start event; returns a mark id
+void kt_end(Ctx *c, int mark);            // records the matching stop event
+void kt_reset(Ctx *c);
+int kt_collect(Ctx *c);                   // synchronises and sums elapsed times per category
 
 // device memory helpers
 int buf_reserve(Ctx *c, DevBuf &b, size_t bytes);

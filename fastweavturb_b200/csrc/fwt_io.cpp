@@ -215,14 +215,42 @@ int io_write_outputs(Ctx *c, const char *outdir)
         fprintf(f, "%s%s%s%s%s\n", f_int(l + 1).c_str(), f_r4((float)c->sigma[l]).c_str(), f_r4((float)c->Gamma[l]).c_str(),
                 f_int(c->n_T[l]).c_str(), f_int(c->if_filter[l]).c_str());
     fclose(f);
-    // centerline_output.dat (tube.f90:171-173,345-372)
+    // centerline_output.dat (tube.f90:171-173,345-372), nodes read back from the device
+    const int64_t nn = c->node_off[c->nline];
+    std::vector<double> X(nn), Y(nn), Z(nn);
+    FWT_CUDA(cudaMemcpyAsync(X.data(), c->d_x, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaMemcpyAsync(Y.data(), c->d_y, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaMemcpyAsync(Z.data(), c->d_z, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
     FWT_TRY(open_w(od + "/centerline_output.dat", &f));
     fprintf(f, "%s\n", f_int(c->nline).c_str());
     for (int l = 0; l < c->nline; ++l) fprintf(f, "%s\n", f_int(c->npoint[l]).c_str());
-    for (size_t i = 0; i + 2 < c->xyz_host.size(); i += 3)
-        fprintf(f, "%s%s%s\n", f_r8(c->xyz_host[i]).c_str(), f_r8(c->xyz_host[i + 1]).c_str(),
-                f_r8(c->xyz_host[i + 2]).c_str());
+    for (int64_t i = 0; i < nn; ++i) fprintf(f, "%s%s%s\n", f_r8(X[i]).c_str(), f_r8(Y[i]).c_str(), f_r8(Z[i]).c_str());
     fclose(f);
+    // total length of every line (tube.f90:501-502): Len_Disc * 2pi, i.e. the periodic
+    // polygon length; lines outside line_s..line_e were not set up on the device
+    c->lengthtot = 0.0;
+    for (int l = 0; l < c->nline; ++l) {
+        double L = (l < (int)c->line_len.size()) ? c->line_len[l] : 0.0;
+        if (L == 0.0) {
+            const int64_t o = c->node_off[l], n = c->npoint[l];
+            double cze = 0.0;
+            for (int64_t i = 0; i < n; ++i) {
+                const int64_t j = (i + 1) % n;
+                const double dd[3] = {std::fabs(X[o + j] - X[o + i]), std::fabs(Y[o + j] - Y[o + i]),
+                                      std::fabs(Z[o + j] - Z[o + i])};
+                double s2 = 0;
+                for (int d = 0; d < 3; ++d) {
+                    double v = dd[d];
+                    if (v > kPi) v -= kPi2;
+                    s2 += v * v;
+                }
+                cze += std::sqrt(s2);
+            }
+            L = cze;
+        }
+        c->lengthtot += L;
+    }
     // test_data.dat (tube.f90:623,673-676): two records per deposited line
     FWT_TRY(open_w(od + "/test_data.dat", &f));
     for (int l = c->p.line_s - 1; l < c->p.line_e && l < (int)c->line_ntf_sum.size(); ++l) {

@@ -6,7 +6,7 @@
 //   sample_kernel      sample points ci with the endpoint copy          tube.f90:706-723
 //   chord_kernel       chords dci, |dci|, unit chords tci               tube.f90:740-751
 //   subseg_kernel      sub-segment records (unwrap, Rtube, box)          tube.f90:766-798
-#include "k_centerline.cuh"
+#include "k_deposit.cuh"
 
 namespace fwt {
 
@@ -320,7 +320,8 @@ __global__ void subseg_kernel(const LineParam *__restrict__ lp, const int *__res
                               const int64_t *__restrict__ qoff, const double *__restrict__ s_in,
                               const double *__restrict__ ci, const double *__restrict__ tci,
                               const double *__restrict__ ndci, int line_base, int N, double Rtube_ratio,
-                              SubSeg *__restrict__ out)
+                              SubSeg *__restrict__ out, SegRec *__restrict__ rec, const double *__restrict__ coe,
+                              const double *__restrict__ dtf, double dzeta_sup, double eta)
 {
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -366,7 +367,14 @@ __global__ void subseg_kernel(const LineParam *__restrict__ lp, const int *__res
             S.box_lo[d] = (int)floor(dadd(__ddiv_rn(dsub(dsub(mn, xstart), Rt), dx), 1.0));
             S.box_hi[d] = (int)ceil(dadd(__ddiv_rn(dadd(dsub(mx, xstart), Rt), dx), 1.0));
         }
-        out[q0 + tj] = S;
+        if (out) out[q0 + tj] = S;
+        if (rec) {
+            SegF G;
+            seg_setup_f32(S, P, coe, dtf[warp], dzeta_sup, eta, N, S.box_lo[0], S.box_lo[1], S.box_lo[2], G);
+            SegRec R;
+            segrec_from(G, S, R);
+            rec[q0 + tj] = R;
+        }
     }
 }
 
@@ -548,12 +556,17 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B)
     FWT_CUDA(cudaMemcpyAsync(B.slot_line, hslot_line.data(), sizeof(int) * (size_t)slots, cudaMemcpyHostToDevice,
                              c->stream));
 
+    int km = kt_begin(c, KT_CENTERLINE);
     line_prep_kernel<<<nl, 256, 0, c->stream>>>(B.lp, nl, c->d_x, c->d_y, c->d_z, B.cze, B.ck, B.ckk, B.Len,
                                                 B.node_base);
+    kt_end(c, km);
     const unsigned wblocks = (unsigned)((slots * 32 + 255) / 256);
+    km = kt_begin(c, KT_SECTION);
     section_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, c->d_x, c->d_y, c->d_z, B.cze, B.ck,
                                                    B.ckk, B.Len, B.node_base, c->p.ntf_times, c->p.ntf_pre,
                                                    B.coe, B.ntf, B.dtf);
+    kt_end(c, km);
+    km = kt_begin(c, KT_CENTERLINE);
     slot_counts_kernel<<<(unsigned)((slots + 255) / 256), 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf,
                                                                                B.soff, B.qoff);
     line_ntf_stats_kernel<<<nl, 256, 0, c->stream>>>(B.lp, nl, B.ntf, d_misc);
@@ -561,6 +574,7 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B)
     FWT_CUDA(cudaGetLastError());
     FWT_TRY(scan_exclusive_i64(c, B.soff, slots, d_misc + 2 * nl, C.scratch[12]));
     FWT_TRY(scan_exclusive_i64(c, B.qoff, slots, d_misc + 2 * nl + 1, C.scratch[13]));
+    kt_end(c, km);
     // per-line Len and ntf statistics + totals to the host
     std::vector<int64_t> hmisc((size_t)(2 * nl + 2));
     std::vector<double> hLen((size_t)nl);
@@ -585,17 +599,24 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B)
     FWT_TRY(buf_reserve(c, C.scratch[15], sizeof(double) * 3 * (size_t)B.nsamples));    // ci
     FWT_TRY(buf_reserve(c, C.scratch[16], sizeof(double) * 3 * (size_t)B.nsamples));    // tci
     FWT_TRY(buf_reserve(c, C.scratch[17], sizeof(double) * (size_t)B.nsamples));        // ndci
-    FWT_TRY(buf_reserve(c, C.scratch[18], sizeof(SubSeg) * (size_t)std::max<int64_t>(B.nsub, 1)));
+    // the tile-owned FP32 kernel reads compact FP32 records; the box walk reads FP64 records
+    const bool tile_mode = c->p.precision == 32 && c->p.deposit_mode == 0;
+    const size_t rec_bytes = tile_mode ? sizeof(SegRec) : sizeof(SubSeg);
+    FWT_TRY(buf_reserve(c, C.scratch[18], rec_bytes * (size_t)std::max<int64_t>(B.nsub, 1)));
     B.s = (double *)C.scratch[14].p;
     B.ci = (double *)C.scratch[15].p;
     B.tci = (double *)C.scratch[16].p;
     B.ndci = (double *)C.scratch[17].p;
-    B.seg = (SubSeg *)C.scratch[18].p;
+    B.seg = tile_mode ? nullptr : (SubSeg *)C.scratch[18].p;
+    B.rec = tile_mode ? (SegRec *)C.scratch[18].p : nullptr;
+    km = kt_begin(c, KT_CENTERLINE);
     sample_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, c->d_x, c->d_y, c->d_z, B.cze, B.Len,
                                                   B.node_base, B.coe, B.ntf, B.dtf, B.soff, B.s, B.ci);
     chord_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf, B.soff, B.ci, B.tci, B.ndci);
     subseg_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf, B.soff, B.qoff, B.s, B.ci, B.tci,
-                                                  B.ndci, la, c->p.N, c->p.Rtube_ratio, B.seg);
+                                                  B.ndci, la, c->p.N, c->p.Rtube_ratio, B.seg, B.rec, B.coe, B.dtf,
+                                                  c->p.dzeta_sup, c->p.eta_t);
+    kt_end(c, km);
     c->launches += 3;
     FWT_CUDA(cudaGetLastError());
     return 0;

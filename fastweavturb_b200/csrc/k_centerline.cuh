@@ -5,6 +5,8 @@
 
 namespace fwt {
 
+struct SegRec;
+
 // Device arrays of one batch of lines (all views into Ctx::scratch).
 struct CenterlineBatch {
     int la = 0, nl = 0;          // first line (0-based) and number of lines
@@ -19,7 +21,8 @@ struct CenterlineBatch {
     int64_t *soff = nullptr;     // nslots + 1: first sample of each slot
     int64_t *qoff = nullptr;     // nslots + 1: first sub-segment of each slot
     double *s = nullptr, *ci = nullptr, *tci = nullptr, *ndci = nullptr;  // per sample
-    SubSeg *seg = nullptr;       // nsub
+    SubSeg *seg = nullptr;       // nsub FP64 records (reference box walk)
+    SegRec *rec = nullptr;       // nsub FP32 records (tile-owned kernel)
     std::vector<int64_t> line_ntf_sum;  // 2 x nl: sum(ntf), max(ntf) per line
     std::vector<double> Lens;           // Len_Disc per line
 };

@@ -171,6 +171,8 @@ int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
     const int64_t want = (B.nsub * 32 + 255) / 256;
     const unsigned blocks = (unsigned)std::min<int64_t>(want, (int64_t)sms * 64);
+    const int km = kt_begin(c, KT_DEPOSIT);
+    c->kbytes[KT_DEPOSIT] += B.nsub * (int64_t)sizeof(SubSeg);
     if (c->p.precision == 64) {
         double *w = (double *)c->b_w.p;
         deposit_walk_kernel<double, true><<<blocks, 256, 0, c->stream>>>(
@@ -184,6 +186,7 @@ int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc)
             deposit_walk_kernel<float, false><<<blocks, 256, 0, c->stream>>>(
                 B.seg, B.nsub, B.lp, B.la, B.coe, B.dtf, N, c->p.dzeta_sup, c->p.eta_t, w, w + n3, w + 2 * n3, d_acc);
     }
+    kt_end(c, km);
     c->launches += 1;
     FWT_CUDA(cudaGetLastError());
     return 0;
@@ -229,7 +232,19 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
             if (lb < line_e && nodes + c->npoint[lb] > cap) break;
         }
         CenterlineBatch B;
-        FWT_TRY(centerline_setup(c, la, lb, B));
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, c->stream);
+        const int rc_setup = centerline_setup(c, la, lb, B);
+        cudaEventRecord(e1, c->stream);
+        cudaEventSynchronize(e1);
+        float ms_setup = 0;
+        cudaEventElapsedTime(&ms_setup, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        FWT_TRY(rc_setup);
+        c->t_setup_acc += ms_setup;
         for (int i = 0; i < B.nl; ++i) {
             c->line_ntf_sum[la + i] = B.line_ntf_sum[2 * i];
             c->line_ntf_max[la + i] = B.line_ntf_sum[2 * i + 1];

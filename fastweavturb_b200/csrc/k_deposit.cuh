@@ -178,6 +178,173 @@ __device__ __forceinline__ bool point_f32(const SegF &G, int ii, int jj, int kk,
     }
 }
 
+// Compact FP32 record of one sub-segment for the tile kernel (224 bytes, 16-byte aligned):
+// the local frame of SegF taken at the box origin box_lo, the line constants, and the box.
+struct __align__(16) SegRec {
+    float off[3], g;        // off: mesh point at box_lo minus ci0
+    float tc0[3], R2;
+    float tc1[3], ph0;
+    float dci[3], q;
+    float b[15], smin;
+    float thi[3], A;
+    float tlo[3], om;
+    float Gamma, Linv, eta, dx;
+    int kq[3];
+    float inv2s2;           // constant core: 1 / (2 sigma^2)
+    int box_lo[3];
+    float ftd;              // constant core: exp(-Rtube^2 / (2 sigma^2)), the truncation offset
+    int box_hi[3];
+    float amp;              // constant core: Gamma / (2 pi sigma^2)
+};
+static_assert(sizeof(SegRec) == 224, "SegRec layout");
+
+__device__ __forceinline__ void segrec_from(const SegF &G, const SubSeg &S, SegRec &R)
+{
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        R.off[d] = G.off[d];
+        R.tc0[d] = G.tc0[d];
+        R.tc1[d] = G.tc1[d];
+        R.dci[d] = G.dci[d];
+        R.thi[d] = G.thi[d];
+        R.tlo[d] = G.tlo[d];
+        R.kq[d] = G.kq[d];
+        R.box_lo[d] = S.box_lo[d];
+        R.box_hi[d] = S.box_hi[d];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) R.b[5 * d + k] = G.b[d][k];
+    }
+    R.g = G.g;
+    R.R2 = G.R2;
+    R.ph0 = G.ph0;
+    R.q = G.q;
+    R.smin = G.smin;
+    R.A = G.A;
+    R.om = G.om;
+    R.Gamma = G.Gamma;
+    R.Linv = G.Linv;
+    R.eta = G.eta;
+    R.dx = G.dx;
+    // per-record constants of the constant-core profile (tube.f90:845-847 with sigma = smin)
+    const double s2 = (double)G.smin * (double)G.smin;
+    R.inv2s2 = (float)(0.5 / s2);
+    R.ftd = (float)exp(-(double)G.R2 * 0.5 / s2);
+    R.amp = (float)((double)G.Gamma / (dev_pi2() * s2));
+}
+
+// SegF of record R with its origin moved by (di, dj, dk) grid points from box_lo
+__device__ __forceinline__ void segf_from(const SegRec &R, int di, int dj, int dk, SegF &G)
+{
+    const int dd[3] = {di, dj, dk};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        G.off[d] = fmaf((float)dd[d], R.dx, R.off[d]);
+        G.tc0[d] = R.tc0[d];
+        G.tc1[d] = R.tc1[d];
+        G.dci[d] = R.dci[d];
+        G.thi[d] = R.thi[d];
+        G.tlo[d] = R.tlo[d];
+        G.kq[d] = R.kq[d];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) G.b[d][k] = R.b[5 * d + k];
+    }
+    G.dx = R.dx;
+    G.g = R.g;
+    G.R2 = R.R2;
+    G.Rt = sqrtf(R.R2);
+    G.smin = R.smin;
+    G.A = R.A;
+    G.ph0 = R.ph0;
+    G.om = R.om;
+    G.q = R.q;
+    G.Gamma = R.Gamma;
+    G.Linv = R.Linv;
+    G.eta = R.eta;
+}
+
+// The predicate and vorticity of point_f32 evaluated straight from a record, for the grid
+// point at offset d = x - ci0 (tube.f90:806-892 in the local frame).
+template <bool General, typename RecT>
+__device__ __forceinline__ bool point_rec(const RecT &R, float d0x, float d0y, float d0z, float out[3])
+{
+    const float t0 = d0x * R.tc0[0] + d0y * R.tc0[1] + d0z * R.tc0[2];
+    if (!(t0 >= 0.0f)) return false;
+    const float ex = d0x - R.dci[0], ey = d0y - R.dci[1], ez = d0z - R.dci[2];
+    const float t1 = ex * R.tc1[0] + ey * R.tc1[1] + ez * R.tc1[2];
+    if (!(t1 < 0.0f)) return false;
+    const float r2 = d0x * d0x + d0y * d0y + d0z * d0z - t0 * t0;
+    if (!(r2 < R.R2)) return false;
+    const float W = t0 * R.g;
+    float P[3], c1[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float *b = R.b + 5 * d;
+        P[d] = W * fmaf(W, fmaf(W, fmaf(W, fmaf(W, b[4], b[3]), b[2]), b[1]), b[0]);
+        c1[d] = fmaf(W, fmaf(W, fmaf(W, fmaf(W, 5.0f * b[4], 4.0f * b[3]), 3.0f * b[2]), 2.0f * b[1]), b[0]);
+    }
+    const float d0[3] = {d0x, d0y, d0z};
+    float xc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        xc[d] = d0[d] - P[d];
+        int n = R.kq[d] + (P[d] >= R.thi[d] ? 1 : 0) - (P[d] < R.tlo[d] ? 1 : 0);
+        const float v = n ? fmaf(6.28318530717958647692f, (float)n, xc[d]) : xc[d];
+        if (v > 3.14159265358979f) n -= 1;
+        else if (v < -3.14159265358979f) n += 1;
+        if (n) xc[d] = fmaf(6.28318530717958647692f, (float)n, xc[d]);
+    }
+    const float rho2 = xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2];
+    const float in1 = rsqrtf(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
+    const float T[3] = {c1[0] * in1, c1[1] * in1, c1[2] * in1};
+    if constexpr (!General) {
+        const float tp = (expf(-rho2 * R.inv2s2) - R.ftd) * R.amp;
+        out[0] = tp * T[0];
+        out[1] = tp * T[1];
+        out[2] = tp * T[2];
+        return true;
+    } else {
+        float c2[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const float *b = R.b + 5 * d;
+            c2[d] = fmaf(W, fmaf(W, fmaf(W, 20.0f * b[4], 12.0f * b[3]), 6.0f * b[2]), 2.0f * b[1]);
+        }
+        const float ph = fmaf(R.om, W, R.ph0);
+        float sn, cs;
+        sincosf(ph, &sn, &cs);
+        const float sigma = fmaf(R.A, sn + 1.0f, R.smin);
+        const float s2 = sigma * sigma;
+        const float inv2s2 = 0.5f / s2;
+        const float tp = (expf(-rho2 * inv2s2) - expf(-R.R2 * inv2s2)) * (0.159154943f / s2) * R.Gamma;
+        const float dsds = R.q * cs * in1 * R.Linv;
+        const float rho = sqrtf(rho2);
+        const float X[3] = {c1[1] * c2[2] - c1[2] * c2[1], c1[2] * c2[0] - c1[0] * c2[2], c1[0] * c2[1] - c1[1] * c2[0]};
+        const float nX = sqrtf(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+        const float inr = 1.0f / (rho + 1.0e-15f);
+        if (nX < 1.0e-8f) {
+            const float er[3] = {xc[0] * inr, xc[1] * inr, xc[2] * inr};
+            const float eth[3] = {er[1] * T[2] - er[2] * T[1], er[2] * T[0] - er[0] * T[2], er[0] * T[1] - er[1] * T[0]};
+            const float a = R.eta * rho, bq = rho * dsds / sigma;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) out[d] = tp * (T[d] + a * eth[d] + bq * er[d]);
+        } else {
+            const float inX = 1.0f / nX;
+            const float B[3] = {X[0] * inX, X[1] * inX, X[2] * inX};
+            const float Nv[3] = {B[1] * T[2] - B[2] * T[1], B[2] * T[0] - B[0] * T[2], B[0] * T[1] - B[1] * T[0]};
+            const float kap = nX * in1 * in1 * in1;
+            const float costh = (xc[0] * Nv[0] + xc[1] * Nv[1] + xc[2] * Nv[2]) * inr;
+            const float sinth = (xc[0] * B[0] + xc[1] * B[1] + xc[2] * B[2]) * inr;
+            const float iden = 1.0f / (1.0f - kap * rho * costh);
+            const float t5 = -sinth * rho * iden, t6 = costh * rho * iden;
+            const float t7 = costh * rho * dsds / sigma * iden, t8 = sinth * rho * dsds / sigma * iden;
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                out[d] = tp * (T[d] + R.eta * (t5 * Nv[d] + t6 * B[d]) + (t7 * Nv[d] + t8 * B[d]));
+        }
+        return true;
+    }
+}
+
 int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc);
 int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out);
 

@@ -159,17 +159,19 @@ static int spec_buffers(Ctx *c)
 
 static int run_r2c(Ctx *c, void *in, void *out)
 {
+    const int km = kt_begin(c, KT_FFT);
     if (c->p.precision == 64) FWT_CUFFT(cufftExecD2Z(c->plan_r2c, (cufftDoubleReal *)in, (cufftDoubleComplex *)out));
     else FWT_CUFFT(cufftExecR2C(c->plan_r2c, (cufftReal *)in, (cufftComplex *)out));
-    c->launches += 3;
+    kt_end(c, km);
     return 0;
 }
 
 static int run_c2r(Ctx *c, void *in, void *out)
 {
+    const int km = kt_begin(c, KT_FFT);
     if (c->p.precision == 64) FWT_CUFFT(cufftExecZ2D(c->plan_c2r, (cufftDoubleComplex *)in, (cufftDoubleReal *)out));
     else FWT_CUFFT(cufftExecC2R(c->plan_c2r, (cufftComplex *)in, (cufftReal *)out));
-    c->launches += 3;
+    kt_end(c, km);
     return 0;
 }
 
@@ -182,6 +184,9 @@ static int launch_bs(Ctx *c, int mode, double kc2, double *d_shw, double *d_shu,
     const int64_t rows = (int64_t)N * N;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((rows + 7) / 8, (int64_t)sms * 8));
     const size_t shb = sizeof(double) * 2 * (N / 2 + 1);
+    const int km = kt_begin(c, KT_SPECTRAL);
+    // algorithmic bytes: the three half-spectrum components read and written once
+    c->kbytes[KT_SPECTRAL] += (int64_t)(2 * 3 * nh * 2 * real_bytes(c));
     if (c->p.precision == 64) {
         cufftDoubleComplex *s = (cufftDoubleComplex *)c->b_spec.p;
         biot_savart_kernel<double><<<blocks, 256, shb, c->stream>>>(s, s + nh, s + 2 * nh, N, mode, kc2, d_shw, d_shu,
@@ -191,6 +196,7 @@ static int launch_bs(Ctx *c, int mode, double kc2, double *d_shw, double *d_shu,
         biot_savart_kernel<float><<<blocks, 256, shb, c->stream>>>(s, s + nh, s + 2 * nh, N, mode, kc2, d_shw, d_shu,
                                                                    d_tot);
     }
+    kt_end(c, km);
     c->launches += 1;
     FWT_CUDA(cudaGetLastError());
     return 0;

@@ -179,6 +179,7 @@ int stats_minmax(Ctx *c, int which)
     void *f = which ? c->b_u.p : c->b_w.p;
     FWT_TRY(buf_reserve(c, c->scratch[19], 64));
     uint32_t *mm = (uint32_t *)((char *)c->scratch[19].p + 16);
+    const int km = kt_begin(c, KT_STATS);
     mm_init2<<<1, 32, 0, c->stream>>>(mm, 6);
     for (int d = 0; d < 3; ++d) {
         if (c->p.precision == 64)
@@ -186,6 +187,7 @@ int stats_minmax(Ctx *c, int which)
         else
             minmax_kernel<float><<<grid_for(c, n3), 256, 0, c->stream>>>((const float *)f + d * n3, n3, mm + 2 * d);
     }
+    kt_end(c, km);
     c->launches += 4;
     FWT_CUDA(cudaGetLastError());
     uint32_t h[6];
@@ -262,6 +264,7 @@ int stats_pdf(Ctx *c, int which, int comp, int nbins, float *val, float *pdf, ui
     const size_t n3 = field_elems(c);
     const void *f = is_u ? c->b_u.p : c->b_w.p;
     const size_t shb = sizeof(float) * 2 * nbins + sizeof(uint32_t) * nbins;
+    const int km = kt_begin(c, KT_STATS);
     for (int d = 0; d < 3; ++d) {
         if (comp >= 0 && d != comp) continue;
         if (c->p.precision == 64)
@@ -272,6 +275,7 @@ int stats_pdf(Ctx *c, int which, int comp, int nbins, float *val, float *pdf, ui
                                                                            d_hi, nbins, d_cnt);
         c->launches += 1;
     }
+    kt_end(c, km);
     FWT_CUDA(cudaGetLastError());
     std::vector<unsigned long long> hc(nbins);
     FWT_CUDA(cudaMemcpyAsync(hc.data(), d_cnt, sizeof(unsigned long long) * nbins, cudaMemcpyDeviceToHost, c->stream));
@@ -314,6 +318,7 @@ int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp)
     const int64_t groups = (int64_t)N * N / W;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, (int64_t)sms * 4));
     const int mpw = (nr + 7) / 8;
+    const int km = kt_begin(c, KT_STATS);
 #define FWT_SP(REAL, MPW)                                                                                        \
     do {                                                                                                         \
         auto k = sp_kernel<REAL, 10, MPW>;                                                                       \
@@ -329,6 +334,7 @@ int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp)
         else FWT_SP(float, 8);
     }
 #undef FWT_SP
+    kt_end(c, km);
     c->launches += 3;
     FWT_CUDA(cudaGetLastError());
     std::vector<double> h(10 * nr);
@@ -349,12 +355,14 @@ int stats_field_wh(Ctx *c, float *host_out)
     FWT_TRY(buf_reserve(c, c->scratch[8], sizeof(float) * 2 * m3));
     float *d = (float *)c->scratch[8].p;
     const double s = 1.0 / c->up;
+    const int km = kt_begin(c, KT_STATS);
     if (c->p.precision == 64)
         field_wh_kernel<double><<<grid_for(c, m3), 256, 0, c->stream>>>((const double *)c->b_w.p,
                                                                         (const double *)c->b_u.p, N, nd, s, d);
     else
         field_wh_kernel<float><<<grid_for(c, m3), 256, 0, c->stream>>>((const float *)c->b_w.p, (const float *)c->b_u.p,
                                                                        N, nd, s, d);
+    kt_end(c, km);
     c->launches += 1;
     FWT_CUDA(cudaGetLastError());
     (void)n3;

@@ -127,6 +127,11 @@ int fwt_run(fwt_ctx *ctx);
  * t[0] centerline set-up, t[1] deposition, t[2] Biot-Savart + spectra, t[3] statistics,
  * t[4] total.  Returns the number of values written (<= n). */
 int fwt_timings(fwt_ctx *ctx, double *t, int n);
+/* Device time (ms, CUDA events on the context's stream) and launch count of each kernel
+ * category in the last fwt_run: 0 section presampling, 1 other centerline set-up, 2 cell-list
+ * binning, 3 deposition, 4 fused Biot-Savart, 5 cuFFT, 6 statistics, 7 generator.  (The
+ * reference has no counterpart; it logs phase wall times to info.dat, tube.f90:519-953.) */
+int fwt_kernel_times(fwt_ctx *ctx, double *ms, int64_t *launches, int n);
 /* Counters of the last deposition: c[0] lines, c[1] sections, c[2] sub-segments,
  * c[3] candidate (tile, sub-segment) pairs, c[4] kernel launches of the last fwt_run. */
 int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);

@@ -241,16 +241,41 @@ def k2_grid(N):
     return k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2  # [kz, ky, kx]
 
 
+_FFT_WORKERS = 1
+
+
+def set_fft_workers(n):
+    """Threads for the oracle's FFTs (scipy.fft's pocketfft; numpy's when scipy is absent)."""
+    global _FFT_WORKERS
+    _FFT_WORKERS = max(1, int(n))
+
+
+def _fftn(a):
+    try:
+        import scipy.fft as sf
+        return sf.fftn(a, workers=_FFT_WORKERS)
+    except ImportError:
+        return np.fft.fftn(a)
+
+
+def _ifftn(a):
+    try:
+        import scipy.fft as sf
+        return sf.ifftn(a, workers=_FFT_WORKERS)
+    except ImportError:
+        return np.fft.ifftn(a)
+
+
 def fourier_forward(phy):
     """3-D forward transform scaled by 1/N per axis (subroutine.f90:983-1024)."""
     N = phy.shape[0]
-    return np.fft.fftn(phy) / float(N) ** 3
+    return _fftn(phy) / float(N) ** 3
 
 
 def fourier_backward(spec):
     """Unscaled backward transform, real part (subroutine.f90:1037-1084)."""
     N = spec.shape[0]
-    return np.real(np.fft.ifftn(spec)) * float(N) ** 3
+    return np.real(_ifftn(spec)) * float(N) ** 3
 
 
 def filter_spec(k_c, vor):
@@ -363,15 +388,16 @@ def pdf_counts(data_f32, vmin, vmax, nbins):
 
 
 def pdf(data_f32, nbins=1000):
-    """PDF of REAL(4) data: (val, pdf) as REAL(4) (subroutine.f90:1-40)."""
+    """PDF of REAL(4) data shaped (nz, ny, nx) -- the pooled components stacked along z as in
+    tube.f90:1169-1177 -- as (val, pdf) in REAL(4) plus integer counts (subroutine.f90:1-40)."""
     d = np.asarray(data_f32, dtype=np.float32)
+    if d.ndim != 3:
+        raise ValueError("pdf expects a 3-D (nz, ny, nx) array")
     vmin, vmax = d.min(), d.max()
     val, counts, bsz = pdf_counts(d, vmin, vmax, nbins)
-    n = d.size
-    # pdf_v(l)/(bin_size*nx*ny*nzp*nproc) evaluated left to right in REAL(4)
-    shape = d.shape if d.ndim == 3 else (n, 1, 1)
+    # pdf_v(l)/(bin_size*nx*ny*nzp*nproc), left to right in REAL(4)
     den = np.float32(bsz)
-    for s in shape:
+    for s in (d.shape[2], d.shape[1], d.shape[0]):
         den = np.float32(den * np.float32(s))
     p = (counts.astype(np.float32) / den).astype(np.float32)
     return val, p, counts
@@ -449,8 +475,9 @@ def run(params: Params, cl: Centerlines, nthreads=None, faithful_spectrum=False,
     out["vor"] = vor
     out["vel"] = vel
     out["spectrum"] = spectrum(vel, faithful=faithful_spectrum)
-    out["pdf_u"] = pdf(vel.astype(np.float32).reshape(-1))
-    out["pdf_w"] = pdf(vor.astype(np.float32).reshape(-1))
+    N = params.N
+    out["pdf_u"] = pdf(vel.astype(np.float32).reshape(3 * N, N, N))
+    out["pdf_w"] = pdf(vor.astype(np.float32).reshape(3 * N, N, N))
     out["Sp_r"], out["Sp"] = structure_functions(vel, pmax=sp_pmax, nthreads=nthreads)
     out["field_wh"] = field_wh(vor, vel, params.N_downsample)
     return out
