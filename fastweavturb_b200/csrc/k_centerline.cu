@@ -161,8 +161,44 @@ __global__ void section_kernel(const LineParam *__restrict__ lp, const int *__re
         coe[6 * d + 5] = (12.0 * (xpr - xpl) - 6.0 * (vl + vr) * zr - (al - ar) * z2) / (2.0 * z5);
     }
     if (lane < 18) coe_out[18 * warp + lane] = coe[lane];
-    // turning angle theta = sum |c' x c''| / |c'|^2 * dtf_pre * Len over ntf_pre+1 samples
+    // turning angle theta = sum |c' x c''| / |c'|^2 * dtf_pre * Len over ntf_pre+1 samples.
+    // The integrand is evaluated in FP32 and summed in FP64; only an FP32 result that falls
+    // near a step of ceil(ntf_times theta / 2 pi) is recomputed exactly in FP64 below.
     const double dtfp = (zr_ - zl) / (1.0 * ntf_pre);
+    {
+        float cf[18];
+#pragma unroll
+        for (int k = 0; k < 18; ++k) cf[k] = (float)coe[k];
+        const float zstep = (float)(dtfp * L);
+        float thf = 0.0f;
+        for (int tj = lane; tj <= ntf_pre; tj += 32) {
+            const float z = zstep * (float)tj;
+            float dc[3], dd[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float *a = cf + 6 * d;
+                dc[d] = fmaf(fmaf(fmaf(fmaf(5.0f * a[5], z, 4.0f * a[4]), z, 3.0f * a[3]), z, 2.0f * a[2]), z, a[1]);
+                dd[d] = fmaf(fmaf(fmaf(20.0f * a[5], z, 12.0f * a[4]), z, 6.0f * a[3]), z, 2.0f * a[2]);
+            }
+            const float x0 = dc[1] * dd[2] - dc[2] * dd[1];
+            const float x1 = dc[2] * dd[0] - dc[0] * dd[2];
+            const float x2 = dc[0] * dd[1] - dc[1] * dd[0];
+            const float ndc2 = dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2];
+            thf += __fdividef(sqrtf(x0 * x0 + x1 * x1 + x2 * x2), ndc2);
+        }
+        const double th32 = warp_sum((double)thf) * dtfp * L;
+        const double xr = ntf_times * th32 / dev_pi2();
+        const double fr = xr - floor(xr);
+        const bool near_step = fmin(fr, 1.0 - fr) < 1e-4 * (xr + 1.0) || !(xr == xr);
+        if (!__any_sync(0xffffffffu, near_step)) {
+            if (lane == 0) {
+                const int ntf = (int)ceil(xr) + 1;
+                ntf_out[warp] = ntf;
+                dtf_out[warp] = (zr_ - zl) / (1.0 * ntf);
+            }
+            return;
+        }
+    }
     double th = 0.0;
     for (int tj = lane; tj <= ntf_pre; tj += 32) {
         const double s = zl + dtfp * tj;
@@ -377,6 +413,126 @@ __global__ void subseg_kernel(const LineParam *__restrict__ lp, const int *__res
         }
     }
 }
+
+// ------------------------------------------------------------------ fused sub-segment records
+// Sub-segment records straight from the spline coefficients, one thread per sub-segment
+// (tube.f90:706-798): each thread evaluates the three sample points it needs (ci_j, ci_j+1,
+// ci_j+2), the two chords and the FP32 record, with no sample arrays in global memory.
+// Extended samples of section t: ci_j (j < ntf) on the spline, ci_ntf = node t+1 (the endpoint
+// copy, tube.f90:721-723) and ci_{ntf+1} = the first sample of section t+1, so that
+// chord_j = cminus(ci_{j+1}, ci_j) covers j = 0..ntf (tube.f90:740-751).
+__device__ __forceinline__ void spl_pos_fma(const double *__restrict__ a6, double z, double *c3)
+{
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double *a = a6 + 6 * d;
+        double v = fma(fma(fma(fma(fma(a[5], z, a[4]), z, a[3]), z, a[2]), z, a[1]), z, a[0]);
+        if (v >= dev_pi()) v = v - dev_pi2();
+        if (v < -dev_pi()) v = v + dev_pi2();
+        c3[d] = v;
+    }
+}
+
+// slot of every sub-segment of the batch (one warp per section)
+__global__ void subseg_map_kernel(const LineParam *__restrict__ lp, const int *__restrict__ slot_line, int64_t nslots,
+                                  const int *__restrict__ ntf, const int64_t *__restrict__ qoff, int *__restrict__ map)
+{
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= nslots) return;
+    const LineParam &P = lp[slot_line[warp]];
+    if ((int)(warp - P.slot_off) >= P.n_sec) return;
+    const int n = ntf[warp];
+    const int64_t q0 = qoff[warp];
+    for (int j = lane; j < n; j += 32) map[q0 + j] = (int)warp;
+}
+
+__global__ void __launch_bounds__(256) subseg_fused_kernel(
+    const LineParam *__restrict__ lp, const int *__restrict__ slot_line, const int *__restrict__ map, int64_t nsub,
+    const double *__restrict__ X, const double *__restrict__ Y, const double *__restrict__ Z,
+    const double *__restrict__ cze, int64_t node_base, const double *__restrict__ coe, const int *__restrict__ ntf,
+    const double *__restrict__ dtf, const int64_t *__restrict__ qoff, int line_base, int N, double Rtube_ratio,
+    double dzeta_sup, double eta, SegRec *__restrict__ rec)
+{
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nsub) return;
+    const int slot = map[q];
+    const int l = slot_line[slot];
+    const LineParam P = lp[l];
+    const int t = slot - (int)P.slot_off;
+    const int np = P.n_sec;
+    const int j = (int)(q - qoff[slot]);
+    const int n = ntf[slot];
+    const double L = P.Len;
+    const double *czl = cze + (P.node_off - node_base);
+    const double zl = cze_pl_at(czl, np, t), zl1 = cze_pl_at(czl, np, t + 1);
+    const double d = dtf[slot];
+    const double *cf = coe + 18 * (size_t)slot;
+    const int inext = (t + 1 < np) ? t + 1 : 0;
+    // extended sample k of this section (k = j, j+1, j+2)
+    auto sample = [&](int k, double *c3) {
+        if (k < n) {
+            spl_pos_fma(cf, (zl + d * k - zl) * L, c3);
+        } else if (k == n) {
+            c3[0] = X[P.node_off + inext];
+            c3[1] = Y[P.node_off + inext];
+            c3[2] = Z[P.node_off + inext];
+        } else {
+            spl_pos_fma(coe + 18 * (size_t)(slot + 1), (zl1 + dtf[slot + 1] * 1 - zl1) * L, c3);
+        }
+    };
+    double c0[3], c1[3], c2[3];
+    sample(j, c0);
+    sample(j + 1, c1);
+    sample(j + 2, c2);
+    double ch0[3], ch1[3];
+    cminus3(c1, c0, ch0);
+    cminus3(c2, c1, ch1);
+    const double n0 = sqrt(ch0[0] * ch0[0] + ch0[1] * ch0[1] + ch0[2] * ch0[2]);
+    const double n1 = sqrt(ch1[0] * ch1[0] + ch1[1] * ch1[1] + ch1[2] * ch1[2]);
+    const double i0 = 1.0 / n0, i1 = 1.0 / n1;
+    SubSeg S;
+    const double s0 = zl + d * j, s1 = zl + d * (j + 1);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double a = c0[k], b = c1[k];
+        if (b - a > dev_pi()) a = a + dev_pi2();   // mark1, tube.f90:779-785
+        else if (b - a < -dev_pi()) b = b + dev_pi2();
+        S.ci0[k] = a;
+        S.ci1[k] = b;
+        S.tci0[k] = ch0[k] * i0;
+        S.tci1[k] = ch1[k] * i1;
+    }
+    S.s0 = s0;
+    S.s1 = s1;
+    S.ndci0 = n0;
+    S.ssec = zl;
+    S.zs0 = s0 - zl;
+    double Rt;
+    if (P.sigma_max == P.sigma_min) {
+        Rt = Rtube_ratio * P.sigma_min;   // sigma_func is exactly sigma_min when sigma_max = sigma_min
+    } else {
+        Rt = Rtube_ratio * sigma_func(s0, P.length, P.sigma_max, P.sigma_min, P.n_T);
+        Rt = fmax(Rt, Rtube_ratio * sigma_func(s1, P.length, P.sigma_max, P.sigma_min, P.n_T));
+    }
+    S.Rt = Rt;
+    S.slot = slot;
+    S.line = l + line_base;
+    const double inv_dx = (double)N / dev_pi2(), xstart = -dev_pi();
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double mn = fmin(S.ci0[k], S.ci1[k]), mx = fmax(S.ci0[k], S.ci1[k]);
+        // i_min = floor((min - xstart - Rtube)/dx + 1), i_max = ceiling((max - xstart + Rtube)/dx + 1)
+        S.box_lo[k] = (int)floor((mn - xstart - Rt) * inv_dx + 1.0);
+        S.box_hi[k] = (int)ceil((mx - xstart + Rt) * inv_dx + 1.0);
+    }
+    SegF G;
+    seg_setup_f32(S, P, coe, d, dzeta_sup, eta, N, S.box_lo[0], S.box_lo[1], S.box_lo[2], G);
+    SegRec R;
+    segrec_from(G, S, R);
+    rec[q] = R;
+}
+
 
 // ------------------------------------------------------------------ scan
 // Exclusive scan of n int64 values in place; out[n] receives the total.  Three launches:
@@ -595,14 +751,30 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B)
     FWT_CUDA(cudaMemcpyAsync(B.soff + slots, &B.nsamples, sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
     FWT_CUDA(cudaMemcpyAsync(B.qoff + slots, &B.nsub, sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
 
+    // the tile-owned FP32 kernel reads compact FP32 records built by one fused kernel; the box
+    // walk reads FP64 records built from sample arrays
+    const bool tile_mode = c->p.precision == 32 && c->p.deposit_mode == 0;
+    const size_t rec_bytes = tile_mode ? sizeof(SegRec) : sizeof(SubSeg);
+    FWT_TRY(buf_reserve(c, C.scratch[18], rec_bytes * (size_t)std::max<int64_t>(B.nsub, 1)));
+    if (tile_mode) {
+        B.rec = (SegRec *)C.scratch[18].p;
+        FWT_TRY(buf_reserve(c, C.scratch[14], sizeof(int) * (size_t)std::max<int64_t>(B.nsub, 1)));
+        int *d_map = (int *)C.scratch[14].p;
+        km = kt_begin(c, KT_CENTERLINE);
+        subseg_map_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf, B.qoff, d_map);
+        if (B.nsub > 0)
+            subseg_fused_kernel<<<(unsigned)((B.nsub + 255) / 256), 256, 0, c->stream>>>(
+                B.lp, B.slot_line, d_map, B.nsub, c->d_x, c->d_y, c->d_z, B.cze, B.node_base, B.coe, B.ntf, B.dtf,
+                B.qoff, la, c->p.N, c->p.Rtube_ratio, c->p.dzeta_sup, c->p.eta_t, B.rec);
+        kt_end(c, km);
+        c->launches += 2;
+        FWT_CUDA(cudaGetLastError());
+        return 0;
+    }
     FWT_TRY(buf_reserve(c, C.scratch[14], sizeof(double) * (size_t)B.nsamples));        // s
     FWT_TRY(buf_reserve(c, C.scratch[15], sizeof(double) * 3 * (size_t)B.nsamples));    // ci
     FWT_TRY(buf_reserve(c, C.scratch[16], sizeof(double) * 3 * (size_t)B.nsamples));    // tci
     FWT_TRY(buf_reserve(c, C.scratch[17], sizeof(double) * (size_t)B.nsamples));        // ndci
-    // the tile-owned FP32 kernel reads compact FP32 records; the box walk reads FP64 records
-    const bool tile_mode = c->p.precision == 32 && c->p.deposit_mode == 0;
-    const size_t rec_bytes = tile_mode ? sizeof(SegRec) : sizeof(SubSeg);
-    FWT_TRY(buf_reserve(c, C.scratch[18], rec_bytes * (size_t)std::max<int64_t>(B.nsub, 1)));
     B.s = (double *)C.scratch[14].p;
     B.ci = (double *)C.scratch[15].p;
     B.tci = (double *)C.scratch[16].p;

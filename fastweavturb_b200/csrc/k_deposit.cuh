@@ -41,30 +41,23 @@ __device__ __forceinline__ void seg_setup_f32(const SubSeg &S, const LineParam &
         G.dci[d] = (float)(S.ci1[d] - S.ci0[d]);
     }
     G.dx = (float)dx;
-    G.g = (float)((S.s1 - S.s0) * L / S.ndci0);
-    // Taylor shift of the quintic around z0 = zs0 * Len: b_k = sum_{m>=k} C(m,k) a_m z0^(m-k)
+    G.g = (float)((S.s1 - S.s0) * L * (1.0 / S.ndci0));
+    // Taylor shift of the quintic around z0 = zs0 * Len by repeated synthetic division:
+    // c(z0 + W) = sum_k b_k W^k, b_0 = c(z0) (the unwrapped polynomial value at the start)
     const double z0 = S.zs0 * L;
-    double zp[6];
-    zp[0] = 1.0;
-    for (int m = 1; m < 6; ++m) zp[m] = zp[m - 1] * z0;
-    const double C[6][6] = {{1, 0, 0, 0, 0, 0},  {1, 1, 0, 0, 0, 0},  {1, 2, 1, 0, 0, 0},
-                            {1, 3, 3, 1, 0, 0},  {1, 4, 6, 4, 1, 0},  {1, 5, 10, 10, 5, 1}};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const double *a = coe + 6 * d;
-        for (int k = 1; k <= 5; ++k) {
-            double b = 0.0;
-            for (int m = k; m <= 5; ++m) b += C[m][k] * a[m] * zp[m - k];
-            G.b[d][k - 1] = (float)b;
-        }
-        // unwrapped polynomial value at the start, as spl_pos evaluates it before its wrap
-        double c0 = dmul(a[5], zp[5]);
-        c0 = dadd(c0, dmul(a[4], zp[4]));
-        c0 = dadd(c0, dmul(a[3], zp[3]));
-        c0 = dadd(c0, dmul(a[2], zp[2]));
-        c0 = dadd(c0, dmul(a[1], z0));
-        c0 = dadd(c0, a[0]);
-        G.kq[d] = (int)rint((S.ci0[d] - c0) / dev_pi2());
+        double a[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) a[m] = coe[6 * d + m];
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+#pragma unroll
+            for (int j = 4; j >= k; --j) a[j] = fma(z0, a[j + 1], a[j]);
+#pragma unroll
+        for (int k = 1; k <= 5; ++k) G.b[d][k - 1] = (float)a[k];
+        const double c0 = a[0];
+        G.kq[d] = (int)rint((S.ci0[d] - c0) * (1.0 / dev_pi2()));
         G.thi[d] = (float)(dev_pi() - c0);
         G.tlo[d] = (float)(-dev_pi() - c0);
     }
@@ -75,13 +68,18 @@ __device__ __forceinline__ void seg_setup_f32(const SubSeg &S, const LineParam &
     const double A = (P.sigma_max - P.sigma_min) / 2.0;
     G.smin = (float)P.sigma_min;
     G.A = (float)A;
-    double ph = fmod(omega * S.s0, dev_pi2());
-    G.ph0 = (float)ph;
     G.om = (float)(omega / L);
-    // central difference of dsigmadzeta (subroutine.f90:748-761) in closed form:
-    // (sigma(z+h) - sigma(z-h)) / (2h) = A cos(omega z) sin(omega h) / h
-    const double h = fmin(dzeta_sup, 1.0 * dtf);
-    G.q = (float)(A * sin(omega * h) / h);
+    if (A == 0.0) {
+        // constant core: sigma = sigma_min and d sigma / d zeta = 0 exactly
+        G.ph0 = 0.0f;
+        G.q = 0.0f;
+    } else {
+        G.ph0 = (float)fmod(omega * S.s0, dev_pi2());
+        // central difference of dsigmadzeta (subroutine.f90:748-761) in closed form:
+        // (sigma(z+h) - sigma(z-h)) / (2h) = A cos(omega z) sin(omega h) / h
+        const double h = fmin(dzeta_sup, 1.0 * dtf);
+        G.q = (float)(A * sin(omega * h) / h);
+    }
     G.Gamma = (float)P.Gamma;
     G.Linv = (float)(1.0 / L);
     G.eta = (float)eta0;
@@ -178,6 +176,8 @@ __device__ __forceinline__ bool point_f32(const SegF &G, int ii, int jj, int kk,
     }
 }
 
+constexpr int kNoWrap = 1 << 20;   // SegRec::kq[0] marker: the record never needs the wrap logic
+
 // Compact FP32 record of one sub-segment for the tile kernel (224 bytes, 16-byte aligned):
 // the local frame of SegF taken at the box origin box_lo, the line constants, and the box.
 struct __align__(16) SegRec {
@@ -226,10 +226,28 @@ __device__ __forceinline__ void segrec_from(const SegF &G, const SubSeg &S, SegR
     R.eta = G.eta;
     R.dx = G.dx;
     // per-record constants of the constant-core profile (tube.f90:845-847 with sigma = smin)
-    const double s2 = (double)G.smin * (double)G.smin;
-    R.inv2s2 = (float)(0.5 / s2);
-    R.ftd = (float)exp(-(double)G.R2 * 0.5 / s2);
-    R.amp = (float)((double)G.Gamma / (dev_pi2() * s2));
+    const float s2 = G.smin * G.smin;
+    R.inv2s2 = 0.5f / s2;
+    R.ftd = expf(-G.R2 * R.inv2s2);
+    R.amp = G.Gamma * (0.159154943091895336f / s2);
+    // No-wrap flag (kq[0] = kNoWrap): for every point that passes the tests, |W| <= Wm, so
+    // |P| stays clear of both wrap thresholds and |x - c| < pi; the wrap bookkeeping of
+    // point_rec then reduces to x - c = d0 - P.
+    const float dl = sqrtf(G.dci[0] * G.dci[0] + G.dci[1] * G.dci[1] + G.dci[2] * G.dci[2]);
+    const float Wm = (dl + G.Rt) * fabsf(G.g) * 1.01f;
+    bool nowrap = true;
+    float pmax = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float *b = G.b[d];
+        const float pb = Wm * (fabsf(b[0]) + Wm * (fabsf(b[1]) + Wm * (fabsf(b[2]) + Wm * (fabsf(b[3]) + Wm * fabsf(b[4])))));
+        pmax = fmaxf(pmax, pb);
+        if (G.kq[d] != 0 || !(G.thi[d] > pb * 1.01f + 1e-5f) || !(G.tlo[d] < -pb * 1.01f - 1e-5f)) nowrap = false;
+    }
+    if ((dl + 2.0f * G.Rt) * 1.7321f + pmax > 3.0f) nowrap = false;
+    // t0 <= dl + Rt tan(bend) <= dl + Rt holds for bends below 45 degrees
+    if (G.tc0[0] * G.tc1[0] + G.tc0[1] * G.tc1[1] + G.tc0[2] * G.tc1[2] < 0.75f) nowrap = false;
+    if (nowrap) R.kq[0] = kNoWrap;
 }
 
 // SegF of record R with its origin moved by (di, dj, dk) grid points from box_lo
@@ -285,13 +303,16 @@ __device__ __forceinline__ bool point_rec(const RecT &R, float d0x, float d0y, f
     const float d0[3] = {d0x, d0y, d0z};
     float xc[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        xc[d] = d0[d] - P[d];
-        int n = R.kq[d] + (P[d] >= R.thi[d] ? 1 : 0) - (P[d] < R.tlo[d] ? 1 : 0);
-        const float v = n ? fmaf(6.28318530717958647692f, (float)n, xc[d]) : xc[d];
-        if (v > 3.14159265358979f) n -= 1;
-        else if (v < -3.14159265358979f) n += 1;
-        if (n) xc[d] = fmaf(6.28318530717958647692f, (float)n, xc[d]);
+    for (int d = 0; d < 3; ++d) xc[d] = d0[d] - P[d];
+    if (R.kq[0] != kNoWrap) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            int n = R.kq[d] + (P[d] >= R.thi[d] ? 1 : 0) - (P[d] < R.tlo[d] ? 1 : 0);
+            const float v = n ? fmaf(6.28318530717958647692f, (float)n, xc[d]) : xc[d];
+            if (v > 3.14159265358979f) n -= 1;
+            else if (v < -3.14159265358979f) n += 1;
+            if (n) xc[d] = fmaf(6.28318530717958647692f, (float)n, xc[d]);
+        }
     }
     const float rho2 = xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2];
     const float in1 = rsqrtf(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);

@@ -186,6 +186,7 @@ struct CandBox {
     float isb;      // 1 / (dx tc1[axis]), 0 when |tc1[axis]| <= 0.05 (no bound from t1)
     float q2;       // dx^2 (1 - tc0[axis]^2), 0 when the cylinder bound is not used
     float i2q;      // 1 / (2 q2)
+    float rnb;      // (1 + 1e-6) / n[(axis+1)%3]: row -> (jb, jc) without an integer divide
 };
 
 __device__ __forceinline__ void bulk_copy_g2s(void *smem, const void *gmem, uint32_t bytes, uint64_t *bar)
@@ -286,6 +287,7 @@ __device__ __forceinline__ void clip_box(const SegRec &R, uint32_t img, int N, i
     const float q2 = dx * dx * (1.0f - ta * ta);
     B.q2 = q2 > 0.01f * dx * dx ? q2 : 0.0f;
     B.i2q = B.q2 > 0.0f ? 0.5f / B.q2 : 0.0f;
+    B.rnb = nonempty ? 1.000001f / (float)B.n[(B.axis + 1) % 3] : 0.0f;
 }
 
 // Warp-autonomous tile deposition.  Each warp claims chunks of kWarpChunk candidates of the
@@ -406,7 +408,7 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
             // rows run over (b, c) = ((a+1)%3, (a+2)%3); per-axis offsets by selects (no
             // runtime-indexed local arrays)
             const int nb = a == 0 ? B.n[1] : (a == 1 ? B.n[2] : B.n[0]);
-            const int jc = rr / nb, jb = rr - jc * nb;
+            const int jc = (int)((float)rr * B.rnb), jb = rr - jc * nb;
             const int ex = a == 0 ? 0 : (a == 1 ? jc : jb);
             const int ey = a == 0 ? jb : (a == 1 ? 0 : jc);
             const int ez = a == 0 ? jc : (a == 1 ? jb : 0);
