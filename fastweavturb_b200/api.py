@@ -55,7 +55,7 @@ class _Params(ctypes.Structure):
 EXPORTS = [
     "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_set_centerlines",
     "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
-    "fwt_pdf", "fwt_sp", "fwt_field_wh", "fwt_copy_field", "fwt_write_outputs", "fwt_run_dir", "fwt_run",
+    "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_field_wh", "fwt_copy_field", "fwt_write_outputs", "fwt_run_dir", "fwt_run",
     "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
 ]
 

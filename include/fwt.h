@@ -102,6 +102,16 @@ int fwt_spectrum(fwt_ctx *ctx, int which, double *Ek, int nshell);
  * val, pdf: nbins floats; counts (may be NULL): nbins uint64. */
 int fwt_pdf(fwt_ctx *ctx, int which, int component, int nbins, float *val, float *pdf,
             uint64_t *counts);
+/* The same PDF for callers that cannot allocate device memory (no counterpart in the
+ * reference).  d_data: a device field of nx*ny*nz floats (precision 32) or doubles (64) on the
+ * current device; values binned are (float)(x * scale); val, pdf: nbins floats, counts (may
+ * be NULL): nbins uint64, all host memory.  Allocates nothing: its scratch is a static device
+ * array of at most 8192 bins (about 128 KB, held by every GPU that loads the library); larger
+ * nbins is rejected with FWT_E_RANGE.  The first call on a device looks up that array's
+ * address and should come before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race.  stream: a cudaStream_t or NULL. */
+int fwt_pdf_noalloc(const void *d_data, int precision, int nx, int ny, int nz, double scale, int nbins,
+                    void *stream, float *val, float *pdf, uint64_t *counts);
 /* Longitudinal structure functions S_p(r), p = 1..pmax, at nr separations r (grid units)
  * (subroutine.f90:64-129).  Sp: pmax x nr doubles, Sp[(p-1)*nr + m]. */
 int fwt_sp(fwt_ctx *ctx, int pmax, const int *r, int nr, double *Sp);
