@@ -100,6 +100,23 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+# --------------------------------------------------------------------------- replicas
+def max_over_ranks(ms, dist=None, device="cpu"):
+    """The job's time is its slowest rank's: all-reduce MAX of a per-rank device time."""
+    if dist is None:
+        return float(ms)
+    import torch
+
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, steps, N, ms):
+    """Mpts/s of the whole job: every rank builds `steps` fields of N^3 points in `ms`."""
+    return world * steps * N ** 3 / (ms / 1e3) / 1e6
+
+
 # --------------------------------------------------------------------------- CPU sample
 def cpu_sample_estimate(w, nthreads=None):
     """Estimated FP64 CPU time (s) of one whole woven field of workload `w` with the oracle:
@@ -152,7 +169,8 @@ def run_reference(args):
 
     w = CONFIGS[args.config](seed=0)
     nthreads = os.cpu_count() or 1
-    for _ in range(args.warmup):
+    # one untimed sample warms the caches and builds the oracle; more would only cost minutes
+    for _ in range(min(args.warmup, 1)):
         cpu_sample_estimate(w, nthreads)
     ests = []
     t0 = time.perf_counter()
@@ -189,6 +207,8 @@ def main():
     ap.add_argument("--deposit-mode", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--level", type=int, default=None,
+                    help="deposit only this scale level of the workload (a bounded case for profiler captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -211,6 +231,9 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     w = CONFIGS[args.config](seed=rank)
+    if args.level is not None:
+        w.levels = [w.levels[args.level]]
+        w.name += f" -- level {args.level} only (profiling case)"
     stream = torch.cuda.current_stream()
     params = F.Params(N=w.N, N_downsample=w.N, line_s=1, line_e=w.ntubes, sigma_ratio=w.sigma_ratio,
                       eta_t=w.eta_t, ntf_times=w.ntf_times, ntf_pre=w.ntf_pre, Rtube_ratio=w.Rtube_ratio,
@@ -245,20 +268,17 @@ def main():
         dist.barrier()
     clocks.stop()
     ms = e0.elapsed_time(e1)
-    t_max = ms
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = max_over_ranks(ms, dist, "cuda")
     ms_step = t_max / args.steps
-    value = world * args.steps * w.N ** 3 / (t_max / 1e3) / 1e6
+    value = whole_job_rate(world, args.steps, w.N, t_max)
     counters = ctx.counters()
 
     # dominant kernel and its roofline
     peaks, pk_kind = measured_peaks()
     dom = max(ktimes.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_n) = dom
-    kb = _kernel_bytes(ctx, w, counters, args.precision)
+    dep_launches = ktimes.get("deposit", [0.0, 0])[1] // args.steps
+    kb = _kernel_bytes(ctx, w, counters, args.precision, dep_launches)
     dom_bytes = kb.get(dom_name)
     roofline = None
     if dom_n:
@@ -287,15 +307,11 @@ def main():
             ctx.output_v()
         f1.record(stream)
         torch.cuda.synchronize()
-        ems = f0.elapsed_time(f1)
-        if dist:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(f0.elapsed_time(f1), dist, "cuda")
         h2d = int(hx.nbytes)
         d2h = int(2 * nd ** 3 * 4 + 2 * (w.N // 2) * 8 + 2 * params.pdf_bins * 8 * 2
                   + 10 * len(F.sp_separations(w.N)) * 8)
-        e2e = {"value": world * args.steps * w.N ** 3 / (ems / 1e3) / 1e6, "unit": "Mpts/s",
+        e2e = {"value": whole_job_rate(world, args.steps, w.N, ems), "unit": "Mpts/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ems / args.steps}
 
     cpu = None
@@ -330,21 +346,23 @@ def main():
     return 0
 
 
-def _kernel_bytes(ctx, w, counters, precision):
-    """Algorithmic bytes per step of each kernel category (the unit definitions are in
-    DESIGN.md): section presampling reads the node data and writes coefficients, the
-    deposition writes omega once and reads one record per (tile, sub-segment) pair, the fused
+def _kernel_bytes(ctx, w, counters, precision, dep_launches):
+    """Algorithmic bytes per step of each kernel category: section presampling reads the node
+    data and writes coefficients; the deposition writes omega in its first launch, reads and
+    writes it in each later launch (one launch per batch of lines), and reads one 224-byte
+    sub-segment record plus a 4-byte cell-list entry per (tile, sub-segment) pair; the fused
     Biot-Savart reads and writes the half spectrum once."""
     N = w.N
     rb = 4 if precision == 32 else 8
     n3 = N ** 3
     nh = N * N * (N // 2 + 1)
     secs = counters["sections"] + counters["lines"]
-    subseg_record = 152
+    subseg_record = 224
+    field = 3 * n3 * rb * (1 + 2 * max(0, dep_launches - 1))
     return {
         "section_presample": secs * (3 * 8 + 6 * 8 + 8) + secs * (18 * 8 + 4 + 8),
-        "deposit": 3 * n3 * rb + counters["pairs"] * (4 + subseg_record) if counters["pairs"]
-        else counters["subsegments"] * subseg_record + 3 * n3 * rb,
+        "deposit": field + counters["pairs"] * (4 + subseg_record) if counters["pairs"]
+        else counters["subsegments"] * subseg_record + field,
         "biot_savart": 2 * 3 * nh * 2 * rb,
         "cufft": 6 * 3 * n3 * rb * 2,
         "statistics": 3 * n3 * rb * 4,

@@ -39,6 +39,14 @@ static void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1)
     }
 }
 
+/* the bare block function on an arbitrary counter and key (for the published KAT vectors) */
+void orc_philox_raw(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+    philox4x32_10(c, key[0], key[1]);
+    out[0] = c[0]; out[1] = c[1]; out[2] = c[2]; out[3] = c[3];
+}
+
 void orc_philox(uint64_t seed, uint32_t index, uint32_t tube, uint32_t stream, uint32_t out[4])
 {
     uint32_t c[4] = {index, tube, stream, 0u};

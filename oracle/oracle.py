@@ -67,6 +67,8 @@ def lib():
         L.orc_sp.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ip, ctypes.c_int, dp, ctypes.c_int]
         L.orc_philox.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                  ctypes.POINTER(ctypes.c_uint32)]
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.orc_philox_raw.argtypes = [u32p, u32p, u32p]
         L.orc_fbb_gauss.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, dp, dp]
         L.orc_fbb_shift.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
         L.orc_fbb_shift.restype = ctypes.c_double
@@ -529,3 +531,13 @@ def fbb_tube(seed, tube, Np, H, dB):
 
 def fbb_sign(seed, tube):
     return lib().orc_fbb_sign(ctypes.c_uint64(seed), tube)
+
+
+def philox_raw(ctr, key):
+    """Philox4x32-10 block function on a 4-word counter and 2-word key (for KAT vectors)."""
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    lib().orc_philox_raw(c.ctypes.data_as(u32p), k.ctypes.data_as(u32p), out.ctypes.data_as(u32p))
+    return out

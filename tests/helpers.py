@@ -31,3 +31,12 @@ def rel_l2(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def two_tubes(O, N=24, seed=4):
+    """Two closed fBb tubes of different core size and sign on an N^3 grid (oracle inputs)."""
+    xyz = np.concatenate([O.fbb_tube(seed, 0, 96, 0.7, 0.5), O.fbb_tube(seed, 1, 128, 0.6, 0.3)])
+    p = O.Params(N=N, N_downsample=N, line_s=1, line_e=2, sigma_ratio=1.0, sigma=np.array([0.3, 0.17]),
+                 Gamma=np.array([1.0, -0.6]), n_T=np.array([1, 1], dtype=np.int32),
+                 if_filter=np.zeros(2, dtype=np.int32))
+    return p, O.Centerlines(npoint=np.array([96, 128], dtype=np.int64), xyz=xyz)
