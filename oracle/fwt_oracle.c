@@ -341,9 +341,31 @@ typedef struct {
 /* Deposit one centerline into vor (3 arrays of N^3, x fastest = Fortran (i,j,k) order).
  * tube.f90:536-904.  Returns the number of sub-segments, or -1. stats[0]=sum(ntf),
  * stats[1]=ntf_max, stats[2]=accepted points. */
+static long deposit_line(const orc_grid *g, int np, const double *cx, const double *cy, const double *cz,
+                         double sigma_min, double Gamma, int n_T, double *vorx, double *vory, double *vorz,
+                         int nthreads, double *stats, double *cond);
+
 long orc_deposit_line(const orc_grid *g, int np, const double *cx, const double *cy, const double *cz,
                       double sigma_min, double Gamma, int n_T, double *vorx, double *vory,
                       double *vorz, int nthreads, double *stats)
+{
+    return deposit_line(g, np, cx, cy, cz, sigma_min, Gamma, n_T, vorx, vory, vorz, nthreads, stats, NULL);
+}
+
+/* Same, and cond[idx] = max(cond[idx], |1 / (1 - kappa rho cos theta)|) over the point's
+ * contributions (1 on the straight branch): the amplification of the curved branch's
+ * denominator (tube.f90:876-879).  Near the centre of curvature of a bend tighter than the
+ * tube radius it grows without bound and the reference's own FP64 value is ill-conditioned. */
+long orc_deposit_line_cond(const orc_grid *g, int np, const double *cx, const double *cy, const double *cz,
+                           double sigma_min, double Gamma, int n_T, double *vorx, double *vory,
+                           double *vorz, int nthreads, double *stats, double *cond)
+{
+    return deposit_line(g, np, cx, cy, cz, sigma_min, Gamma, n_T, vorx, vory, vorz, nthreads, stats, cond);
+}
+
+static long deposit_line(const orc_grid *g, int np, const double *cx, const double *cy, const double *cz,
+                         double sigma_min, double Gamma, int n_T, double *vorx, double *vory, double *vorz,
+                         int nthreads, double *stats, double *cond)
 {
     orc_line ln;
     if (line_setup(np, cx, cy, cz, g->ntf_times, g->ntf_pre, &ln)) return -1;
@@ -443,6 +465,7 @@ long orc_deposit_line(const orc_grid *g, int np, const double *cx, const double 
                                 cross3(er, T, eth);
                                 for (int d = 0; d < 3; ++d)
                                     vor[d][idx] = vor[d][idx] + tp * Gamma * (T[d] + eta * rho * eth[d] + (rho * dsds / sigma) * er[d]);
+                                if (cond && cond[idx] < 1.0) cond[idx] = 1.0;
                             } else { /* curved branch, tube.f90:868-892 */
                                 double B[3], Nv[3];
                                 for (int d = 0; d < 3; ++d) B[d] = dcddc[d] / ndcddc;
@@ -457,6 +480,7 @@ long orc_deposit_line(const orc_grid *g, int np, const double *cx, const double 
                                 const double t8 = sinth * rho * dsds / sigma / den;
                                 for (int d = 0; d < 3; ++d)
                                     vor[d][idx] = vor[d][idx] + tp * Gamma * (T[d] + eta * (t5 * Nv[d] + t6 * B[d]) + (t7 * Nv[d] + t8 * B[d]));
+                                if (cond && cond[idx] < fabs(1.0 / den)) cond[idx] = fabs(1.0 / den);
                             }
                             accepted_total += 1;
                         }

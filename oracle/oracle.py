@@ -64,6 +64,8 @@ def lib():
         L.orc_deposit_line.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_int, dp, dp, dp, ctypes.c_int, dp]
         L.orc_deposit_line.restype = ctypes.c_long
+        L.orc_deposit_line_cond.argtypes = L.orc_deposit_line.argtypes + [dp]
+        L.orc_deposit_line_cond.restype = ctypes.c_long
         L.orc_sp.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ip, ctypes.c_int, dp, ctypes.c_int]
         L.orc_philox.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
                                  ctypes.POINTER(ctypes.c_uint32)]
@@ -199,9 +201,12 @@ def line_subsegs(xyz, ntf_times=50, ntf_pre=1000):
     return out[:cnt * 15].reshape(cnt, 15)
 
 
-def deposit(params: Params, cl: Centerlines, nthreads=None, line_s=None, line_e=None, vor=None):
+def deposit(params: Params, cl: Centerlines, nthreads=None, line_s=None, line_e=None, vor=None, cond=None):
     """Deposit lines line_s..line_e (1-based, inclusive) into vor (3,N,N,N); applies the
-    per-line spectral filter of lines flagged if_filter (tube.f90:528-946)."""
+    per-line spectral filter of lines flagged if_filter (tube.f90:528-946).
+
+    cond: optional (N,N,N) array; each point receives the maximum over its contributions of
+    |1/(1 - kappa rho cos theta)|, the curved branch's amplification (1 when straight)."""
     N = params.N
     if vor is None:
         vor = np.zeros((3, N, N, N))
@@ -217,10 +222,14 @@ def deposit(params: Params, cl: Centerlines, nthreads=None, line_s=None, line_e=
     for il in range(ls, le + 1):
         xyz = np.ascontiguousarray(cl.line(il - 1), dtype=np.float64)
         cx, cy, cz = (np.ascontiguousarray(xyz[:, d]) for d in range(3))
-        nsub = lib().orc_deposit_line(ctypes.byref(g), xyz.shape[0], _dp(cx), _dp(cy), _dp(cz),
-                                      float(params.sigma[il - 1]), float(params.Gamma[il - 1]),
-                                      int(params.n_T[il - 1]), _dp(vx), _dp(vy), _dp(vz), nthreads,
-                                      _dp(stats))
+        args = (ctypes.byref(g), xyz.shape[0], _dp(cx), _dp(cy), _dp(cz), float(params.sigma[il - 1]),
+                float(params.Gamma[il - 1]), int(params.n_T[il - 1]), _dp(vx), _dp(vy), _dp(vz), nthreads,
+                _dp(stats))
+        if cond is None:
+            nsub = lib().orc_deposit_line(*args)
+        else:
+            assert cond.shape == (N, N, N) and cond.dtype == np.float64 and cond.flags.c_contiguous
+            nsub = lib().orc_deposit_line_cond(*args, _dp(cond))
         if nsub < 0:
             raise ValueError(f"line {il}: needs at least 2 nodes")
         info.append((il, xyz.shape[0], int(stats[0]) // (xyz.shape[0] + 1), int(stats[1]), int(stats[2])))

@@ -154,7 +154,9 @@ def test_straight_tube_is_the_truncated_gaussian_core(orc, axis):
     N, sigma, Gamma = 32, 0.21, 1.7
     y0, z0 = 0.1234, -0.377
     p, cl = _straight_tube(N, sigma, Gamma, y0, z0, axis=axis)
-    vor, _ = orc.deposit(p, cl, nthreads=2)
+    cond = np.zeros((N, N, N))
+    vor, _ = orc.deposit(p, cl, nthreads=2, cond=cond)
+    assert set(np.unique(cond)) <= {0.0, 1.0}          # the straight branch amplifies nothing
     x = -PI + 2 * PI * np.arange(N) / N
     R = 3.0 * sigma
     d1 = (x - y0 + PI) % (2 * PI) - PI
