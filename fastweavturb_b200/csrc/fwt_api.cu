@@ -1,5 +1,7 @@
 // fwt_api.cu -- the C-ABI of libfwt (include/fwt.h): context life cycle, inputs, the phase
 // entry points and the whole-program driver.
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -66,7 +68,22 @@ int kt_begin(Ctx *c, int cat)
     return id;
 }
 
-void kt_end(Ctx *c, int mark) { cudaEventRecord(c->ev_pool[mark + 1], c->stream); }
+void kt_end(Ctx *c, int mark)
+{
+    cudaEventRecord(c->ev_pool[mark + 1], c->stream);
+    // FWT_SYNC_CHECK=1: wait after every timed kernel group and name the group of a fault
+    static const bool check = std::getenv("FWT_SYNC_CHECK") != nullptr;
+    if (check) {
+        const cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            int cat = -1;
+            for (auto &m : c->ev_marks)
+                if (m.second == mark) cat = m.first;
+            std::fprintf(stderr, "libfwt: %s after kernel group %d (mark %d, %lld launches)\n", cudaGetErrorString(e),
+                         cat, mark, (long long)c->launches);
+        }
+    }
+}
 
 void kt_reset(Ctx *c)
 {

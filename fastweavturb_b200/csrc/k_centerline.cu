@@ -108,13 +108,6 @@ __global__ void line_prep_kernel(const LineParam *__restrict__ lp, int nlines, c
     }
 }
 
-// cze_pl of slot t of a line (tube.f90:565,578,590)
-__device__ __forceinline__ double cze_pl_at(const double *cze_line, int np, int t)
-{
-    if (t < np) return cze_line[t];
-    if (t == np) return dev_pi2();
-    return dev_pi2() + cze_line[1];
-}
 
 // ------------------------------------------------------------------ a3/a5: sections
 // One warp per section slot (n_sec + 1 slots per line; slot n_sec is the periodic copy).
@@ -311,16 +304,6 @@ __global__ void sample_kernel(const LineParam *__restrict__ lp, const int *__res
     }
 }
 
-__device__ __forceinline__ void cminus3(const double *r, const double *l, double *d)
-{
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        double v = r[k] - l[k];
-        if (v > dev_pi()) v = v - dev_pi2();
-        if (v < -dev_pi()) v = v + dev_pi2();
-        d[k] = v;
-    }
-}
 
 // ------------------------------------------------------------------ chords
 // One warp per real section; tci(t, t_j) for t_j = 0..ntf; t_j = ntf uses the first
@@ -421,17 +404,6 @@ __global__ void subseg_kernel(const LineParam *__restrict__ lp, const int *__res
 // Extended samples of section t: ci_j (j < ntf) on the spline, ci_ntf = node t+1 (the endpoint
 // copy, tube.f90:721-723) and ci_{ntf+1} = the first sample of section t+1, so that
 // chord_j = cminus(ci_{j+1}, ci_j) covers j = 0..ntf (tube.f90:740-751).
-__device__ __forceinline__ void spl_pos_fma(const double *__restrict__ a6, double z, double *c3)
-{
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const double *a = a6 + 6 * d;
-        double v = fma(fma(fma(fma(fma(a[5], z, a[4]), z, a[3]), z, a[2]), z, a[1]), z, a[0]);
-        if (v >= dev_pi()) v = v - dev_pi2();
-        if (v < -dev_pi()) v = v + dev_pi2();
-        c3[d] = v;
-    }
-}
 
 // slot of every sub-segment of the batch (one warp per section)
 __global__ void subseg_map_kernel(const LineParam *__restrict__ lp, const int *__restrict__ slot_line, int64_t nslots,
@@ -651,7 +623,7 @@ int scan_exclusive_i64(Ctx *c, int64_t *d_data, int64_t n, int64_t *d_total, Dev
 }
 
 // ------------------------------------------------------------------ driver
-int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B)
+int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mode)
 {
     // la..lb-1: 0-based lines of this batch
     const int nl = lb - la;
@@ -751,9 +723,10 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B)
     FWT_CUDA(cudaMemcpyAsync(B.soff + slots, &B.nsamples, sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
     FWT_CUDA(cudaMemcpyAsync(B.qoff + slots, &B.nsub, sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
 
+    if (mode == BatchRecords::Pieces) return piece_setup(c, B);
     // the tile-owned FP32 kernel reads compact FP32 records built by one fused kernel; the box
     // walk reads FP64 records built from sample arrays
-    const bool tile_mode = c->p.precision == 32 && c->p.deposit_mode == 0;
+    const bool tile_mode = mode == BatchRecords::SubSeg;
     const size_t rec_bytes = tile_mode ? sizeof(SegRec) : sizeof(SubSeg);
     FWT_TRY(buf_reserve(c, C.scratch[18], rec_bytes * (size_t)std::max<int64_t>(B.nsub, 1)));
     if (tile_mode) {

@@ -11,6 +11,9 @@
 // FP32 arithmetic is done in a frame local to the sub-segment start ci0: grid-point offsets
 // x - ci0, and the spline re-expanded around the start, c(z0 + W) - c(z0) = sum_k b_k W^k
 // (Taylor shift of the quintic in FP64), so no FP32 quantity carries the absolute position.
+#include <cstdio>
+#include <cstdlib>
+
 #include "k_deposit.cuh"
 
 namespace fwt {
@@ -220,9 +223,18 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
     FWT_CUDA(cudaMemsetAsync(d_acc, 0, sizeof(unsigned long long), c->stream));
     int64_t sections = 0, subsegs = 0, pairs = 0;
     const int64_t cap = batch_node_cap(c);
+    const bool tile_path = c->p.precision == 32 && c->p.deposit_mode == 0;
+    const double dxg = kPi2 / c->p.N;
+    // FWT_PIECE_RT_CELLS overrides the piece kernel's radius limit (in grid spacings)
+    const char *env = std::getenv("FWT_PIECE_RT_CELLS");
+    const double rt_cells = env ? std::atof(env) : kPieceMaxRtCells;
+    auto thin = [&](int l) {
+        return tile_path && c->p.Rtube_ratio * c->p.sigma_ratio * c->sigma[l] <= rt_cells * dxg;
+    };
     int la = line_s - 1;
     while (la < line_e) {
-        // batch: consecutive lines up to the node cap, ending after a filtered line
+        // batch: consecutive lines up to the node cap, ending after a filtered line and where
+        // the lines change between the sub-segment and the piece kernel
         int lb = la;
         int64_t nodes = 0;
         while (lb < line_e) {
@@ -230,13 +242,18 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
             ++lb;
             if (c->if_filter[lb - 1]) break;
             if (lb < line_e && nodes + c->npoint[lb] > cap) break;
+            if (lb < line_e && thin(lb) != thin(la)) break;
         }
+        const BatchRecords mode =
+            !tile_path ? BatchRecords::Walk : (thin(la) ? BatchRecords::Pieces : BatchRecords::SubSeg);
+        if (std::getenv("FWT_SYNC_CHECK"))
+            std::fprintf(stderr, "libfwt: batch lines %d..%d records %d\n", la + 1, lb, (int)mode);
         CenterlineBatch B;
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, c->stream);
-        const int rc_setup = centerline_setup(c, la, lb, B);
+        const int rc_setup = centerline_setup(c, la, lb, B, mode);
         cudaEventRecord(e1, c->stream);
         cudaEventSynchronize(e1);
         float ms_setup = 0;
@@ -252,11 +269,12 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
         }
         sections += B.nslots - B.nl;
         subsegs += B.nsub;
-        if (c->p.deposit_mode == 1 || c->p.precision == 64) {
+        if (mode == BatchRecords::Walk) {
             FWT_TRY(launch_walk(c, B, d_acc));
         } else {
             int64_t np_ = 0;
-            FWT_TRY(launch_tile(c, B, &np_));
+            if (mode == BatchRecords::Pieces) FWT_TRY(launch_piece(c, B, &np_));
+            else FWT_TRY(launch_tile(c, B, &np_));
             pairs += np_;
         }
         if (c->if_filter[lb - 1]) {

@@ -280,30 +280,62 @@ __device__ __forceinline__ void segf_from(const SegRec &R, int di, int dj, int d
     G.eta = R.eta;
 }
 
-// The predicate and vorticity of point_f32 evaluated straight from a record, for the grid
-// point at offset d = x - ci0 (tube.f90:806-892 in the local frame).
-template <bool General, typename RecT>
-__device__ __forceinline__ bool point_rec(const RecT &R, float d0x, float d0y, float d0z, float out[3])
+// The three acceptance tests of tube.f90:806-818 for the grid point at offset d = x - ci0 in
+// the record's local frame: t0 >= 0, t1 < 0 and rho^2 < Rtube^2.  The arithmetic is spelled
+// out with explicit fmaf so that every caller (the row filter and the evaluation of the tile
+// kernel) decides a point identically.  t0 is returned for the spline argument.
+template <typename RecT>
+__device__ __forceinline__ bool rec_tests(const RecT &R, float d0x, float d0y, float d0z, float &t0)
 {
-    const float t0 = d0x * R.tc0[0] + d0y * R.tc0[1] + d0z * R.tc0[2];
+    t0 = fmaf(d0z, R.tc0[2], fmaf(d0y, R.tc0[1], d0x * R.tc0[0]));
     if (!(t0 >= 0.0f)) return false;
     const float ex = d0x - R.dci[0], ey = d0y - R.dci[1], ez = d0z - R.dci[2];
-    const float t1 = ex * R.tc1[0] + ey * R.tc1[1] + ez * R.tc1[2];
+    const float t1 = fmaf(ez, R.tc1[2], fmaf(ey, R.tc1[1], ex * R.tc1[0]));
     if (!(t1 < 0.0f)) return false;
-    const float r2 = d0x * d0x + d0y * d0y + d0z * d0z - t0 * t0;
-    if (!(r2 < R.R2)) return false;
-    const float W = t0 * R.g;
-    float P[3], c1[3];
+    const float r2 = fmaf(-t0, t0, fmaf(d0z, d0z, fmaf(d0y, d0y, d0x * d0x)));
+    return r2 < R.R2;
+}
+
+// The vorticity of tube.f90:819-892 for the spline argument W = zb + w, measured from the
+// z0 of a record's Taylor coefficients R.b (c(z0 + W) - c(z0) = sum_k b[k-1] W^k), and the
+// squared truncation radius R2 of the accepting chord.
+//
+// Delta = false: zb = 0 and d = x - c(z0) (up to the record's wrap bookkeeping), so
+// x - c(z) = d - P(W) with P evaluated by Horner.
+// Delta = true: d = x - c(z0 + zb), the offset from the accepting chord's start sample, and
+// x - c(z) = d - (P(zb + w) - P(zb)), the difference taken in the divided-difference form
+// w sum_k b_k D_k, D_k = ((zb + w)^k - zb^k) / w, which keeps its relative accuracy however
+// large zb is.  The wrap decisions still use P(W), which needs no such accuracy: a decision
+// moved by rounding is undone by the final single wrap.
+template <bool General, bool Delta, typename RecT>
+__device__ __forceinline__ void vort_w(const RecT &R, float d0x, float d0y, float d0z, float zb, float w, float R2,
+                                       float out[3])
+{
+    const float W = Delta ? zb + w : w;
+    float P[3], c1[3], Q[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const float *b = R.b + 5 * d;
         P[d] = W * fmaf(W, fmaf(W, fmaf(W, fmaf(W, b[4], b[3]), b[2]), b[1]), b[0]);
         c1[d] = fmaf(W, fmaf(W, fmaf(W, fmaf(W, 5.0f * b[4], 4.0f * b[3]), 3.0f * b[2]), 2.0f * b[1]), b[0]);
     }
+    if constexpr (Delta) {
+        const float u = zb, v = W;
+        const float u2 = u * u, u3 = u2 * u, u4 = u3 * u;
+        const float D2 = v + u, D3 = fmaf(v, D2, u2), D4 = fmaf(v, D3, u3), D5 = fmaf(v, D4, u4);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const float *b = R.b + 5 * d;
+            Q[d] = w * fmaf(b[4], D5, fmaf(b[3], D4, fmaf(b[2], D3, fmaf(b[1], D2, b[0]))));
+        }
+    } else {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Q[d] = P[d];
+    }
     const float d0[3] = {d0x, d0y, d0z};
     float xc[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) xc[d] = d0[d] - P[d];
+    for (int d = 0; d < 3; ++d) xc[d] = d0[d] - Q[d];
     if (R.kq[0] != kNoWrap) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -322,7 +354,6 @@ __device__ __forceinline__ bool point_rec(const RecT &R, float d0x, float d0y, f
         out[0] = tp * T[0];
         out[1] = tp * T[1];
         out[2] = tp * T[2];
-        return true;
     } else {
         float c2[3];
 #pragma unroll
@@ -336,7 +367,7 @@ __device__ __forceinline__ bool point_rec(const RecT &R, float d0x, float d0y, f
         const float sigma = fmaf(R.A, sn + 1.0f, R.smin);
         const float s2 = sigma * sigma;
         const float inv2s2 = 0.5f / s2;
-        const float tp = (expf(-rho2 * inv2s2) - expf(-R.R2 * inv2s2)) * (0.159154943f / s2) * R.Gamma;
+        const float tp = (expf(-rho2 * inv2s2) - expf(-R2 * inv2s2)) * (0.159154943f / s2) * R.Gamma;
         const float dsds = R.q * cs * in1 * R.Linv;
         const float rho = sqrtf(rho2);
         const float X[3] = {c1[1] * c2[2] - c1[2] * c2[1], c1[2] * c2[0] - c1[0] * c2[2], c1[0] * c2[1] - c1[1] * c2[0]};
@@ -362,11 +393,34 @@ __device__ __forceinline__ bool point_rec(const RecT &R, float d0x, float d0y, f
             for (int d = 0; d < 3; ++d)
                 out[d] = tp * (T[d] + R.eta * (t5 * Nv[d] + t6 * B[d]) + (t7 * Nv[d] + t8 * B[d]));
         }
-        return true;
     }
+}
+
+// The vorticity of tube.f90:819-892 for a point that passed rec_tests with argument t0
+// (sub-segment record: W = t0 g).
+template <bool General, typename RecT>
+__device__ __forceinline__ void rec_vorticity(const RecT &R, float d0x, float d0y, float d0z, float t0, float out[3])
+{
+    vort_w<General, false>(R, d0x, d0y, d0z, 0.0f, t0 * R.g, R.R2, out);
+}
+
+// Predicate and vorticity together (tube.f90:806-892 in the local frame).
+template <bool General, typename RecT>
+__device__ __forceinline__ bool point_rec(const RecT &R, float d0x, float d0y, float d0z, float out[3])
+{
+    float t0;
+    if (!rec_tests(R, d0x, d0y, d0z, t0)) return false;
+    rec_vorticity<General>(R, d0x, d0y, d0z, t0, out);
+    return true;
 }
 
 int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc);
 int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out);
+int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out);
+
+// Lines whose truncation radius Rtube_ratio * sigma_max is at most this many grid spacings go
+// through the piece kernel; thicker tubes through the sub-segment kernel, whose analytic
+// row intervals skip most of a large box.
+constexpr double kPieceMaxRtCells = 4.5;
 
 }  // namespace fwt

@@ -17,145 +17,62 @@
 //    the reference walks the whole box (about 11 points per accepted one at these
 //    sub-segment lengths).  The tile is written once with coalesced float4 stores; its
 //    component min/max are folded into the epilogue.
+#include <cstdio>
+#include <cstdlib>
+
 #include "k_deposit.cuh"
+#include "k_tile_common.cuh"
 
 namespace fwt {
-
-constexpr int TX = 16, TY = 8, TZ = 8, TP = TX * TY * TZ;
-constexpr int kCandChunk = 32;   // candidates per chunk (two chunks staged: ~44 KB of shared memory)
-constexpr int kDepThreads = 256;
-constexpr int kMaxRows = kCandChunk * 128;   // a clipped cross-section has at most 16 x 8 rows
-constexpr int kRecVec = (int)(sizeof(SegRec) / 16);
-
-__device__ __forceinline__ int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
-
-__device__ __forceinline__ int axis_entries(int glo, int ghi, int N, int T)
-{
-    int cnt = 0;
-    const int m0 = floordiv(glo, N), m1 = floordiv(ghi, N);
-    for (int m = m0; m <= m1; ++m) {
-        const int a = max(glo, m * N) - m * N, b = min(ghi, m * N + N - 1) - m * N;
-        cnt += b / T - a / T + 1;
-    }
-    return cnt;
-}
 
 // Can the tile's points (unwrapped grid offsets o0..o0+n-1 from the record's box origin) pass
 // t0 >= 0, t1 < 0 and rho < Rtube (tube.f90:806-818)?  Conservative: extremes of the linear
 // tests over the tile's bounding box, and the box's distance to the chord line.
 __device__ __forceinline__ bool tile_may_hit(const SegRec &R, int ox, int oy, int oz, int nx, int ny, int nz)
 {
+    // Every operation is spelled out (fmaf, __fmul_rn, __fadd_rn): the counting and the
+    // emitting kernel of the binning inline this test separately and must decide each tile
+    // identically, which free contraction by the compiler would not guarantee.
     const float dx = R.dx;
-    const float hx = 0.5f * (nx - 1) * dx, hy = 0.5f * (ny - 1) * dx, hz = 0.5f * (nz - 1) * dx;
-    const float cx = fmaf((float)ox, dx, R.off[0]) + hx, cy = fmaf((float)oy, dx, R.off[1]) + hy,
-                cz = fmaf((float)oz, dx, R.off[2]) + hz;
-    const float hn = sqrtf(hx * hx + hy * hy + hz * hz);
+    const float hx = __fmul_rn(0.5f * (float)(nx - 1), dx), hy = __fmul_rn(0.5f * (float)(ny - 1), dx),
+                hz = __fmul_rn(0.5f * (float)(nz - 1), dx);
+    const float cx = __fadd_rn(fmaf((float)ox, dx, R.off[0]), hx), cy = __fadd_rn(fmaf((float)oy, dx, R.off[1]), hy),
+                cz = __fadd_rn(fmaf((float)oz, dx, R.off[2]), hz);
+    const float hn = sqrtf(fmaf(hz, hz, fmaf(hy, hy, __fmul_rn(hx, hx))));
     const float Rt = sqrtf(R.R2);
-    const float e = 1e-3f * (hn + Rt + dx);   // slack for the FP32 rounding of these bounds
-    const float t0c = cx * R.tc0[0] + cy * R.tc0[1] + cz * R.tc0[2];
-    const float t0h = hx * fabsf(R.tc0[0]) + hy * fabsf(R.tc0[1]) + hz * fabsf(R.tc0[2]);
-    if (t0c + t0h < -e) return false;
-    const float t1c = (cx - R.dci[0]) * R.tc1[0] + (cy - R.dci[1]) * R.tc1[1] + (cz - R.dci[2]) * R.tc1[2];
-    const float t1h = hx * fabsf(R.tc1[0]) + hy * fabsf(R.tc1[1]) + hz * fabsf(R.tc1[2]);
-    if (t1c - t1h > e) return false;
-    const float d2 = fmaxf(cx * cx + cy * cy + cz * cz - t0c * t0c, 0.0f);
-    const float rr = Rt + hn + e;
-    return d2 <= rr * rr;
+    const float e = __fmul_rn(1e-3f, __fadd_rn(__fadd_rn(hn, Rt), dx));   // slack for the rounding of the bounds
+    const float t0c = fmaf(cz, R.tc0[2], fmaf(cy, R.tc0[1], __fmul_rn(cx, R.tc0[0])));
+    const float t0h = fmaf(hz, fabsf(R.tc0[2]), fmaf(hy, fabsf(R.tc0[1]), __fmul_rn(hx, fabsf(R.tc0[0]))));
+    if (__fadd_rn(t0c, t0h) < -e) return false;
+    const float t1c = fmaf(__fadd_rn(cz, -R.dci[2]), R.tc1[2],
+                           fmaf(__fadd_rn(cy, -R.dci[1]), R.tc1[1], __fmul_rn(__fadd_rn(cx, -R.dci[0]), R.tc1[0])));
+    const float t1h = fmaf(hz, fabsf(R.tc1[2]), fmaf(hy, fabsf(R.tc1[1]), __fmul_rn(hx, fabsf(R.tc1[0]))));
+    if (__fadd_rn(t1c, -t1h) > e) return false;
+    const float d2 = fmaxf(fmaf(-t0c, t0c, fmaf(cz, cz, fmaf(cy, cy, __fmul_rn(cx, cx)))), 0.0f);
+    const float rr = __fadd_rn(__fadd_rn(Rt, hn), e);
+    return d2 <= __fmul_rn(rr, rr);
 }
 
 // Visit every (tile, image) of record S's box that may hold accepted points.
 template <typename F>
 __device__ __forceinline__ void for_each_tile(const SegRec &S, int N, F &&f)
 {
-    const int glo0 = S.box_lo[0] - 1, ghi0 = S.box_hi[0] - 1;
-    const int glo1 = S.box_lo[1] - 1, ghi1 = S.box_hi[1] - 1;
-    const int glo2 = S.box_lo[2] - 1, ghi2 = S.box_hi[2] - 1;
-    for (int mz = floordiv(glo2, N); mz <= floordiv(ghi2, N); ++mz) {
-        const int az = max(glo2, mz * N) - mz * N, bz = min(ghi2, mz * N + N - 1) - mz * N;
-        for (int tz = az / TZ; tz <= bz / TZ; ++tz) {
-            const int uz0 = max(tz * TZ + mz * N, glo2), uz1 = min(min(tz * TZ + TZ, N) - 1 + mz * N, ghi2);
-            for (int my = floordiv(glo1, N); my <= floordiv(ghi1, N); ++my) {
-                const int ay = max(glo1, my * N) - my * N, by = min(ghi1, my * N + N - 1) - my * N;
-                for (int ty = ay / TY; ty <= by / TY; ++ty) {
-                    const int uy0 = max(ty * TY + my * N, glo1), uy1 = min(min(ty * TY + TY, N) - 1 + my * N, ghi1);
-                    for (int mx = floordiv(glo0, N); mx <= floordiv(ghi0, N); ++mx) {
-                        const int ax = max(glo0, mx * N) - mx * N, bx = min(ghi0, mx * N + N - 1) - mx * N;
-                        for (int tx = ax / TX; tx <= bx / TX; ++tx) {
-                            const int ux0 = max(tx * TX + mx * N, glo0), ux1 = min(min(tx * TX + TX, N) - 1 + mx * N, ghi0);
-                            if (!tile_may_hit(S, ux0 - glo0, uy0 - glo1, uz0 - glo2, ux1 - ux0 + 1, uy1 - uy0 + 1,
-                                              uz1 - uz0 + 1))
-                                continue;
-                            f(tx, ty, tz, (uint32_t)((mx + 1) + 3 * (my + 1) + 9 * (mz + 1)));
-                        }
-                    }
-                }
-            }
-        }
-    }
+    for_each_box_tile(S.box_lo, S.box_hi, N,
+                      [&](int ox, int oy, int oz, int nx, int ny, int nz) {
+                          return tile_may_hit(S, ox, oy, oz, nx, ny, nz);
+                      },
+                      f);
 }
 
-template <typename Rec>
-__global__ void pair_count_kernel(const Rec *__restrict__ seg, int64_t nsub, int N, int64_t *__restrict__ cnt,
-                                  int *__restrict__ err)
-{
-    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nsub) return;
-    const Rec &S = seg[q];
-    int64_t c = 0;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const int glo = S.box_lo[d] - 1, ghi = S.box_hi[d] - 1;
-        if (floordiv(glo, N) < -1 || floordiv(ghi, N) > 1 || ghi < glo) atomicOr(err, 1);
-    }
-    for_each_tile(S, N, [&](int, int, int, uint32_t) { ++c; });
-    cnt[q] = c;
-}
-
-// warp-aggregated increment of tile_cnt[key]: consecutive sub-segments share tiles
-__device__ __forceinline__ void agg_inc(uint32_t *cnt, uint32_t key, bool active)
-{
-    const unsigned act = __ballot_sync(0xffffffffu, active);
-    if (!active) return;
-    const unsigned peers = __match_any_sync(act, key);
-    const int leader = __ffs(peers) - 1;
-    if ((int)(threadIdx.x & 31) == leader) atomicAdd(cnt + key, (uint32_t)__popc(peers));
-}
-
-template <typename Rec>
-__global__ void pair_emit_kernel(const Rec *__restrict__ seg, int64_t nsub, int N, int ntx, int nty,
-                                 const int64_t *__restrict__ off, uint32_t *__restrict__ key,
-                                 uint32_t *__restrict__ val, uint32_t *__restrict__ tile_cnt)
-{
-    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = q < nsub;
-    const Rec &S = seg[live ? q : 0];
-    int64_t o = live ? off[q] : 0;
-    // the first pair of each thread is counted through a warp-aggregated atomic below
-    bool first = true;
-    uint32_t k0 = 0;
-    if (live)
-        for_each_tile(S, N, [&](int tx, int ty, int tz, uint32_t img) {
-            const uint32_t tile = (uint32_t)(tx + ntx * (ty + nty * tz));
-            key[o] = tile;
-            val[o] = (uint32_t)q | (img << 26);
-            ++o;
-            if (first) {
-                first = false;
-                k0 = tile;
-                return;
-            }
-            atomicAdd(tile_cnt + tile, 1u);
-        });
-    agg_inc(tile_cnt, k0, live && !first);
-}
-
+// Counting sort, last step: every emitted pair to its tile's list.  Slots left unfilled by
+// the emitting pass (key kNoTile) are skipped.
 __global__ void tile_scatter_kernel(const uint32_t *__restrict__ key, const uint32_t *__restrict__ val, int64_t n,
                                     const int64_t *__restrict__ tile_off, uint32_t *__restrict__ cursor,
                                     uint32_t *__restrict__ list)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < n;
-    const uint32_t t = live ? key[i] : 0u;
+    const uint32_t t = i < n ? key[i] : kNoTile;
+    const bool live = t != kNoTile;
     // warp-aggregated cursor: lanes with the same tile take consecutive slots
     const unsigned act = __ballot_sync(0xffffffffu, live);
     if (!live) return;
@@ -187,42 +104,9 @@ struct CandBox {
     float q2;       // dx^2 (1 - tc0[axis]^2), 0 when the cylinder bound is not used
     float i2q;      // 1 / (2 q2)
     float rnb;      // (1 + 1e-6) / n[(axis+1)%3]: row -> (jb, jc) without an integer divide
+    int dl[3];      // dorg - lo: tile-local coordinate -> grid offset from the record's box_lo
+    int pad;
 };
-
-__device__ __forceinline__ void bulk_copy_g2s(void *smem, const void *gmem, uint32_t bytes, uint64_t *bar)
-{
-    // 1-D bulk asynchronous copy through the TMA engine, completion on an mbarrier
-    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
-    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(s),
-                 "l"(gmem), "r"(bytes), "r"(b)
-                 : "memory");
-}
-
-// Wait for the mbarrier phase with a bounded spin; returns false if it ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase)
-{
-    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
-    for (int it = 0; it < (1 << 22); ++it) {
-        uint32_t done;
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(b), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // Index interval [ilo, ihi] (clamped to [0, n-1]) of the grid row d0 + i dx e_a that can pass
 // t0 >= 0, t1 < 0 and rho^2 < R2; a one-point margin covers the FP32 rounding of the bounds.
@@ -276,18 +160,25 @@ __device__ __forceinline__ void clip_box(const SegRec &R, uint32_t img, int N, i
         B.lo[d] = lo - ulo;
         B.n[d] = max(0, hi - lo + 1);
         B.dorg[d] = lo - (R.box_lo[d] - 1);
+        B.dl[d] = B.dorg[d] - B.lo[d];
         nonempty = nonempty && B.n[d] > 0;
     }
     const float ax = fabsf(R.tc0[0]), ay = fabsf(R.tc0[1]), az = fabsf(R.tc0[2]);
-    B.axis = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
-    B.nrows = nonempty ? B.n[(B.axis + 1) % 3] * B.n[(B.axis + 2) % 3] : 0;
-    const float ta = R.tc0[B.axis], tb = R.tc1[B.axis], dx = R.dx;
+    const int a = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+    B.axis = a;
+    // per-axis picks by selects: a runtime index would put B in local memory
+    const int nbv = a == 0 ? B.n[1] : (a == 1 ? B.n[2] : B.n[0]);
+    const int ncv = a == 0 ? B.n[2] : (a == 1 ? B.n[0] : B.n[1]);
+    B.nrows = nonempty ? nbv * ncv : 0;
+    const float ta = a == 0 ? R.tc0[0] : (a == 1 ? R.tc0[1] : R.tc0[2]);
+    const float tb = a == 0 ? R.tc1[0] : (a == 1 ? R.tc1[1] : R.tc1[2]);
+    const float dx = R.dx;
     B.isa = 1.0f / (dx * ta);
     B.isb = fabsf(tb) > 0.05f ? 1.0f / (dx * tb) : 0.0f;
     const float q2 = dx * dx * (1.0f - ta * ta);
     B.q2 = q2 > 0.01f * dx * dx ? q2 : 0.0f;
     B.i2q = B.q2 > 0.0f ? 0.5f / B.q2 : 0.0f;
-    B.rnb = nonempty ? 1.000001f / (float)B.n[(B.axis + 1) % 3] : 0.0f;
+    B.rnb = nonempty ? 1.000001f / (float)nbv : 0.0f;
 }
 
 // Warp-autonomous tile deposition.  Each warp claims chunks of kWarpChunk candidates of the
@@ -296,18 +187,53 @@ __device__ __forceinline__ void clip_box(const SegRec &R, uint32_t img, int N, i
 // grid rows across its lanes, and adds into the CTA's fixed-point accumulators.  Only the
 // accumulator set-up and the epilogue synchronise the whole CTA.
 constexpr int kWarpChunk = 16;
-constexpr int kDepWarps = kDepThreads / 32;
+constexpr int kQueue = 64;       // accepted-point queue of a warp (< 32 left over + 32 new)
 struct WarpStage {
     SegRec rec[kWarpChunk];
     CandBox box[kWarpChunk];
+    uint32_t q[kQueue];         // accepted points: candidate | x << 4 | y << 8 | z << 11 (tile-local)
     uint64_t bar;
     uint64_t pad;
 };
-// Accumulator cell of tile point (x, y, z): x + kSY y + kSZ z.  A warp's lanes take adjacent
-// rows, so along a y- or z-walk they hit cells kSY or kSZ apart; with both strides odd in
-// 8-byte words the lanes spread over all shared-memory banks.
-constexpr int kSY = TX + 1, kSZ = kSY * TY + 1, kAccN = kSZ * TZ;
-constexpr size_t kDepSmem = sizeof(long long) * 3 * kAccN + sizeof(WarpStage) * kDepWarps;
+constexpr size_t kDepSmem = kAccBytes + sizeof(WarpStage) * kDepWarps;
+
+// Evaluate the first `cnt` queued points of the warp, one per lane (rec_tests again for t0,
+// then the vorticity), add them into the tile's fixed-point cells and drop them from the queue.
+template <bool General>
+__device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN], int lane, int cnt, int &qn,
+                                            float fscale, float fmaxq, int *__restrict__ err)
+{
+    if (lane < cnt) {
+        const uint32_t e = S.q[lane];
+        const int k = (int)(e & 15u);
+        const int lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)(e >> 11);
+        const CandBox &B = S.box[k];
+        const SegRec &R = S.rec[k];
+        const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
+        const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
+        const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
+        float t0, vv[3];
+        rec_tests(R, d0x, d0y, d0z, t0);
+        rec_vorticity<General>(R, d0x, d0y, d0z, t0, vv);
+        const int p = lx + kSY * ly + kSZ * lz;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            float sv = vv[d] * fscale;
+            if (!(fabsf(sv) < fmaxq)) {
+                atomicOr(err, 4);
+                sv = sv != sv ? 0.0f : copysignf(fmaxq, sv);
+            }
+            atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(sv));
+        }
+    }
+    __syncwarp();
+    const int rem = qn - cnt;
+    const uint32_t keep = lane < rem ? S.q[cnt + lane] : 0u;
+    __syncwarp();
+    if (lane < rem) S.q[lane] = keep;
+    __syncwarp();
+    qn = rem;
+}
 
 template <bool General, bool Accumulate>
 __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
@@ -321,27 +247,9 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
     const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
     const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    WarpStage &S = reinterpret_cast<WarpStage *>(dsm + sizeof(long long) * 3 * kAccN)[warp];
-    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&S.bar);
-    if (lane == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    for (int p = tid; p < TP; p += kDepThreads) {
-        const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
-        const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
-        long long a0 = 0, a1 = 0, a2 = 0;
-        if (Accumulate && gx < N && gy < N && gz < N) {
-            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
-            a0 = __double2ll_rn((double)wx[g] * scale);
-            a1 = __double2ll_rn((double)wy[g] * scale);
-            a2 = __double2ll_rn((double)wz[g] * scale);
-        }
-        const int pa = lx + kSY * ly + kSZ * lz;
-        acc[0][pa] = a0;
-        acc[1][pa] = a1;
-        acc[2][pa] = a2;
-    }
+    WarpStage &S = reinterpret_cast<WarpStage *>(dsm + kAccBytes)[warp];
+    if (lane == 0) mbar_init(&S.bar);
+    tile_acc_init<Accumulate>(acc, N, x0, y0, z0, scale, wx, wy, wz);
     __syncthreads();
     const int64_t c0 = tile_off[tile], c1 = tile_off[tile + 1];
     const int nchunks = (int)((c1 - c0 + kWarpChunk - 1) / kWarpChunk);
@@ -349,24 +257,15 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
     const float fmaxq = 4.0e18f;
     uint32_t phase = 0;
     bool failed = false;
+    int qn = 0;   // queued points of this warp (warp-uniform)
     for (int ch = warp; ch < nchunks && !failed; ch += kDepWarps) {
         const int64_t base = c0 + (int64_t)ch * kWarpChunk;
         const int nc = (c1 - base < kWarpChunk) ? (int)(c1 - base) : kWarpChunk;
         const uint32_t v = lane < nc ? __ldg(list + base + lane) : 0u;
         // stage the records: expect nc * sizeof(SegRec) bytes, then one bulk copy per record
-        if (lane == 0)
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                         "r"((uint32_t)(nc * sizeof(SegRec)))
-                         : "memory");
+        if (lane == 0) mbar_expect(&S.bar, (uint32_t)(nc * sizeof(SegRec)));
         __syncwarp();
-        if (lane < nc) {
-            const uint32_t q = v & ((1u << 26) - 1u);
-            const uint32_t s = (uint32_t)__cvta_generic_to_shared(&S.rec[lane]);
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(s),
-                "l"(rec + q), "r"((uint32_t)sizeof(SegRec)), "r"(bar)
-                : "memory");
-        }
+        if (lane < nc) bulk_g2s(&S.rec[lane], rec + (v & ((1u << 26) - 1u)), (uint32_t)sizeof(SegRec), &S.bar);
         if (!mbar_wait(&S.bar, phase)) {
             failed = true;
             break;
@@ -389,6 +288,9 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
         const int rowoff = incl - nrows;
         const int total = __shfl_sync(0xffffffffu, incl, kWarpChunk - 1);
         __syncwarp();
+        // Rows, one per lane: solve the row's index interval, test its points (rec_tests) in
+        // lock step and queue the accepted ones; every 32 queued points are evaluated with
+        // all lanes busy.
         for (int r0 = 0; r0 < total; r0 += 32) {
             const int r = r0 + lane;
             // candidate of row r: last k with rowoff_k <= r (binary search over the lanes)
@@ -400,96 +302,58 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
                 if (t < nc && ot <= r) k = t;
             }
             const int rk = __shfl_sync(0xffffffffu, rowoff, k);
-            if (r >= total) continue;
-            const CandBox &B = S.box[k];
-            const SegRec &R = S.rec[k];
-            const int a = B.axis;
-            const int rr = r - rk;
-            // rows run over (b, c) = ((a+1)%3, (a+2)%3); per-axis offsets by selects (no
-            // runtime-indexed local arrays)
-            const int nb = a == 0 ? B.n[1] : (a == 1 ? B.n[2] : B.n[0]);
-            const int jc = (int)((float)rr * B.rnb), jb = rr - jc * nb;
-            const int ex = a == 0 ? 0 : (a == 1 ? jc : jb);
-            const int ey = a == 0 ? jb : (a == 1 ? 0 : jc);
-            const int ez = a == 0 ? jc : (a == 1 ? jb : 0);
-            const float d0x = fmaf((float)(B.dorg[0] + ex), R.dx, R.off[0]);
-            const float d0y = fmaf((float)(B.dorg[1] + ey), R.dx, R.off[1]);
-            const float d0z = fmaf((float)(B.dorg[2] + ez), R.dx, R.off[2]);
-            const int na = a == 0 ? B.n[0] : (a == 1 ? B.n[1] : B.n[2]);
-            int ilo, ihi;
-            row_interval(R, B, d0x, d0y, d0z, a, na, ilo, ihi);
-            const int pstride = a == 0 ? 1 : (a == 1 ? kSY : kSZ);
-            const int p0 = (B.lo[0] + ex) + kSY * (B.lo[1] + ey) + kSZ * (B.lo[2] + ez);
-            const float sx = a == 0 ? R.dx : 0.f, sy = a == 1 ? R.dx : 0.f, sz = a == 2 ? R.dx : 0.f;
-            for (int ii = ilo; ii <= ihi; ++ii) {
-                float vv[3];
-                const float fi = (float)ii;
-                if (!point_rec<General>(R, fmaf(fi, sx, d0x), fmaf(fi, sy, d0y), fmaf(fi, sz, d0z), vv)) continue;
-                const int p = p0 + ii * pstride;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    float s = vv[d] * fscale;
-                    if (!(fabsf(s) < fmaxq)) {
-                        atomicOr(err, 4);
-                        s = s != s ? 0.0f : copysignf(fmaxq, s);
-                    }
-                    atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(s));
+            int i = 1, ihi = 0;
+            int a = 0, lb0 = 0, lb1 = 0, lb2 = 0;
+            if (r < total) {
+                const CandBox &B = S.box[k];
+                const SegRec &R = S.rec[k];
+                a = B.axis;
+                const int rr = r - rk;
+                // rows run over (b, c) = ((a+1)%3, (a+2)%3); per-axis offsets by selects
+                const int nb = a == 0 ? B.n[1] : (a == 1 ? B.n[2] : B.n[0]);
+                const int jc = (int)((float)rr * B.rnb), jb = rr - jc * nb;
+                const int ex = a == 0 ? 0 : (a == 1 ? jc : jb);
+                const int ey = a == 0 ? jb : (a == 1 ? 0 : jc);
+                const int ez = a == 0 ? jc : (a == 1 ? jb : 0);
+                lb0 = B.lo[0] + ex;
+                lb1 = B.lo[1] + ey;
+                lb2 = B.lo[2] + ez;
+                const float d0x = fmaf((float)(B.dorg[0] + ex), R.dx, R.off[0]);
+                const float d0y = fmaf((float)(B.dorg[1] + ey), R.dx, R.off[1]);
+                const float d0z = fmaf((float)(B.dorg[2] + ez), R.dx, R.off[2]);
+                const int na = a == 0 ? B.n[0] : (a == 1 ? B.n[1] : B.n[2]);
+                int ilo;
+                row_interval(R, B, d0x, d0y, d0z, a, na, ilo, ihi);
+                i = ilo;
+            }
+            while (__any_sync(0xffffffffu, i <= ihi)) {
+                bool ok = false;
+                uint32_t code = 0;
+                if (i <= ihi) {
+                    const CandBox &B = S.box[k];
+                    const SegRec &R = S.rec[k];
+                    const int lx = lb0 + (a == 0 ? i : 0), ly = lb1 + (a == 1 ? i : 0), lz = lb2 + (a == 2 ? i : 0);
+                    const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
+                    const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
+                    const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
+                    float t0;
+                    ok = rec_tests(R, d0x, d0y, d0z, t0);
+                    code = (uint32_t)k | ((uint32_t)lx << 4) | ((uint32_t)ly << 8) | ((uint32_t)lz << 11);
+                    ++i;
                 }
+                const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                if (ok) S.q[qn + __popc(bal & ((1u << lane) - 1u))] = code;
+                qn += __popc(bal);
+                __syncwarp();
+                if (qn >= 32) drain_queue<General>(S, acc, lane, 32, qn, fscale, fmaxq, err);
             }
         }
+        if (qn > 0) drain_queue<General>(S, acc, lane, qn, qn, fscale, fmaxq, err);
         __syncwarp();   // the warp's stage is reused by its next chunk
     }
     if (failed && lane == 0) atomicOr(err, 2);
     __syncthreads();
-    // epilogue: fixed point -> float, coalesced float4 stores, tile min/max per component
-    const double inv = 1.0 / scale;
-    float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, mx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
-    const bool full = (x0 + TX <= N) && (y0 + TY <= N) && (z0 + TZ <= N);
-    float *w[3] = {wx, wy, wz};
-    if (full) {
-        for (int q4 = tid; q4 < TP / 4; q4 += kDepThreads) {
-            const int p = 4 * q4;
-            const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
-            const size_t g = (size_t)(x0 + lx) + (size_t)N * ((size_t)(y0 + ly) + (size_t)N * (z0 + lz));
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                float4 v4;
-                const int pa = lx + kSY * ly + kSZ * lz;
-                v4.x = (float)((double)acc[d][pa] * inv);
-                v4.y = (float)((double)acc[d][pa + 1] * inv);
-                v4.z = (float)((double)acc[d][pa + 2] * inv);
-                v4.w = (float)((double)acc[d][pa + 3] * inv);
-                *reinterpret_cast<float4 *>(w[d] + g) = v4;
-                mn[d] = fminf(mn[d], fminf(fminf(v4.x, v4.y), fminf(v4.z, v4.w)));
-                mx[d] = fmaxf(mx[d], fmaxf(fmaxf(v4.x, v4.y), fmaxf(v4.z, v4.w)));
-            }
-        }
-    } else {
-        for (int p = tid; p < TP; p += kDepThreads) {
-            const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
-            const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
-            if (gx >= N || gy >= N || gz >= N) continue;
-            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const float v1 = (float)((double)acc[d][lx + kSY * ly + kSZ * lz] * inv);
-                w[d][g] = v1;
-                mn[d] = fminf(mn[d], v1);
-                mx[d] = fmaxf(mx[d], v1);
-            }
-        }
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        for (int o2 = 16; o2 > 0; o2 >>= 1) {
-            mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o2));
-            mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o2));
-        }
-        if (lane == 0) {
-            atomicMin(mm + 2 * d, f2ord(mn[d]));
-            atomicMax(mm + 2 * d + 1, f2ord(mx[d]));
-        }
-    }
+    tile_epilogue(acc, N, x0, y0, z0, scale, wx, wy, wz, mm);
 }
 
 
@@ -559,6 +423,13 @@ int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     kt_end(c, km);
     c->launches += 5;
     FWT_CUDA(cudaGetLastError());
+    if (std::getenv("FWT_SYNC_CHECK")) {
+        int64_t emitted = 0;
+        FWT_CUDA(cudaMemcpyAsync(&emitted, d_toff + ntiles, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+        FWT_CUDA(cudaStreamSynchronize(c->stream));
+        if (emitted != npairs)
+            std::fprintf(stderr, "libfwt: binning emitted %lld of %lld pairs\n", (long long)emitted, (long long)npairs);
+    }
 
     const size_t n3 = field_elems(c);
     float *w = (float *)c->b_w.p;

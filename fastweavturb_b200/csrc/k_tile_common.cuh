@@ -1,0 +1,253 @@
+// k_tile_common.cuh -- pieces shared by the tile-owned deposition kernels: the tile shape, the
+// periodic tile walk of a record's box, the binning kernels, warp-aggregated counters, bulk
+// asynchronous copies with bounded mbarrier waits, and the tile's int64 fixed-point
+// accumulator (set-up and the coalesced epilogue).
+#pragma once
+
+#include "k_common.cuh"
+
+namespace fwt {
+
+constexpr int TX = 16, TY = 8, TZ = 8, TP = TX * TY * TZ;
+constexpr int kDepThreads = 256;
+constexpr int kDepWarps = kDepThreads / 32;
+
+// Accumulator cell of tile point (x, y, z): x + kSY y + kSZ z.  Lanes working on adjacent
+// rows hit cells kSY or kSZ apart; with both strides odd in 8-byte words the lanes spread
+// over all shared-memory banks.
+constexpr int kSY = TX + 1, kSZ = kSY * TY + 1, kAccN = kSZ * TZ;
+constexpr size_t kAccBytes = sizeof(long long) * 3 * kAccN;
+
+__device__ __forceinline__ int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// Visit every (tile, periodic image) that the box [box_lo, box_hi] (1-based, unwrapped grid
+// indices, at most one period beyond the domain on either side) overlaps and that `cull`
+// does not rule out.  cull(ox, oy, oz, nx, ny, nz) receives the clipped part as offsets from
+// box_lo and extents; f(tx, ty, tz, image) receives the tile and the image code
+// (mx+1) + 3 (my+1) + 9 (mz+1).
+template <typename C, typename F>
+__device__ __forceinline__ void for_each_box_tile(const int *box_lo, const int *box_hi, int N, C &&cull, F &&f)
+{
+    const int glo0 = box_lo[0] - 1, ghi0 = box_hi[0] - 1;
+    const int glo1 = box_lo[1] - 1, ghi1 = box_hi[1] - 1;
+    const int glo2 = box_lo[2] - 1, ghi2 = box_hi[2] - 1;
+    for (int mz = floordiv(glo2, N); mz <= floordiv(ghi2, N); ++mz) {
+        const int az = max(glo2, mz * N) - mz * N, bz = min(ghi2, mz * N + N - 1) - mz * N;
+        for (int tz = az / TZ; tz <= bz / TZ; ++tz) {
+            const int uz0 = max(tz * TZ + mz * N, glo2), uz1 = min(min(tz * TZ + TZ, N) - 1 + mz * N, ghi2);
+            for (int my = floordiv(glo1, N); my <= floordiv(ghi1, N); ++my) {
+                const int ay = max(glo1, my * N) - my * N, by = min(ghi1, my * N + N - 1) - my * N;
+                for (int ty = ay / TY; ty <= by / TY; ++ty) {
+                    const int uy0 = max(ty * TY + my * N, glo1), uy1 = min(min(ty * TY + TY, N) - 1 + my * N, ghi1);
+                    for (int mx = floordiv(glo0, N); mx <= floordiv(ghi0, N); ++mx) {
+                        const int ax = max(glo0, mx * N) - mx * N, bx = min(ghi0, mx * N + N - 1) - mx * N;
+                        for (int tx = ax / TX; tx <= bx / TX; ++tx) {
+                            const int ux0 = max(tx * TX + mx * N, glo0), ux1 = min(min(tx * TX + TX, N) - 1 + mx * N, ghi0);
+                            if (!cull(ux0 - glo0, uy0 - glo1, uz0 - glo2, ux1 - ux0 + 1, uy1 - uy0 + 1, uz1 - uz0 + 1))
+                                continue;
+                            f(tx, ty, tz, (uint32_t)((mx + 1) + 3 * (my + 1) + 9 * (mz + 1)));
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+// warp-aggregated increment of cnt[key]: consecutive records share tiles
+__device__ __forceinline__ void agg_inc(uint32_t *cnt, uint32_t key, bool active)
+{
+    const unsigned act = __ballot_sync(0xffffffffu, active);
+    if (!active) return;
+    const unsigned peers = __match_any_sync(act, key);
+    const int leader = __ffs(peers) - 1;
+    if ((int)(threadIdx.x & 31) == leader) atomicAdd(cnt + key, (uint32_t)__popc(peers));
+}
+
+// Binning, step 1: number of (tile, image) pairs of every record (for_each_tile is overloaded
+// per record type).  Boxes wider than one period beyond the domain set err bit 1.
+template <typename Rec>
+__global__ void pair_count_kernel(const Rec *__restrict__ seg, int64_t nsub, int N, int64_t *__restrict__ cnt,
+                                  int *__restrict__ err)
+{
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nsub) return;
+    const Rec &S = seg[q];
+    int64_t c = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int glo = S.box_lo[d] - 1, ghi = S.box_hi[d] - 1;
+        if (floordiv(glo, N) < -1 || floordiv(ghi, N) > 1 || ghi < glo) atomicOr(err, 1);
+    }
+    for_each_tile(S, N, [&](int, int, int, uint32_t) { ++c; });
+    cnt[q] = c;
+}
+
+constexpr uint32_t kNoTile = 0xffffffffu;   // key of a pair slot that the emitting pass left empty
+
+// Binning, step 2: the (tile, record | image << 26) pairs at the record's offset, and the
+// per-tile counts (warp-aggregated for the first tile of each record).  The pass writes only
+// inside the record's slots [off[q], off[q+1]) reserved by step 1 and marks any slot it leaves
+// empty, so the sort stays in bounds even if the two passes ever decided a tile differently.
+template <typename Rec>
+__global__ void pair_emit_kernel(const Rec *__restrict__ seg, int64_t nsub, int N, int ntx, int nty,
+                                 const int64_t *__restrict__ off, uint32_t *__restrict__ key,
+                                 uint32_t *__restrict__ val, uint32_t *__restrict__ tile_cnt)
+{
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = q < nsub;
+    const Rec &S = seg[live ? q : 0];
+    int64_t o = live ? off[q] : 0;
+    const int64_t end = live ? off[q + 1] : 0;
+    // the first pair of each thread is counted through a warp-aggregated atomic below
+    bool first = true;
+    uint32_t k0 = 0;
+    if (live)
+        for_each_tile(S, N, [&](int tx, int ty, int tz, uint32_t img) {
+            if (o >= end) return;
+            const uint32_t tile = (uint32_t)(tx + ntx * (ty + nty * tz));
+            key[o] = tile;
+            val[o] = (uint32_t)q | (img << 26);
+            ++o;
+            if (first) {
+                first = false;
+                k0 = tile;
+                return;
+            }
+            atomicAdd(tile_cnt + tile, 1u);
+        });
+    for (; o < end; ++o) key[o] = kNoTile;
+    agg_inc(tile_cnt, k0, live && !first);
+}
+
+// Wait for the mbarrier phase with a bounded spin; returns false if it ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t phase)
+{
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(b), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar)
+{
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes)
+{
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
+}
+
+// 1-D bulk asynchronous copy (TMA engine) of `bytes` (a multiple of 16, both addresses 16-byte
+// aligned) from global to this CTA's shared memory, completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(void *smem, const void *gmem, uint32_t bytes, uint64_t *bar)
+{
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(s),
+                 "l"(gmem), "r"(bytes), "r"(b)
+                 : "memory");
+}
+
+// Load the tile's current values into the fixed-point cells (Accumulate) or zero them.
+template <bool Accumulate>
+__device__ __forceinline__ void tile_acc_init(long long (*acc)[kAccN], int N, int x0, int y0, int z0, double scale,
+                                              const float *__restrict__ wx, const float *__restrict__ wy,
+                                              const float *__restrict__ wz)
+{
+    for (int p = threadIdx.x; p < TP; p += blockDim.x) {
+        const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
+        const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
+        long long a0 = 0, a1 = 0, a2 = 0;
+        if (Accumulate && gx < N && gy < N && gz < N) {
+            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
+            a0 = __double2ll_rn((double)wx[g] * scale);
+            a1 = __double2ll_rn((double)wy[g] * scale);
+            a2 = __double2ll_rn((double)wz[g] * scale);
+        }
+        const int pa = lx + kSY * ly + kSZ * lz;
+        acc[0][pa] = a0;
+        acc[1][pa] = a1;
+        acc[2][pa] = a2;
+    }
+}
+
+// Fixed point -> float, coalesced float4 stores of the tile, component min/max folded in.
+__device__ __forceinline__ void tile_epilogue(long long (*acc)[kAccN], int N, int x0, int y0, int z0, double scale,
+                                              float *__restrict__ wx, float *__restrict__ wy, float *__restrict__ wz,
+                                              uint32_t *__restrict__ mm)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    const double inv = 1.0 / scale;
+    float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, mx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    const bool full = (x0 + TX <= N) && (y0 + TY <= N) && (z0 + TZ <= N);
+    if (full) {
+        for (int q4 = tid; q4 < TP / 4; q4 += blockDim.x) {
+            const int p = 4 * q4;
+            const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
+            const size_t g = (size_t)(x0 + lx) + (size_t)N * ((size_t)(y0 + ly) + (size_t)N * (z0 + lz));
+            const int pa = lx + kSY * ly + kSZ * lz;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                float4 v4;
+                v4.x = (float)((double)acc[d][pa] * inv);
+                v4.y = (float)((double)acc[d][pa + 1] * inv);
+                v4.z = (float)((double)acc[d][pa + 2] * inv);
+                v4.w = (float)((double)acc[d][pa + 3] * inv);
+                float *w = d == 0 ? wx : (d == 1 ? wy : wz);
+                *reinterpret_cast<float4 *>(w + g) = v4;
+                mn[d] = fminf(mn[d], fminf(fminf(v4.x, v4.y), fminf(v4.z, v4.w)));
+                mx[d] = fmaxf(mx[d], fmaxf(fmaxf(v4.x, v4.y), fmaxf(v4.z, v4.w)));
+            }
+        }
+    } else {
+        for (int p = tid; p < TP; p += blockDim.x) {
+            const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
+            const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
+            if (gx >= N || gy >= N || gz >= N) continue;
+            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float v1 = (float)((double)acc[d][lx + kSY * ly + kSZ * lz] * inv);
+                float *w = d == 0 ? wx : (d == 1 ? wy : wz);
+                w[g] = v1;
+                mn[d] = fminf(mn[d], v1);
+                mx[d] = fmaxf(mx[d], v1);
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        for (int o2 = 16; o2 > 0; o2 >>= 1) {
+            mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o2));
+            mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o2));
+        }
+        if (lane == 0) {
+            atomicMin(mm + 2 * d, f2ord(mn[d]));
+            atomicMax(mm + 2 * d + 1, f2ord(mx[d]));
+        }
+    }
+}
+
+// Shared kernels of the binning (defined in k_deposit_tile.cu).
+__global__ void tile_scatter_kernel(const uint32_t *__restrict__ key, const uint32_t *__restrict__ val, int64_t n,
+                                    const int64_t *__restrict__ tile_off, uint32_t *__restrict__ cursor,
+                                    uint32_t *__restrict__ list);
+__global__ void u32_to_i64_kernel(const uint32_t *__restrict__ a, int64_t n, int64_t *__restrict__ b);
+__global__ void mm_init_kernel(uint32_t *mm, int n);
+
+// Scale of the int64 fixed-point tile sums for the context's lines.
+double fixed_point_scale(const Ctx *c);
+
+}  // namespace fwt
