@@ -209,6 +209,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--level", type=int, default=None,
                     help="deposit only this scale level of the workload (a bounded case for profiler captures)")
+    ap.add_argument("--lines", type=int, default=None,
+                    help="with --level: keep only the first LINES tubes of that level")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -234,6 +236,9 @@ def main():
     if args.level is not None:
         w.levels = [w.levels[args.level]]
         w.name += f" -- level {args.level} only (profiling case)"
+        if args.lines:
+            w.levels[0].tubes = min(w.levels[0].tubes, args.lines)
+            w.name += f", first {w.levels[0].tubes} lines"
     stream = torch.cuda.current_stream()
     params = F.Params(N=w.N, N_downsample=w.N, line_s=1, line_e=w.ntubes, sigma_ratio=w.sigma_ratio,
                       eta_t=w.eta_t, ntf_times=w.ntf_times, ntf_pre=w.ntf_pre, Rtube_ratio=w.Rtube_ratio,

@@ -110,6 +110,23 @@ __global__ void line_prep_kernel(const LineParam *__restrict__ lp, int nlines, c
 
 
 // ------------------------------------------------------------------ a3/a5: sections
+// |c' x c''| / |c'|^2 of the quintic cf ([coord][6], FP32) at z (tube.f90:633-647)
+__device__ __forceinline__ float turning_integrand(const float *cf, float z)
+{
+    float dc[3], dd[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float *a = cf + 6 * d;
+        dc[d] = fmaf(fmaf(fmaf(fmaf(5.0f * a[5], z, 4.0f * a[4]), z, 3.0f * a[3]), z, 2.0f * a[2]), z, a[1]);
+        dd[d] = fmaf(fmaf(fmaf(20.0f * a[5], z, 12.0f * a[4]), z, 6.0f * a[3]), z, 2.0f * a[2]);
+    }
+    const float x0 = dc[1] * dd[2] - dc[2] * dd[1];
+    const float x1 = dc[2] * dd[0] - dc[0] * dd[2];
+    const float x2 = dc[0] * dd[1] - dc[1] * dd[0];
+    const float ndc2 = dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2];
+    return __fdividef(sqrtf(x0 * x0 + x1 * x1 + x2 * x2), ndc2);
+}
+
 // One warp per section slot (n_sec + 1 slots per line; slot n_sec is the periodic copy).
 __global__ void section_kernel(const LineParam *__restrict__ lp, const int *__restrict__ slot_line, int64_t nslots,
                                const double *__restrict__ X, const double *__restrict__ Y,
@@ -134,64 +151,76 @@ __global__ void section_kernel(const LineParam *__restrict__ lp, const int *__re
     const double zl = cze_pl_at(cz_line, np, t), zr_ = cze_pl_at(cz_line, np, t + 1);
     // spline argument is cze_pl*Len (tube.f90:598)
     const double zr = zr_ * L - zl * L;
-    double coe[18];
-    const double *c[3] = {X + P.node_off, Y + P.node_off, Z + P.node_off};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        // get_spline_5th_coe, subroutine.f90:440-461
-        const double xl = c[d][il], xr = c[d][ir];
+    // lane d < 3 builds coordinate d's coefficients in FP64 (get_spline_5th_coe,
+    // subroutine.f90:440-461); the other lanes get their FP32 copies by shuffles
+    double a6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (lane < 3) {
+        const int d = lane;
+        const double *cd = (d == 0 ? X : (d == 1 ? Y : Z)) + P.node_off;
+        const double xl = cd[il], xr = cd[ir];
         const double vl = ck[3 * (o + il) + d], vr = ck[3 * (o + ir) + d];
         const double al = ckk[3 * (o + il) + d], ar = ckk[3 * (o + ir) + d];
         double xpl = xl, xpr = xr;
         if (xl - xr > dev_pi()) xpr = xr + dev_pi2();
         else if (xl - xr < -dev_pi()) xpl = xl + dev_pi2();
         const double z2 = zr * zr, z3 = z2 * zr, z4 = z3 * zr, z5 = z4 * zr;
-        coe[6 * d + 0] = xl;
-        coe[6 * d + 1] = vl;
-        coe[6 * d + 2] = al / 2.0;
-        coe[6 * d + 3] = (20.0 * (xpr - xpl) - (12.0 * vl + 8.0 * vr) * zr - (3.0 * al - ar) * z2) / (2.0 * z3);
-        coe[6 * d + 4] = (-30.0 * (xpr - xpl) + (16.0 * vl + 14.0 * vr) * zr + (3.0 * al - 2.0 * ar) * z2) / (2.0 * z4);
-        coe[6 * d + 5] = (12.0 * (xpr - xpl) - 6.0 * (vl + vr) * zr - (al - ar) * z2) / (2.0 * z5);
+        a6[0] = xl;
+        a6[1] = vl;
+        a6[2] = al / 2.0;
+        a6[3] = (20.0 * (xpr - xpl) - (12.0 * vl + 8.0 * vr) * zr - (3.0 * al - ar) * z2) / (2.0 * z3);
+        a6[4] = (-30.0 * (xpr - xpl) + (16.0 * vl + 14.0 * vr) * zr + (3.0 * al - 2.0 * ar) * z2) / (2.0 * z4);
+        a6[5] = (12.0 * (xpr - xpl) - 6.0 * (vl + vr) * zr - (al - ar) * z2) / (2.0 * z5);
+#pragma unroll
+        for (int m = 0; m < 6; ++m) coe_out[18 * warp + 6 * d + m] = a6[m];
     }
-    if (lane < 18) coe_out[18 * warp + lane] = coe[lane];
     // turning angle theta = sum |c' x c''| / |c'|^2 * dtf_pre * Len over ntf_pre+1 samples.
-    // The integrand is evaluated in FP32 and summed in FP64; only an FP32 result that falls
-    // near a step of ceil(ntf_times theta / 2 pi) is recomputed exactly in FP64 below.
+    // The integrand is evaluated in FP32 and summed in FP64; a result that falls near a step of
+    // ceil(ntf_times theta / 2 pi) is marked (ntf = 0) and recomputed in FP64 by
+    // section_fp64_kernel, which keeps the FP64 code and its registers out of this loop.
     const double dtfp = (zr_ - zl) / (1.0 * ntf_pre);
-    {
-        float cf[18];
+    float cf[18];
 #pragma unroll
-        for (int k = 0; k < 18; ++k) cf[k] = (float)coe[k];
-        const float zstep = (float)(dtfp * L);
-        float thf = 0.0f;
-        for (int tj = lane; tj <= ntf_pre; tj += 32) {
-            const float z = zstep * (float)tj;
-            float dc[3], dd[3];
+    for (int d = 0; d < 3; ++d)
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const float *a = cf + 6 * d;
-                dc[d] = fmaf(fmaf(fmaf(fmaf(5.0f * a[5], z, 4.0f * a[4]), z, 3.0f * a[3]), z, 2.0f * a[2]), z, a[1]);
-                dd[d] = fmaf(fmaf(fmaf(20.0f * a[5], z, 12.0f * a[4]), z, 6.0f * a[3]), z, 2.0f * a[2]);
-            }
-            const float x0 = dc[1] * dd[2] - dc[2] * dd[1];
-            const float x1 = dc[2] * dd[0] - dc[0] * dd[2];
-            const float x2 = dc[0] * dd[1] - dc[1] * dd[0];
-            const float ndc2 = dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2];
-            thf += __fdividef(sqrtf(x0 * x0 + x1 * x1 + x2 * x2), ndc2);
-        }
-        const double th32 = warp_sum((double)thf) * dtfp * L;
-        const double xr = ntf_times * th32 / dev_pi2();
-        const double fr = xr - floor(xr);
-        const bool near_step = fmin(fr, 1.0 - fr) < 1e-4 * (xr + 1.0) || !(xr == xr);
-        if (!__any_sync(0xffffffffu, near_step)) {
-            if (lane == 0) {
-                const int ntf = (int)ceil(xr) + 1;
-                ntf_out[warp] = ntf;
-                dtf_out[warp] = (zr_ - zl) / (1.0 * ntf);
-            }
-            return;
-        }
+        for (int m = 0; m < 6; ++m) cf[6 * d + m] = __shfl_sync(0xffffffffu, (float)a6[m], d);
+    const float zstep = (float)(dtfp * L);
+    float th0 = 0.0f, th1 = 0.0f;
+    int tj = lane;
+    for (; tj + 32 <= ntf_pre; tj += 64) {   // two independent samples per step
+        th0 += turning_integrand(cf, zstep * (float)tj);
+        th1 += turning_integrand(cf, zstep * (float)(tj + 32));
     }
+    if (tj <= ntf_pre) th0 += turning_integrand(cf, zstep * (float)tj);
+    const double th32 = warp_sum((double)th0 + (double)th1) * dtfp * L;
+    const double xr = ntf_times * th32 / dev_pi2();
+    const double fr = xr - floor(xr);
+    const bool near_step = fmin(fr, 1.0 - fr) < 1e-4 * (xr + 1.0) || !(xr == xr);
+    if (lane == 0) {
+        const int ntf = near_step ? 0 : (int)ceil(xr) + 1;
+        ntf_out[warp] = ntf;
+        dtf_out[warp] = near_step ? 0.0 : (zr_ - zl) / (1.0 * ntf);
+    }
+}
+
+// FP64 turning angle of the sections section_kernel marked (ntf = 0): one warp per slot, the
+// reference's integrand (tube.f90:625-657) in FP64 from the stored coefficients.
+__global__ void section_fp64_kernel(const LineParam *__restrict__ lp, const int *__restrict__ slot_line,
+                                    int64_t nslots, const double *__restrict__ cze, const double *__restrict__ Len,
+                                    int64_t node_base, int ntf_times, int ntf_pre, const double *__restrict__ coe_all,
+                                    int *__restrict__ ntf_out, double *__restrict__ dtf_out)
+{
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= nslots || ntf_out[warp] != 0) return;
+    const int l = slot_line[warp];
+    const LineParam P = lp[l];
+    const int t = (int)(warp - P.slot_off);
+    const int np = P.n_sec;
+    const double L = Len[l];
+    const double *cz_line = cze + (P.node_off - node_base);
+    const double zl = cze_pl_at(cz_line, np, t), zr_ = cze_pl_at(cz_line, np, t + 1);
+    const double dtfp = (zr_ - zl) / (1.0 * ntf_pre);
+    const double *coe = coe_all + 18 * (size_t)warp;
     double th = 0.0;
     for (int tj = lane; tj <= ntf_pre; tj += 32) {
         const double s = zl + dtfp * tj;
@@ -693,6 +722,9 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mo
     section_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, c->d_x, c->d_y, c->d_z, B.cze, B.ck,
                                                    B.ckk, B.Len, B.node_base, c->p.ntf_times, c->p.ntf_pre,
                                                    B.coe, B.ntf, B.dtf);
+    section_fp64_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.cze, B.Len, B.node_base,
+                                                        c->p.ntf_times, c->p.ntf_pre, B.coe, B.ntf, B.dtf);
+    c->launches += 1;
     kt_end(c, km);
     km = kt_begin(c, KT_CENTERLINE);
     slot_counts_kernel<<<(unsigned)((slots + 255) / 256), 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf,

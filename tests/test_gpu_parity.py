@@ -82,3 +82,22 @@ def test_generator_matches_oracle(fwt, orc):
     ctx.close()
     del xyz
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("H,dB_over_sigma", [(0.3, 10.0), (0.7, 10.0), (0.8, 40.0), (0.5, 3.0)])
+def test_ntf_bit_exact_across_curvatures(fwt, orc, H, dB_over_sigma):
+    """The sub-segment count of every section, ceil(ntf_times theta / 2 pi) + 1, decided by the
+    quadrature estimate of the turning angle or its fallbacks, equals the oracle's FP64 sum
+    over the reference's ntf_pre + 1 samples, for rough and smooth lines alike."""
+    from fastweavturb_b200.configs import Level, Workload
+
+    lv = [Level(tubes=6, nodes=256, sigma=0.1, Gamma=1.0, H=H, dB=dB_over_sigma * 0.1),
+          Level(tubes=6, nodes=512, sigma=0.05, Gamma=0.5, H=H, dB=dB_over_sigma * 0.05)]
+    w = Workload("ntf", 64, lv, seed=21)
+    p, cl = oracle_inputs(orc, w)
+    ctx = fwt.Context(gpu_params(fwt, w))
+    ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+    ctx.deposit()
+    total = sum(int(orc.line_ntf(cl.line(i), p.ntf_times, p.ntf_pre)[0][:-1].sum()) for i in range(len(cl.npoint)))
+    assert ctx.counters()["subsegments"] == total
+    ctx.close()
