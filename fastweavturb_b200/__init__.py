@@ -12,6 +12,7 @@ from .api import (  # noqa: F401
     fbb_signs,
     library,
     run_dir,
+    sp_exponents,
     sp_separations,
 )
 from .configs import CONFIGS, Workload, build_workload  # noqa: F401

@@ -55,7 +55,8 @@ class _Params(ctypes.Structure):
 EXPORTS = [
     "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_set_centerlines",
     "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
-    "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_field_wh", "fwt_copy_field", "fwt_write_outputs", "fwt_run_dir", "fwt_run",
+    "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_copy_field",
+    "fwt_write_outputs", "fwt_run_dir", "fwt_run",
     "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
 ]
 
@@ -88,6 +89,7 @@ def library(path: str | None = None):
         "fwt_pdf": [vp, ip, ip, ip, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
                     ctypes.POINTER(ctypes.c_uint64)],
         "fwt_sp": [vp, ip, ctypes.POINTER(ctypes.c_int), ip, dp],
+        "fwt_sp_exponents": [dp, dp, ip, ip, dp, dp],
         "fwt_field_wh": [vp, ctypes.POINTER(ctypes.c_float)],
         "fwt_copy_field": [vp, ip, ip, dp],
         "fwt_write_outputs": [vp, ctypes.c_char_p],
@@ -317,6 +319,21 @@ class Context:
         _check(library().fwt_fbb_generate(self._h, ctypes.c_uint64(seed), len(tubes), _ptr(tubes, ctypes.c_int),
                                           _ptr(nodes, ctypes.c_int), _ptr(H, ctypes.c_double),
                                           _ptr(dB, ctypes.c_double), dx, dy, dz))
+
+
+def sp_exponents(rdr, Sp):
+    """Scaling exponents zeta_p (p = 1..pmax) and flatness S_4/S_2^2 per separation of an
+    S_p table (output/stat/Sp_zeta.m:3-23, output/stat/Flatness.m:14-19).
+
+    rdr: nr separations r*dr; Sp: (pmax, nr).  Returns (zeta, flatness)."""
+    rdr = np.ascontiguousarray(rdr, dtype=np.float64)
+    Sp = np.ascontiguousarray(Sp, dtype=np.float64)
+    pmax, nr = Sp.shape
+    zeta = np.zeros(pmax)
+    flat = np.zeros(nr)
+    _check(library().fwt_sp_exponents(_ptr(rdr, ctypes.c_double), _ptr(Sp, ctypes.c_double), nr, pmax,
+                                      _ptr(zeta, ctypes.c_double), _ptr(flat, ctypes.c_double)))
+    return zeta, flat
 
 
 def run_dir(rundir, params: Params | None = None):

@@ -176,6 +176,7 @@ int io_write_outputs(Ctx *c, const char *outdir);
 int fbb_generate(Ctx *c, uint64_t seed, int nlev, const int *tubes, const int *nodes, const double *H,
                  const double *dB, double *d_x, double *d_y, double *d_z);
 
+int scaling_exponents(const double *rdr, const double *Sp, int nr, int pmax, double *zeta, double *flat);
 inline size_t field_elems(const Ctx *c) { return (size_t)c->p.N * c->p.N * c->p.N; }
 inline size_t real_bytes(const Ctx *c) { return c->p.precision == 64 ? 8 : 4; }
 

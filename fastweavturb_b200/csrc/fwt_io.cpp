@@ -320,6 +320,17 @@ int io_write_outputs(Ctx *c, const char *outdir)
         }
         fclose(f);
     }
+    // Sp_zeta.dat (output/stat/Sp_zeta.m:47-67): p, zeta_p and the K41 value p/3 for even
+    // p = 2..10, tab-separated
+    if (c->p.if_Sp && c->sp_r.size() >= 10 && c->sp.size() / c->sp_r.size() >= 10) {
+        const int nr = (int)c->sp_r.size();
+        std::vector<double> rdr(nr), zeta(10);
+        for (int m = 0; m < nr; ++m) rdr[m] = c->sp_r[m] * (kPi2 / c->p.N);
+        FWT_TRY(scaling_exponents(rdr.data(), c->sp.data(), nr, 10, zeta.data(), nullptr));
+        FWT_TRY(open_w(od + "/stat/Sp_zeta.dat", &f));
+        for (int p = 2; p <= 10; p += 2) fprintf(f, "%d\t%.15g\t%.15g\n", p, zeta[p - 1], p / 3.0);
+        fclose(f);
+    }
     // field_wh.dat: raw float32 stream, Fortran order (n_d, n_d, n_d, 2) (subroutine.f90:1396-1398)
     if (c->p.vorticity_output && !c->field_wh.empty()) {
         FWT_TRY(open_w(od + "/field_wh.dat", &f));

@@ -115,6 +115,13 @@ int fwt_pdf_noalloc(const void *d_data, int precision, int nx, int ny, int nz, d
 /* Longitudinal structure functions S_p(r), p = 1..pmax, at nr separations r (grid units)
  * (subroutine.f90:64-129).  Sp: pmax x nr doubles, Sp[(p-1)*nr + m]. */
 int fwt_sp(fwt_ctx *ctx, int pmax, const int *r, int nr, double *Sp);
+/* Scaling exponents and flatness of a structure-function table, as the reference's
+ * post-processing of Sp.dat (output/stat/Sp_zeta.m:3-23, output/stat/Flatness.m:14-19):
+ * zeta[p-1] = least-squares slope of log|S_p| against log(rdr) over rows nr-9 .. nr-4
+ * (0-based), p = 1..pmax (needs nr >= 10); flat[m] = S_4 / S_2^2 on every row (needs
+ * pmax >= 4).  rdr: nr separations r*dr; Sp: pmax x nr as fwt_sp writes it.  Either output
+ * may be NULL.  Host arithmetic only. */
+int fwt_sp_exponents(const double *rdr, const double *Sp, int nr, int pmax, double *zeta, double *flat);
 /* Downsampled |omega| and omega.u (normalised) as float32, Fortran order
  * (n_d, n_d, n_d, 2) (tube.f90:1055-1071). */
 int fwt_field_wh(fwt_ctx *ctx, float *host_out);

@@ -462,6 +462,20 @@ def structure_functions_np(vel, pmax=10, r=None):
     return np.asarray(r), Sp
 
 
+def sp_exponents(rdr, Sp):
+    """zeta_p = slope of the degree-1 least-squares fit of log|S_p| against log(r dr) over the
+    1-based rows nr-9 .. nr-4 (output/stat/Sp_zeta.m:6-7,18-21); flatness S_4/S_2^2 per row
+    (output/stat/Flatness.m:18)."""
+    rdr = np.asarray(rdr, dtype=np.float64)
+    Sp = np.asarray(Sp, dtype=np.float64)
+    nr = len(rdr)
+    ie = nr - 4
+    rows = slice(ie - 6, ie)
+    zeta = np.array([np.polyfit(np.log(rdr[rows]), np.log(np.abs(Sp[p, rows])), 1)[0] for p in range(Sp.shape[0])])
+    flat = Sp[3] / Sp[1] ** 2
+    return zeta, flat
+
+
 def field_wh(vor, vel, n_d):
     """Downsampled |omega| and omega.u as REAL(4), Fortran order (tube.f90:1055-1071)."""
     N = vor.shape[1]

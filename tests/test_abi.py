@@ -91,3 +91,20 @@ def test_create_fails_loudly_without_a_gpu(fwt):
     with pytest.raises(fwt.FwtError) as e:
         fwt.Context(fwt.Params(N=16, N_downsample=16))
     assert e.value.code == -2       # FWT_E_CUDA: no CPU fallback
+
+
+def test_sp_exponents_match_the_oracle(fwt, orc):
+    """zeta_p and flatness of the reference's post-processing, through the C-ABI, on a
+    synthetic table with known exponents S_p = c_p r^{p/3 + d_p}."""
+    r = fwt.sp_separations(256).astype(np.float64) * (2 * np.pi / 256)
+    p = np.arange(1, 11)[:, None]
+    want = p[:, 0] / 3.0 + 0.01 * (p[:, 0] - 3) ** 2
+    Sp = (0.5 + 0.1 * p) * r[None, :] ** want[:, None]
+    Sp[2] *= -1.0                          # odd orders may be negative; the fit uses |S_p|
+    zeta, flat = fwt.sp_exponents(r, Sp)
+    z_o, f_o = orc.sp_exponents(r, Sp)
+    np.testing.assert_allclose(zeta, want, rtol=1e-12)
+    np.testing.assert_allclose(zeta, z_o, rtol=1e-12)
+    np.testing.assert_allclose(flat, f_o, rtol=1e-14)
+    with pytest.raises(fwt.FwtError):
+        fwt.sp_exponents(r[:8], Sp[:, :8])

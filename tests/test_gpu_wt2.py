@@ -154,6 +154,12 @@ def test_wt2_run_dir_writes_the_reference_outputs(fwt, orc, wt2, tmp_path):
     assert np.all(np.abs(sp[:, 1]) < 1e-12 * scale2) and np.all(np.abs(Sp[0]) < 1e-12 * scale2)   # S_1 ~ 0
     for q in range(1, 10):     # ES16.5
         np.testing.assert_allclose(sp[:, 1 + q], Sp[q], rtol=1e-4, atol=1e-9 * np.abs(Sp[q]).max())
+    # Sp_zeta.dat: even p, zeta_p (output/stat/Sp_zeta.m), K41 p/3
+    zt = np.loadtxt(od / "stat" / "Sp_zeta.dat")
+    zeta, _ = fwt.sp_exponents(r * 2 * np.pi / 64, Sp)
+    assert zt.shape == (5, 3) and np.array_equal(zt[:, 0], [2, 4, 6, 8, 10])
+    np.testing.assert_allclose(zt[:, 1], zeta[1::2], rtol=1e-9)
+    np.testing.assert_allclose(zt[:, 2], zt[:, 0] / 3.0)
     pdf = np.loadtxt(od / "stat" / "pdf_um.dat")
     assert pdf.shape == (1000, 2)
     v, pd, c = ctx.export_pdf(which=0, component=-1, nbins=1000)
