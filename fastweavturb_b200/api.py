@@ -58,6 +58,8 @@ EXPORTS = [
     "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_copy_field",
     "fwt_write_outputs", "fwt_run_dir", "fwt_run",
     "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
+    "fwt_mlp_create", "fwt_mlp_destroy", "fwt_mlp_nparams", "fwt_mlp_get_params", "fwt_mlp_set_params",
+    "fwt_mlp_forward", "fwt_mlp_loss_grad", "fwt_mlp_train_step", "fwt_gemm_bf16",
 ]
 
 

@@ -166,6 +166,36 @@ int fwt_fbb_generate(fwt_ctx *ctx, uint64_t seed, int nlev, const int *tubes, co
 /* Circulation signs (+1/-1) of tubes [0, ntubes) for the same seed. */
 int fwt_fbb_signs(uint64_t seed, int ntubes, int *signs);
 
+/* ------------------------------------------------------------------ learned surrogate
+ * No counterpart in the reference (its statistics are only plotted there).  A multilayer
+ * perceptron n_in -> width (depth hidden layers, GELU) -> n_out trained with Adam on the
+ * weighted mean-square error sum_j w_j (y_j - t_j)^2 / (batch n_out); its matrix products run
+ * on the tensor cores (BF16 operands, FP32 accumulation), everything else in FP32.  Host
+ * arrays are row-major (batch x features). */
+typedef struct fwt_mlp fwt_mlp;
+/* n_in 1..64, width 16..256 (multiple of 16), depth >= 1, n_out 1..256; weights drawn
+ * uniform +-sqrt(6 / (fan_in + fan_out)) from seed, biases zero. */
+int fwt_mlp_create(int device, int n_in, int width, int depth, int n_out, int batch_max, uint64_t seed,
+                   fwt_mlp **out);
+int fwt_mlp_destroy(fwt_mlp *m);
+/* Parameter count and the flattened parameters, layer by layer: W (n_out_l x n_in_l,
+ * row-major) then b. */
+int fwt_mlp_nparams(fwt_mlp *m, int64_t *n);
+int fwt_mlp_get_params(fwt_mlp *m, float *params);
+int fwt_mlp_set_params(fwt_mlp *m, const float *params);
+/* y = mlp(x) for batch <= batch_max rows. */
+int fwt_mlp_forward(fwt_mlp *m, const float *x, int batch, float *y);
+/* Loss and its gradients with respect to the parameters (fwt_mlp_get_params layout) and the
+ * inputs (batch x n_in); loss, grad_params, grad_x and w_out (n_out weights) may be NULL. */
+int fwt_mlp_loss_grad(fwt_mlp *m, const float *x, const float *t, const float *w_out, int batch, double *loss,
+                      float *grad_params, float *grad_x);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8, learning rate lr) on a batch. */
+int fwt_mlp_train_step(fwt_mlp *m, const float *x, const float *t, const float *w_out, int batch, float lr,
+                       double *loss);
+/* The surrogate's tensor-core product on device arrays: C (M x N, FP32, leading dimension
+ * ldc) = A (M x K, BF16) . B (N x K, BF16)^T, K a multiple of 64, operands 16-byte aligned. */
+int fwt_gemm_bf16(const void *A, const void *B, float *C, int M, int N, int K, int ldc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

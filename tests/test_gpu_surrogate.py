@@ -1,0 +1,74 @@
+"""The learned surrogate's network on the GPU: the tcgen05 tensor-core product against an FP64
+product of the same BF16 operands, the forward and backward passes against the CPU oracle
+(oracle/mlp_oracle.py, the same BF16 rounding points, FP64 accumulation), and training.
+
+Tolerances: the product is exact BF16 x BF16 products summed in FP32, <= 1.5e-7 sqrt(K)
+relative L2;
+the network's loss and gradients <= 1e-2 relative L2 (an FP32 sum that lands on the other
+side of a BF16 rounding boundary moves one element by 2^-8).
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("M,N,K", [(256, 256, 256), (200, 45, 128), (64, 256, 4096), (1000, 130, 64)])
+def test_tensor_core_gemm_matches_fp64(fwt, M, N, K):
+    import torch
+
+    from fastweavturb_b200.surrogate import gemm_bf16
+
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    C = torch.full((M, N), float("nan"), device="cuda")
+    gemm_bf16(A.data_ptr(), B.data_ptr(), C.data_ptr(), M, N, K)
+    torch.cuda.synchronize()
+    want = A.double().cpu().numpy() @ B.double().cpu().numpy().T
+    got = C.cpu().numpy()
+    assert np.isfinite(got).all()
+    assert rel_l2(got, want) <= 1.5e-7 * np.sqrt(K)     # FP32 accumulation of K exact products
+
+
+def _mlp(width=64, depth=2, seed=3):
+    from fastweavturb_b200.surrogate import MLP
+    return MLP(n_in=5, width=width, depth=depth, n_out=45, batch_max=256, seed=seed)
+
+
+def test_mlp_forward_and_gradients_match_oracle(fwt):
+    from oracle import mlp_oracle as MO
+
+    rng = np.random.default_rng(1)
+    net = _mlp()
+    p = net.params().astype(np.float64)
+    X = rng.uniform(-1, 1, (100, 5)).astype(np.float32)
+    T = rng.normal(0, 1, (100, 45)).astype(np.float32)
+    w = rng.uniform(0.5, 2.0, 45).astype(np.float32)
+    Y = net.forward(X)
+    Yo, _, _ = MO.forward(p, net.widths, X)
+    assert rel_l2(Y, Yo) <= 1e-3
+    loss, gp, gx = net.loss_grad(X, T, w_out=w)
+    lo, gpo, gxo = MO.loss_grad(p, net.widths, X, T, w_out=w)
+    assert loss == pytest.approx(lo, rel=1e-3)
+    assert rel_l2(gp, gpo) <= 1e-2
+    assert rel_l2(gx, gxo) <= 1e-2
+    # and against the plain FP64 network: BF16 operands cost a few parts in 10^3
+    lo64, gp64, gx64 = MO.loss_grad(p, net.widths, X, T, w_out=w, bf16_ops=False)
+    assert rel_l2(gp, gp64) <= 5e-2
+    net.close()
+
+
+def test_mlp_training_fits_a_smooth_map(fwt):
+    rng = np.random.default_rng(2)
+    net = _mlp(width=128, depth=3)
+    X = rng.uniform(-1, 1, (256, 5)).astype(np.float32)
+    k = np.arange(45)
+    T = (np.sin(X[:, :1] * (1 + k / 15.0)) + X[:, 1:2] * X[:, 2:3] * np.cos(k / 7.0)).astype(np.float32)
+    first = net.train_step(X, T, 1e-3)
+    for _ in range(400):
+        last = net.train_step(X, T, 1e-3)
+    assert last < 0.05 * first
+    net.close()

@@ -383,3 +383,36 @@ def test_field_wh_picks_every_rd_th_point(orc):
     # Fortran sample index i*r_d (1-based) is 0-based i*r_d - 1
     i = 2 * (N // nd) - 1
     assert out[0, 0, 1, 1] == np.float32(np.sqrt(np.sum(w[:, N // nd - 1, i, i] ** 2)))
+
+
+# ----------------------------------------------------------------------------- surrogate oracle
+
+def test_mlp_oracle_gradients_by_finite_differences():
+    """The FP64 network's backward pass against central differences of its loss."""
+    from oracle import mlp_oracle as MO
+    rng = np.random.default_rng(4)
+    widths = [5, 16, 16, 7]
+    n = sum(k * m + m for k, m in zip(widths[:-1], widths[1:]))
+    p = rng.normal(0, 0.5, n)
+    X = rng.uniform(-1, 1, (9, 5))
+    T = rng.normal(0, 1, (9, 7))
+    w = rng.uniform(0.5, 2, 7)
+    loss, gp, gx = MO.loss_grad(p, widths, X, T, w, bf16_ops=False)
+    h = 1e-6
+    for i in rng.choice(n, 25, replace=False):
+        e = np.zeros(n)
+        e[i] = h
+        fd = (MO.loss_grad(p + e, widths, X, T, w, False)[0] - MO.loss_grad(p - e, widths, X, T, w, False)[0]) / (2 * h)
+        assert gp[i] == pytest.approx(fd, rel=1e-5, abs=1e-9)
+    for (r, c) in [(0, 0), (3, 2), (8, 4)]:
+        E = np.zeros_like(X)
+        E[r, c] = h
+        fd = (MO.loss_grad(p, widths, X + E, T, w, False)[0] - MO.loss_grad(p, widths, X - E, T, w, False)[0]) / (2 * h)
+        assert gx[r, c] == pytest.approx(fd, rel=1e-5, abs=1e-9)
+
+
+def test_bf16_rounding_is_round_to_nearest_even():
+    from oracle import mlp_oracle as MO
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -9, 1.0 + 2 ** -9, -2.5, 3.0e38], dtype=np.float32)
+    r = MO.bf16(x)
+    assert list(r[:5]) == [1.0, 1.0, 1.0 + 2 ** -7, 1.0, -2.5]
