@@ -58,7 +58,7 @@ EXPORTS = [
     "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_copy_field",
     "fwt_write_outputs", "fwt_run_dir", "fwt_run",
     "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
-    "fwt_mlp_create", "fwt_mlp_destroy", "fwt_mlp_nparams", "fwt_mlp_get_params", "fwt_mlp_set_params",
+    "fwt_set_tuning", "fwt_mlp_create", "fwt_mlp_destroy", "fwt_mlp_nparams", "fwt_mlp_get_params", "fwt_mlp_set_params",
     "fwt_mlp_forward", "fwt_mlp_loss_grad", "fwt_mlp_train_step", "fwt_gemm_bf16",
 ]
 
@@ -100,6 +100,7 @@ def library(path: str | None = None):
         "fwt_timings": [vp, dp, ip],
         "fwt_kernel_times": [vp, dp, i64p, ip],
         "fwt_counters": [vp, i64p, ip],
+        "fwt_set_tuning": [vp, ip, ctypes.c_double],
         "fwt_last_error": [ctypes.c_char_p, ip],
         "fwt_fbb_generate": [vp, ctypes.c_uint64, ip, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), dp,
                              dp, vp, vp, vp],
@@ -306,6 +307,10 @@ class Context:
         n = np.zeros(8, dtype=np.int64)
         library().fwt_kernel_times(self._h, _ptr(ms, ctypes.c_double), _ptr(n, ctypes.c_int64), 8)
         return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(self.KERNEL_CATEGORIES)}
+
+    def set_piece_radius_limit(self, cells):
+        """Tubes up to this truncation radius (grid spacings) take the chord-piece kernel."""
+        _check(library().fwt_set_tuning(self._h, 1, float(cells)))
 
     def counters(self):
         v = np.zeros(5, dtype=np.int64)

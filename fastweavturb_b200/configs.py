@@ -120,6 +120,20 @@ def ensemble_member(seed, N=None, rng=None):
     return w
 
 
+def surrogate_member(params, seed, N=64):
+    """A realisation for the learned surrogate from its five inputs (H, sigma_max/sigma_min,
+    density multiplier, levels, circulation exponent): the ensemble family of
+    ensemble_member with 64 * 2^l nodes per tube (a quarter of the benchmark's, so thousands
+    of realisations fit the training budget) and sigma_max/sigma_min = 2^(levels - 1)."""
+    H, _, dens, nlev, gexp = params
+    nlev = int(round(nlev))
+    w = Workload(f"surrogate member seed={seed}: N={N}, H={H:.3f}, levels={nlev}, density={dens:.2f}, "
+                 f"Gamma exponent={gexp:.3f}", N, _levels(nlev, 0.4, 4, 64, float(H), gexp=float(gexp),
+                                                           density=float(dens)), seed=seed)
+    w.extra = {"H": H, "levels": nlev, "density": dens, "gexp": gexp, "sigma_ratio_levels": 2.0 ** (nlev - 1)}
+    return w
+
+
 def small(N=32, seed=1, nlev=2, tubes0=2, nodes0=64, sigma0=0.4, H=0.7):
     """A small workload for parity tests (the FP64 oracle finishes it in seconds)."""
     return Workload(f"small: {N}^3, {nlev} levels", N, _levels(nlev, sigma0, tubes0, nodes0, H), seed=seed)

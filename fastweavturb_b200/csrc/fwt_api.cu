@@ -463,7 +463,7 @@ int fwt_run(fwt_ctx *h)
     PhaseTimer total(c->stream);
     {
         PhaseTimer t(c->stream);
-        FWT_TRY(deposit_lines(c, c->p.line_s, c->p.line_e));
+        FWT_TRY(deposit_lines(c, c->p.line_s, c->p.line_e > 0 ? c->p.line_e : c->nline));
         c->t_ms[1] = t.stop();
     }
     {
@@ -502,8 +502,9 @@ int fwt_run(fwt_ctx *h)
     // per-line times: the batch times apportioned by section count
     c->timing_line.assign(2 * (size_t)c->nline, 0.0);
     int64_t secs = 0;
-    for (int l = c->p.line_s - 1; l < c->p.line_e; ++l) secs += c->npoint[l];
-    for (int l = c->p.line_s - 1; l < c->p.line_e; ++l) {
+    const int le = c->p.line_e > 0 ? c->p.line_e : c->nline;
+    for (int l = c->p.line_s - 1; l < le; ++l) secs += c->npoint[l];
+    for (int l = c->p.line_s - 1; l < le; ++l) {
         const double f = secs ? (double)c->npoint[l] / secs : 0.0;
         c->timing_line[2 * l] = c->t_ms[0] * 1e-3 * f;
         c->timing_line[2 * l + 1] = c->t_ms[1] * 1e-3 * f;
@@ -561,6 +562,17 @@ int fwt_kernel_times(fwt_ctx *h, double *ms, int64_t *launches, int n)
         if (launches) launches[k] = c->kcount[k];
     }
     return k;
+}
+
+int fwt_set_tuning(fwt_ctx *h, int key, double value)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    if (key == FWT_TUNE_PIECE_RT_CELLS) {
+        c->piece_rt_cells = value;
+        return 0;
+    }
+    return fail(FWT_E_ARG, "unknown tuning key");
 }
 
 int fwt_counters(fwt_ctx *h, int64_t *v, int n)

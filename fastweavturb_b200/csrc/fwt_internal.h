@@ -74,6 +74,7 @@ struct Timers {
 struct Ctx {
     fwt_params p{};
     int dev = 0;
+    double piece_rt_cells = -1.0;   // tuning: piece kernel radius limit in grid spacings (< 0: default)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
 

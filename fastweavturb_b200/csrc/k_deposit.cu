@@ -225,9 +225,10 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
     const int64_t cap = batch_node_cap(c);
     const bool tile_path = c->p.precision == 32 && c->p.deposit_mode == 0;
     const double dxg = kPi2 / c->p.N;
-    // FWT_PIECE_RT_CELLS overrides the piece kernel's radius limit (in grid spacings)
+    // radius limit of the piece kernel in grid spacings: fwt_set_tuning, else the environment
+    // variable FWT_PIECE_RT_CELLS, else the default
     const char *env = std::getenv("FWT_PIECE_RT_CELLS");
-    const double rt_cells = env ? std::atof(env) : kPieceMaxRtCells;
+    const double rt_cells = c->piece_rt_cells >= 0.0 ? c->piece_rt_cells : (env ? std::atof(env) : kPieceMaxRtCells);
     auto thin = [&](int l) {
         return tile_path && c->p.Rtube_ratio * c->p.sigma_ratio * c->sigma[l] <= rt_cells * dxg;
     };

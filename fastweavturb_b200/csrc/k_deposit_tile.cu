@@ -249,6 +249,10 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     WarpStage &S = reinterpret_cast<WarpStage *>(dsm + kAccBytes)[warp];
     if (lane == 0) mbar_init(&S.bar);
+    // chunks are handed out through a shared counter: a warp that finishes early takes the
+    // next one, so the warps of a tile end close together at the epilogue's barrier
+    __shared__ int next_chunk;
+    if (threadIdx.x == 0) next_chunk = kDepWarps;
     tile_acc_init<Accumulate>(acc, N, x0, y0, z0, scale, wx, wy, wz);
     __syncthreads();
     const int64_t c0 = tile_off[tile], c1 = tile_off[tile + 1];
@@ -258,7 +262,7 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
     uint32_t phase = 0;
     bool failed = false;
     int qn = 0;   // queued points of this warp (warp-uniform)
-    for (int ch = warp; ch < nchunks && !failed; ch += kDepWarps) {
+    for (int ch = warp; ch < nchunks && !failed;) {
         const int64_t base = c0 + (int64_t)ch * kWarpChunk;
         const int nc = (c1 - base < kWarpChunk) ? (int)(c1 - base) : kWarpChunk;
         const uint32_t v = lane < nc ? __ldg(list + base + lane) : 0u;
@@ -350,6 +354,9 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
         }
         if (qn > 0) drain_queue<General>(S, acc, lane, qn, qn, fscale, fmaxq, err);
         __syncwarp();   // the warp's stage is reused by its next chunk
+        int nxt = 0;
+        if (lane == 0) nxt = atomicAdd(&next_chunk, 1);
+        ch = __shfl_sync(0xffffffffu, nxt, 0);
     }
     if (failed && lane == 0) atomicOr(err, 2);
     __syncthreads();

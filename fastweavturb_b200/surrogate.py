@@ -16,7 +16,7 @@ import time
 
 import numpy as np
 
-from .api import Context, FwtError, Params, _check, _ptr, library, sp_exponents, sp_separations
+from .api import _check, _ptr, library
 
 N_IN, N_OUT = 5, 45
 PARAM_LO = np.array([0.3, 2.0, 0.5, 2.0, 1.2])    # H, sigma ratio, density, levels, Gamma exponent
@@ -110,3 +110,170 @@ class MLP:
 def gemm_bf16(A_dev, B_dev, C_dev, M, N, K, ldc=None, stream=None):
     """C = A . B^T on the tensor cores for device pointers (BF16 A, B; FP32 C)."""
     _check(_lib().fwt_gemm_bf16(A_dev, B_dev, C_dev, M, N, K, ldc or N, stream))
+
+
+# ------------------------------------------------------------------------------ statistics
+N_SHELLS, N_FLAT = 32, 8
+
+
+def features(st, N):
+    """The 45 statistics of one realisation: log E(k) at 32 log-spaced wavenumbers in
+    [1, N/2] (linear in log-log between shells), the flatness at the first 8 distinct
+    separations of the reference's S_p grid and zeta_2 .. zeta_6."""
+    Ek = np.maximum(np.asarray(st["Ek"], dtype=np.float64), 1e-300)
+    k = np.arange(1, len(Ek) + 1, dtype=np.float64)
+    kq = np.exp(np.linspace(0.0, np.log(N / 2), N_SHELLS))
+    logE = np.interp(np.log(kq), np.log(k), np.log(Ek))
+    r = np.asarray(st["r"])
+    rows = [0] + [i for i in range(1, len(r)) if r[i] != r[i - 1]]
+    flat = np.asarray(st["flat"])[rows[:N_FLAT]]
+    zeta = np.asarray(st["zeta"])[1:6]
+    return np.concatenate([logE, flat, zeta])
+
+
+def fit_error(y, y_target):
+    """(mean |d log E|, mean relative flatness error): the fit is within 2 % when both <= 0.02."""
+    y, t = np.asarray(y), np.asarray(y_target)
+    eE = float(np.mean(np.abs(y[:N_SHELLS] - t[:N_SHELLS])))
+    eF = float(np.mean(np.abs(y[N_SHELLS:N_SHELLS + N_FLAT] - t[N_SHELLS:N_SHELLS + N_FLAT]) /
+                       np.abs(t[N_SHELLS:N_SHELLS + N_FLAT])))
+    return eE, eF
+
+
+def draw_params(rng, n):
+    """n parameter draws of the ensemble family: H ~ U[0.3, 0.8], levels in {2, 3, 4},
+    sigma ratio 2^(levels-1), density ~ U[0.5, 4], circulation exponent ~ U[1.2, 1.5]."""
+    lev = rng.integers(2, 5, n).astype(np.float64)
+    return np.stack([rng.uniform(0.3, 0.8, n), 2.0 ** (lev - 1), rng.uniform(0.5, 4.0, n), lev,
+                     rng.uniform(1.2, 1.5, n)], axis=1)
+
+
+def generate(P, seeds, N=64, ens=None):
+    """Statistics of one realisation per parameter row, by the batched generator."""
+    from .configs import surrogate_member
+    from .ensemble import Ensemble
+    own = ens is None
+    ens = ens or Ensemble()
+    members = [surrogate_member(p, int(s), N=N) for p, s in zip(P, seeds)]
+    stats, secs, rate = ens.run(members)
+    Y = np.stack([features(s, N) for s in stats])
+    if own:
+        ens.close()
+    return Y, secs
+
+
+class Surrogate:
+    """The network with its input scaling (to [-1, 1] over the parameter box) and output
+    standardisation (training-set mean and deviation)."""
+
+    def __init__(self, width=256, depth=4, seed=0, batch_max=4096):
+        self.net = MLP(N_IN, width, depth, N_OUT, batch_max=batch_max, seed=seed)
+        self.ymu = np.zeros(N_OUT)
+        self.ysd = np.ones(N_OUT)
+
+    @staticmethod
+    def xin(P):
+        return 2.0 * (np.asarray(P) - PARAM_LO) / (PARAM_HI - PARAM_LO) - 1.0
+
+    def fit(self, P, Y, steps=3000, batch=256, lr=1e-3, seed=0):
+        rng = np.random.default_rng(seed)
+        self.ymu = Y.mean(axis=0)
+        self.ysd = Y.std(axis=0) + 1e-9
+        X = self.xin(P)
+        T = (Y - self.ymu) / self.ysd
+        losses = []
+        for s in range(steps):
+            idx = rng.choice(len(X), size=min(batch, len(X)), replace=False)
+            lr_s = lr * (0.1 ** (s / steps))          # exponential decay to lr/10
+            losses.append(self.net.train_step(X[idx], T[idx], lr_s))
+        return np.array(losses)
+
+    def predict(self, P):
+        return self.net.forward(self.xin(P)) * self.ysd + self.ymu
+
+    def close(self):
+        self.net.close()
+
+
+def inverse_fit(sur, y_target, starts=64, iters=300, lr=0.05, seed=0):
+    """Parameters whose predicted statistics best match y_target (spectrum and flatness):
+    Adam on the network's input gradient from `starts` random starts for each level count
+    (levels and the sigma ratio held at their discrete values), best predicted per level."""
+    rng = np.random.default_rng(seed)
+    w = np.zeros(N_OUT)
+    w[:N_SHELLS + N_FLAT] = 1.0                    # fit the spectrum and the flatness
+    t = (np.asarray(y_target) - sur.ymu) / sur.ysd
+    best = []
+    for lev in (2.0, 3.0, 4.0):
+        P = draw_params(rng, starts)
+        P[:, 3] = lev
+        P[:, 1] = 2.0 ** (lev - 1)
+        X = Surrogate.xin(P).astype(np.float32)
+        m1 = np.zeros_like(X)
+        m2 = np.zeros_like(X)
+        free = np.array([1, 0, 1, 0, 1], dtype=np.float32)   # H, density, Gamma exponent
+        T = np.repeat(t[None, :], starts, axis=0).astype(np.float32)
+        for it in range(1, iters + 1):
+            _, _, gx = sur.net.loss_grad(X, T, w_out=w, params=False, inputs=True)
+            g = gx * free
+            m1 = 0.9 * m1 + 0.1 * g
+            m2 = 0.999 * m2 + 0.001 * g * g
+            X -= lr * (m1 / (1 - 0.9 ** it)) / (np.sqrt(m2 / (1 - 0.999 ** it)) + 1e-8)
+            X = np.clip(X, -1.0, 1.0)
+        Y = sur.net.forward(X) * sur.ysd + sur.ymu
+        err = np.array([sum(fit_error(y, y_target)) for y in Y])
+        i = int(np.argmin(err))
+        Pfit = (X[i] + 1.0) / 2.0 * (PARAM_HI - PARAM_LO) + PARAM_LO
+        Pfit[3], Pfit[1] = lev, 2.0 ** (lev - 1)
+        best.append((err[i], Pfit))
+    best.sort(key=lambda b: b[0])
+    return [b[1] for b in best]
+
+
+def refine_with_generator(cands, y_target, seed_eval, runs, N=64, ens=None, seed=5, rounds_per_shrink=2):
+    """Generator-judged search from starting candidates: the candidates are run, then the
+    remaining runs perturb the best one's continuous parameters (H, density, circulation
+    exponent; the level count stays) in batches of 4 with a radius that shrinks by 0.7 every
+    `rounds_per_shrink` batches, keeping improvements.  Returns (params, (errE, errF), runs)."""
+    rng = np.random.default_rng(seed)
+    P = np.array(cands, dtype=np.float64)
+    Y, _ = generate(P, [seed_eval] * len(P), N=N, ens=ens)
+    errs = [sum(fit_error(y, y_target)) for y in Y]
+    i = int(np.argmin(errs))
+    best, best_e, best_y = P[i].copy(), errs[i], Y[i]
+    used = len(P)
+    span = PARAM_HI - PARAM_LO
+    radius, rnd = 0.15, 0
+    while used < runs:
+        k = min(4, runs - used)
+        Q = np.repeat(best[None, :], k, axis=0)
+        for j in (0, 2, 4):
+            Q[:, j] = np.clip(Q[:, j] + rng.normal(0, radius * span[j], k), PARAM_LO[j], PARAM_HI[j])
+        Yq, _ = generate(Q, [seed_eval] * k, N=N, ens=ens)
+        used += k
+        for q, y in zip(Q, Yq):
+            e = sum(fit_error(y, y_target))
+            if e < best_e:
+                best, best_e, best_y = q.copy(), e, y
+        rnd += 1
+        if rnd % rounds_per_shrink == 0:
+            radius *= 0.7
+    return best, fit_error(best_y, y_target), used
+
+
+def fit_surrogate_driven(sur, y_target, seed_eval, runs, N=64, ens=None):
+    """The network's best parameters for each level count start the generator-judged search."""
+    t0 = time.perf_counter()
+    p, e, used = refine_with_generator(inverse_fit(sur, y_target), y_target, seed_eval, runs, N=N, ens=ens)
+    return p, e, time.perf_counter() - t0, used
+
+
+def fit_generator_only(y_target, seed_eval, runs, N=64, ens=None, seed=1):
+    """The method without the network: one random draw per level count starts the same
+    generator-judged search."""
+    t0 = time.perf_counter()
+    P = draw_params(np.random.default_rng(seed), 3)
+    P[:, 3] = [2.0, 3.0, 4.0]
+    P[:, 1] = 2.0 ** (P[:, 3] - 1)
+    p, e, used = refine_with_generator(list(P), y_target, seed_eval, runs, N=N, ens=ens)
+    return p, e, time.perf_counter() - t0, used

@@ -37,7 +37,8 @@ typedef struct fwt_ctx fwt_ctx;
 typedef struct {
     int N;              /* grid points per side, nx = ny = nz (tube.f90:193,200-201) */
     int N_downsample;   /* field output points per side (tube.f90:195,1056) */
-    int line_s, line_e; /* 1-based inclusive range of lines to deposit (tube.f90:197-199,528) */
+    int line_s, line_e; /* 1-based inclusive range of lines to deposit (tube.f90:197-199,528);
+                           line_e = 0: up to the last line */
     double sigma_ratio; /* sigma_max / sigma_min (tube.f90:203,538) */
     double eta_t;       /* twist rate eta0 (tube.f90:206) */
     int ntf_times;      /* sub-segments per 2pi of turning (tube.f90:210,641) */
@@ -152,6 +153,14 @@ int fwt_kernel_times(fwt_ctx *ctx, double *ms, int64_t *launches, int n);
 /* Counters of the last deposition: c[0] lines, c[1] sections, c[2] sub-segments,
  * c[3] candidate (tile, sub-segment) pairs, c[4] kernel launches of the last fwt_run. */
 int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
+
+/* Tuning knobs of the context (no counterpart in the reference).  FWT_TUNE_PIECE_RT_CELLS:
+ * lines whose truncation radius Rtube_ratio * sigma_max is at most `value` grid spacings are
+ * deposited by the chord-piece kernel, thicker ones by the sub-segment kernel (value < 0
+ * restores the default, 2.5).  Results agree within FP32 rounding either way; the choice is
+ * speed only, and the ensemble autotuner sets it per grid size. */
+#define FWT_TUNE_PIECE_RT_CELLS 1
+int fwt_set_tuning(fwt_ctx *ctx, int key, double value);
 
 /* Message of the last error on this thread. */
 int fwt_last_error(char *buf, int len);

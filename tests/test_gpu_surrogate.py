@@ -72,3 +72,25 @@ def test_mlp_training_fits_a_smooth_map(fwt):
         last = net.train_step(X, T, 1e-3)
     assert last < 0.05 * first
     net.close()
+
+
+def test_surrogate_learns_the_generator_and_fits_held_out_targets(fwt):
+    """Trained on 512 realisations of the batched generator (64^3), the network predicts
+    held-out statistics better than the training mean, and the surrogate-driven inverse fit
+    (16 generator runs per target) finds parameters whose realisation matches each held-out
+    target's spectrum and flatness more closely than the training set's mean statistics do.
+
+    Which of the two searches (from the network's proposals or from random draws) wins on a
+    handful of targets is a noisy quantity; the experiment's command line reports it over
+    more targets and this test does not assert it."""
+    from fastweavturb_b200 import surrogate_experiment as E
+
+    line = E.main(["--train", "512", "--valid", "32", "--N", "64", "--steps", "1500", "--seed", "3",
+                   "--runs", "16", "--targets", "3"])
+    v = line["valid_rms_std_units"]
+    assert v["network"] < 0.85 * v["training_mean"]
+    assert line["loss_last"] < 0.5 * line["loss_first"]
+    for f in line["fits"]:
+        s, m = f["surrogate"], f["training_mean"]
+        assert s["runs"] <= 16 and f["generator_only"]["runs"] <= 16
+        assert s["err_logE"] + s["err_flat"] < m["err_logE"] + m["err_flat"], f
