@@ -195,34 +195,36 @@ class Surrogate:
         self.net.close()
 
 
-def inverse_fit(sur, y_target, starts=64, iters=300, lr=0.05, seed=0):
+def inverse_fit(sur, y_target, starts=64, iters=200, lr=0.05, seed=0):
     """Parameters whose predicted statistics best match y_target (spectrum and flatness):
-    Adam on the network's input gradient from `starts` random starts for each level count
-    (levels and the sigma ratio held at their discrete values), best predicted per level."""
+    Adam on the network's input gradient from `starts` random starts for each level count,
+    all level counts in one batch (levels and the sigma ratio held at their discrete values);
+    returns the best predicted parameters of each level count, best first."""
     rng = np.random.default_rng(seed)
     w = np.zeros(N_OUT)
     w[:N_SHELLS + N_FLAT] = 1.0                    # fit the spectrum and the flatness
     t = (np.asarray(y_target) - sur.ymu) / sur.ysd
+    levels = (2.0, 3.0, 4.0)
+    P = draw_params(rng, starts * len(levels))
+    P[:, 3] = np.repeat(levels, starts)
+    P[:, 1] = 2.0 ** (P[:, 3] - 1)
+    X = Surrogate.xin(P).astype(np.float32)
+    m1 = np.zeros_like(X)
+    m2 = np.zeros_like(X)
+    free = np.array([1, 0, 1, 0, 1], dtype=np.float32)   # H, density, Gamma exponent
+    T = np.repeat(t[None, :], len(X), axis=0).astype(np.float32)
+    for it in range(1, iters + 1):
+        _, _, gx = sur.net.loss_grad(X, T, w_out=w, params=False, inputs=True)
+        g = gx * free
+        m1 = 0.9 * m1 + 0.1 * g
+        m2 = 0.999 * m2 + 0.001 * g * g
+        X -= lr * (m1 / (1 - 0.9 ** it)) / (np.sqrt(m2 / (1 - 0.999 ** it)) + 1e-8)
+        X = np.clip(X, -1.0, 1.0)
+    Y = sur.net.forward(X) * sur.ysd + sur.ymu
+    err = np.array([sum(fit_error(y, y_target)) for y in Y])
     best = []
-    for lev in (2.0, 3.0, 4.0):
-        P = draw_params(rng, starts)
-        P[:, 3] = lev
-        P[:, 1] = 2.0 ** (lev - 1)
-        X = Surrogate.xin(P).astype(np.float32)
-        m1 = np.zeros_like(X)
-        m2 = np.zeros_like(X)
-        free = np.array([1, 0, 1, 0, 1], dtype=np.float32)   # H, density, Gamma exponent
-        T = np.repeat(t[None, :], starts, axis=0).astype(np.float32)
-        for it in range(1, iters + 1):
-            _, _, gx = sur.net.loss_grad(X, T, w_out=w, params=False, inputs=True)
-            g = gx * free
-            m1 = 0.9 * m1 + 0.1 * g
-            m2 = 0.999 * m2 + 0.001 * g * g
-            X -= lr * (m1 / (1 - 0.9 ** it)) / (np.sqrt(m2 / (1 - 0.999 ** it)) + 1e-8)
-            X = np.clip(X, -1.0, 1.0)
-        Y = sur.net.forward(X) * sur.ysd + sur.ymu
-        err = np.array([sum(fit_error(y, y_target)) for y in Y])
-        i = int(np.argmin(err))
+    for j, lev in enumerate(levels):
+        i = j * starts + int(np.argmin(err[j * starts:(j + 1) * starts]))
         Pfit = (X[i] + 1.0) / 2.0 * (PARAM_HI - PARAM_LO) + PARAM_LO
         Pfit[3], Pfit[1] = lev, 2.0 ** (lev - 1)
         best.append((err[i], Pfit))
@@ -230,21 +232,31 @@ def inverse_fit(sur, y_target, starts=64, iters=300, lr=0.05, seed=0):
     return [b[1] for b in best]
 
 
-def refine_with_generator(cands, y_target, seed_eval, runs, N=64, ens=None, seed=5, rounds_per_shrink=2):
+def within(e, tol=0.02):
+    """A fit is within tol when both its spectrum and its flatness error are."""
+    return max(e) <= tol
+
+
+def refine_with_generator(cands, y_target, seed_eval, runs, N=64, ens=None, seed=5, rounds_per_shrink=2,
+                          tol=None, t0=None):
     """Generator-judged search from starting candidates: the candidates are run, then the
     remaining runs perturb the best one's continuous parameters (H, density, circulation
     exponent; the level count stays) in batches of 4 with a radius that shrinks by 0.7 every
-    `rounds_per_shrink` batches, keeping improvements.  Returns (params, (errE, errF), runs)."""
+    `rounds_per_shrink` batches, keeping improvements.  With `tol`, the search stops as soon
+    as the best fit is within tol.  Returns (params, (errE, errF), runs, trace) where trace
+    lists (runs, seconds since t0, best errE + errF, within tol) after every batch."""
+    t0 = time.perf_counter() if t0 is None else t0
     rng = np.random.default_rng(seed)
     P = np.array(cands, dtype=np.float64)
     Y, _ = generate(P, [seed_eval] * len(P), N=N, ens=ens)
-    errs = [sum(fit_error(y, y_target)) for y in Y]
-    i = int(np.argmin(errs))
-    best, best_e, best_y = P[i].copy(), errs[i], Y[i]
+    fe = [fit_error(y, y_target) for y in Y]
+    i = int(np.argmin([sum(e) for e in fe]))
+    best, best_fe, best_y = P[i].copy(), fe[i], Y[i]
     used = len(P)
+    trace = [(used, time.perf_counter() - t0, sum(best_fe), within(best_fe, tol or 0.02))]
     span = PARAM_HI - PARAM_LO
     radius, rnd = 0.15, 0
-    while used < runs:
+    while used < runs and not (tol is not None and within(best_fe, tol)):
         k = min(4, runs - used)
         Q = np.repeat(best[None, :], k, axis=0)
         for j in (0, 2, 4):
@@ -252,28 +264,31 @@ def refine_with_generator(cands, y_target, seed_eval, runs, N=64, ens=None, seed
         Yq, _ = generate(Q, [seed_eval] * k, N=N, ens=ens)
         used += k
         for q, y in zip(Q, Yq):
-            e = sum(fit_error(y, y_target))
-            if e < best_e:
-                best, best_e, best_y = q.copy(), e, y
+            e = fit_error(y, y_target)
+            if sum(e) < sum(best_fe):
+                best, best_fe, best_y = q.copy(), e, y
+        trace.append((used, time.perf_counter() - t0, sum(best_fe), within(best_fe, tol or 0.02)))
         rnd += 1
         if rnd % rounds_per_shrink == 0:
             radius *= 0.7
-    return best, fit_error(best_y, y_target), used
+    return best, best_fe, used, trace
 
 
-def fit_surrogate_driven(sur, y_target, seed_eval, runs, N=64, ens=None):
-    """The network's best parameters for each level count start the generator-judged search."""
+def fit_surrogate_driven(sur, y_target, seed_eval, runs, N=64, ens=None, tol=None):
+    """The network's best parameters for each level count start the generator-judged search.
+    Returns (params, (errE, errF), seconds, runs, trace); the network's time is in both."""
     t0 = time.perf_counter()
-    p, e, used = refine_with_generator(inverse_fit(sur, y_target), y_target, seed_eval, runs, N=N, ens=ens)
-    return p, e, time.perf_counter() - t0, used
+    p, e, used, trace = refine_with_generator(inverse_fit(sur, y_target), y_target, seed_eval, runs, N=N,
+                                              ens=ens, tol=tol, t0=t0)
+    return p, e, time.perf_counter() - t0, used, trace
 
 
-def fit_generator_only(y_target, seed_eval, runs, N=64, ens=None, seed=1):
+def fit_generator_only(y_target, seed_eval, runs, N=64, ens=None, seed=1, tol=None):
     """The method without the network: one random draw per level count starts the same
     generator-judged search."""
     t0 = time.perf_counter()
     P = draw_params(np.random.default_rng(seed), 3)
     P[:, 3] = [2.0, 3.0, 4.0]
     P[:, 1] = 2.0 ** (P[:, 3] - 1)
-    p, e, used = refine_with_generator(list(P), y_target, seed_eval, runs, N=N, ens=ens)
-    return p, e, time.perf_counter() - t0, used
+    p, e, used, trace = refine_with_generator(list(P), y_target, seed_eval, runs, N=N, ens=ens, tol=tol, t0=t0)
+    return p, e, time.perf_counter() - t0, used, trace

@@ -93,4 +93,5 @@ def test_surrogate_learns_the_generator_and_fits_held_out_targets(fwt):
     for f in line["fits"]:
         s, m = f["surrogate"], f["training_mean"]
         assert s["runs"] <= 16 and f["generator_only"]["runs"] <= 16
+        assert s["wall_s_to_common"] <= s["wall_s"]
         assert s["err_logE"] + s["err_flat"] < m["err_logE"] + m["err_flat"], f
