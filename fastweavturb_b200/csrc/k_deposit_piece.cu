@@ -13,8 +13,11 @@
 // section's quintic Taylor-shifted to the piece start, the planes (normal, offset), per sample
 // the offset of the box origin in that sample's own frame, and per chord the spline slope,
 // Rtube^2 and the chord's own box.  Pieces are binned into tiles like sub-segments; the kernel
-// stages a warp's pieces with bulk asynchronous copies, scans every point of piece box x tile
-// against the planes, queues the accepted (point, chord) pairs and evaluates them 32 at a time
+// stages a warp's pieces with bulk asynchronous copies and gives each lane one chord: the rows
+// of the chord's box within the tile (along the axis best aligned with the chord) are spread
+// over the lanes, each row's index interval that can pass the chord's two planes and its
+// cylinder is solved in closed form, and only the points of that interval take the
+// reference's tests.  The accepted (point, chord) pairs are queued and evaluated 32 at a time
 // with the vorticity code of the sub-segment kernel, into the same int64 fixed-point cells.
 #include <cstdio>
 #include <cstdlib>
@@ -308,8 +311,9 @@ __device__ __forceinline__ void for_each_tile(const PieceRec &S, int N, F &&f)
 }
 
 // ------------------------------------------------------------------------------ deposit
-constexpr int kPChunk = 8;        // pieces staged per warp chunk
+constexpr int kPChunk = 4;        // pieces staged per warp chunk: 32 chords, one per lane
 constexpr int kPQueue = 64;       // accepted (point, chord) queue of a warp
+static_assert(kPChunk * kPieceMax == 32, "one chord per lane");
 
 // A piece's box clipped to the tile (one periodic image).
 struct PBox {
@@ -321,9 +325,24 @@ struct PBox {
     int pad[2];
 };
 
+// Rows of one chord's box clipped to the tile, along the axis best aligned with the chord; the
+// box is in offsets from the piece's box origin (the piece kernel's rx, ry, rz).
+struct ChordRows {
+    int o[3];       // clipped box origin
+    int n[3];       // clipped box extent
+    int axis, nb;   // walk axis; rows per column (extent along (axis+1)%3)
+    float rnb;      // (1 + 1e-6) / nb
+    float isa;      // 1 / (dx n_j[axis])
+    float isb;      // 1 / (dx n_{j+1}[axis]), 0 when |n_{j+1}[axis]| <= 0.05 (no bound from it)
+    float q2, i2q;  // dx^2 (1 - n_j[axis]^2) (0: no cylinder bound) and 1 / (2 q2)
+    int pad[3];
+};
+
 struct PieceStage {
     PieceRec rec[kPChunk];
     PBox box[kPChunk];
+    ChordRows cr[32];
+    uint32_t cq[kPQueue];  // candidate points: chord lane | x << 5 | y << 9 | z << 12 (tile-local)
     uint32_t q[kPQueue];   // piece | chord << 3 | x << 6 | y << 10 | z << 13 (tile-local)
     uint64_t bar;
     uint64_t pad;
@@ -347,6 +366,39 @@ __device__ __forceinline__ void pclip(const PieceRec &R, uint32_t img, int N, in
     B.vol = nonempty ? B.n[0] * B.n[1] * B.n[2] : 0;
     B.inx = nonempty ? 1.000001f / (float)B.n[0] : 0.0f;
     B.inxy = nonempty ? 1.000001f / (float)(B.n[0] * B.n[1]) : 0.0f;
+}
+
+// The reference's acceptance of mesh point (rx, ry, rz) (offsets from the piece's box origin)
+// by chord j (tube.f90:806-818): t_j >= 0 and t_{j+1} < 0, tested in the piece frame and,
+// within the rounding band of a plane, again in that sample's own frame; then the distance to
+// chord line j below Rtube, in the chord's frame.  The caller keeps the point in chord j's box.
+__device__ __forceinline__ bool piece_accepts(const PieceRec &R, int j, int rx, int ry, int rz)
+{
+    const float dxv = fmaf((float)rx, R.dx, R.off[0]);
+    const float dyv = fmaf((float)ry, R.dx, R.off[1]);
+    const float dzv = fmaf((float)rz, R.dx, R.off[2]);
+    bool pass = true;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const float4 pl = R.pl[j + h];
+        float tk = fmaf(dzv, pl.z, fmaf(dyv, pl.y, fmaf(dxv, pl.x, -pl.w)));
+        if (fabsf(tk) < R.guard) {
+            const float4 po = R.po[j + h];
+            const float ex = fmaf((float)rx, R.dx, po.x);
+            const float ey = fmaf((float)ry, R.dx, po.y);
+            const float ez = fmaf((float)rz, R.dx, po.z);
+            tk = fmaf(ez, pl.z, fmaf(ey, pl.y, ex * pl.x));
+        }
+        pass = pass && (h == 0 ? tk >= 0.0f : !(tk >= 0.0f));
+    }
+    if (!pass) return false;
+    const float4 cp = R.po[j], pn = R.pl[j];
+    const float ex = fmaf((float)rx, R.dx, cp.x);
+    const float ey = fmaf((float)ry, R.dx, cp.y);
+    const float ez = fmaf((float)rz, R.dx, cp.z);
+    const float t0 = fmaf(ez, pn.z, fmaf(ey, pn.y, ex * pn.x));
+    const float r2 = fmaf(-t0, t0, fmaf(ez, ez, fmaf(ey, ey, ex * ex)));
+    return r2 < R.chq[j].y;
 }
 
 // Evaluate the first `cnt` queued (point, chord) pairs, one per lane, into the tile cells.
@@ -387,11 +439,40 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
     qn = rem;
 }
 
-// One CTA per tile.  Each warp claims chunks of kPChunk pieces, stages their records with one
-// bulk asynchronous copy each, then scans the points of every piece box x tile, 32 at a time
-// across the lanes: the plane scan gives the chords whose slab holds the point, the chord's
-// box and the cylinder test (tube.f90:793-818) decide, and the accepted pairs are queued and
-// evaluated 32 at a time.
+// Test the first `cnt` candidate points, one per lane (piece_accepts), queue the accepted
+// (point, chord) pairs, drop the candidates and evaluate the queue when it holds 32 pairs.
+template <bool General>
+__device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[kAccN], int lane, int cnt, int &cn,
+                                                int &qn, float fscale, float fmaxq, int *__restrict__ err)
+{
+    bool ok = false;
+    uint32_t code = 0u;
+    if (lane < cnt) {
+        const uint32_t e = S.cq[lane];
+        const int c = (int)(e & 31u), k = c >> 3, j = c & 7;
+        const int lx = (int)((e >> 5) & 15u), ly = (int)((e >> 9) & 7u), lz = (int)(e >> 12);
+        const PBox &B = S.box[k];
+        ok = piece_accepts(S.rec[k], j, lx + B.dl[0], ly + B.dl[1], lz + B.dl[2]);
+        code = (uint32_t)k | ((uint32_t)j << 3) | ((uint32_t)lx << 6) | ((uint32_t)ly << 10) | ((uint32_t)lz << 13);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+    if (ok) S.q[qn + __popc(bal & ((1u << lane) - 1u))] = code;
+    qn += __popc(bal);
+    const int rem = cn - cnt;
+    const uint32_t keep = lane < rem ? S.cq[cnt + lane] : 0u;
+    __syncwarp();
+    if (lane < rem) S.cq[lane] = keep;
+    __syncwarp();
+    cn = rem;
+    if (qn >= 32) drain_pieces<General>(S, acc, lane, 32, qn, fscale, fmaxq, err);
+}
+
+// One CTA per tile.  Each warp claims chunks of kPChunk pieces (32 chords), stages their
+// records with one bulk asynchronous copy each, then walks the rows of the chords' boxes within
+// the tile, one row per lane: the row's candidate interval, then per candidate point the
+// reference's tests (tube.f90:793-818: t_j >= 0, t_{j+1} < 0, distance to chord line j below
+// Rtube) with the plane tests in the piece frame and, within the rounding band of a plane, in
+// that sample's own frame.  Accepted pairs are queued and evaluated 32 at a time.
 template <bool General, bool Accumulate>
 __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
     const PieceRec *__restrict__ rec, int N, int ntx, int nty, const int64_t *__restrict__ tile_off,
@@ -431,106 +512,143 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
             break;
         }
         phase ^= 1u;
-        int vol = 0;
         if (lane < nc) {
             PBox B;
             pclip(S.rec[lane], v >> 26, N, x0, y0, z0, B);
             S.box[lane] = B;
-            vol = B.vol;
         }
-        int incl = vol;
+        __syncwarp();
+        // lane = (piece k, chord j): chord j's box clipped to the tile and its rows
+        int nrows = 0;
+        {
+            const int k = lane >> 3, j = lane & 7;
+            if (k < nc && j < S.rec[k].nch && S.box[k].vol > 0) {
+                const PieceRec &R = S.rec[k];
+                const PBox &B = S.box[k];
+                const uint32_t blo = __float_as_uint(R.chq[j].z), bhi = __float_as_uint(R.chq[j].w);
+                ChordRows C;
+                bool nonempty = true;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const int tlo = B.lo[d] + B.dl[d], thi = tlo + B.n[d] - 1;   // the tile part of the piece box
+                    const int lo = max(tlo, unpack3(blo, d)), hi = min(thi, unpack3(bhi, d));
+                    C.o[d] = lo;
+                    C.n[d] = max(0, hi - lo + 1);
+                    nonempty = nonempty && C.n[d] > 0;
+                }
+                const float4 pj = R.pl[j], pk = R.pl[j + 1];
+                const float ax = fabsf(pj.x), ay = fabsf(pj.y), az = fabsf(pj.z);
+                const int a = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+                C.axis = a;
+                const int nbv = a == 0 ? C.n[1] : (a == 1 ? C.n[2] : C.n[0]);
+                const int ncv = a == 0 ? C.n[2] : (a == 1 ? C.n[0] : C.n[1]);
+                C.nb = nbv;
+                C.rnb = nonempty ? 1.000001f / (float)nbv : 0.0f;
+                const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
+                const float tb = a == 0 ? pk.x : (a == 1 ? pk.y : pk.z);
+                C.isa = 1.0f / (R.dx * ta);
+                C.isb = fabsf(tb) > 0.05f ? 1.0f / (R.dx * tb) : 0.0f;
+                const float q2 = R.dx * R.dx * (1.0f - ta * ta);
+                C.q2 = q2 > 0.01f * R.dx * R.dx ? q2 : 0.0f;
+                C.i2q = C.q2 > 0.0f ? 0.5f / C.q2 : 0.0f;
+                S.cr[lane] = C;
+                nrows = nonempty ? nbv * ncv : 0;
+            }
+        }
+        int incl = nrows;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int t = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += t;
         }
-        const int voff = incl - vol;
-        const int total = __shfl_sync(0xffffffffu, incl, kPChunk - 1);
+        const int roff = incl - nrows;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
         __syncwarp();
+        // Rows, one per lane: the index interval where the row can pass chord j's two planes
+        // and its cylinder (with a 0.05-point margin and Rtube^2 widened by 2e-3, far above the
+        // FP32 rounding of the bounds); its points join the candidate queue, which is tested
+        // 32 at a time.
+        int cn = 0;   // queued candidates (warp-uniform)
         for (int r0 = 0; r0 < total; r0 += 32) {
             const int r = r0 + lane;
-            int k = 0;
+            int c = 0;   // chord lane of row r: last lane whose first row is <= r
 #pragma unroll
-            for (int step = kPChunk / 2; step > 0; step >>= 1) {
-                const int t = k + step;
-                const int ot = __shfl_sync(0xffffffffu, voff, t);
-                if (t < nc && ot <= r) k = t;
+            for (int step = 16; step > 0; step >>= 1) {
+                const int t = c + step;
+                const int ot = __shfl_sync(0xffffffffu, roff, t);
+                if (ot <= r) c = t;
             }
-            const int rk = __shfl_sync(0xffffffffu, voff, k);
-            uint32_t amask = 0u;   // accepted chords of this lane's point
-            int lx = 0, ly = 0, lz = 0;
+            const int rc = __shfl_sync(0xffffffffu, roff, c);
+            int i = 1, ihi = 0, a = 0, lx = 0, ly = 0, lz = 0;
             if (r < total) {
-                const PBox &B = S.box[k];
+                const int k = c >> 3, j = c & 7;
+                const ChordRows &C = S.cr[c];
                 const PieceRec &R = S.rec[k];
-                const int li = r - rk;
-                const int nxy = B.n[0] * B.n[1];
-                int iz = (int)((float)li * B.inxy);
-                if (iz * nxy > li) --iz;
-                else if ((iz + 1) * nxy <= li) ++iz;
-                const int rxy = li - iz * nxy;
-                int iy = (int)((float)rxy * B.inx);
-                if (iy * B.n[0] > rxy) --iy;
-                else if ((iy + 1) * B.n[0] <= rxy) ++iy;
-                const int ix = rxy - iy * B.n[0];
-                lx = B.lo[0] + ix;
-                ly = B.lo[1] + iy;
-                lz = B.lo[2] + iz;
-                const int rx = lx + B.dl[0], ry = ly + B.dl[1], rz = lz + B.dl[2];   // offsets from box_lo
-                const float dxv = fmaf((float)rx, R.dx, R.off[0]);
-                const float dyv = fmaf((float)ry, R.dx, R.off[1]);
-                const float dzv = fmaf((float)rz, R.dx, R.off[2]);
-                const int nch = R.nch;
-                // plane scan: bit k of sgn = (t_k >= 0), in the piece frame; a point within the
-                // rounding band of a plane is re-tested in that sample's own frame
-                uint32_t sgn = 0u;
-                const float guard = R.guard;
-                for (int kk = 0; kk <= nch; ++kk) {
-                    const float4 pl = R.pl[kk];
-                    float tk = fmaf(dzv, pl.z, fmaf(dyv, pl.y, fmaf(dxv, pl.x, -pl.w)));
-                    if (fabsf(tk) < guard) {
-                        const float4 po = R.po[kk];
-                        const float ex = fmaf((float)rx, R.dx, po.x);
-                        const float ey = fmaf((float)ry, R.dx, po.y);
-                        const float ez = fmaf((float)rz, R.dx, po.z);
-                        tk = fmaf(ez, pl.z, fmaf(ey, pl.y, ex * pl.x));
+                const PBox &B = S.box[k];
+                a = C.axis;
+                const int rr = r - rc;
+                int jc = (int)((float)rr * C.rnb);
+                if (jc * C.nb > rr) --jc;
+                const int jb = rr - jc * C.nb;
+                const int bx = C.o[0] + (a == 0 ? 0 : (a == 1 ? jc : jb));
+                const int by = C.o[1] + (a == 0 ? jb : (a == 1 ? 0 : jc));
+                const int bz = C.o[2] + (a == 0 ? jc : (a == 1 ? jb : 0));
+                lx = bx - B.dl[0];
+                ly = by - B.dl[1];
+                lz = bz - B.dl[2];
+                const float4 pj = R.pl[j], pk = R.pl[j + 1], oj = R.po[j], ok1 = R.po[j + 1];
+                // row base relative to sample j and to sample j + 1
+                const float ex = fmaf((float)bx, R.dx, oj.x), ey = fmaf((float)by, R.dx, oj.y),
+                            ez = fmaf((float)bz, R.dx, oj.z);
+                const float T0 = fmaf(ez, pj.z, fmaf(ey, pj.y, ex * pj.x));
+                const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
+                const int na = a == 0 ? C.n[0] : (a == 1 ? C.n[1] : C.n[2]);
+                float lo = -2.0f, hi = (float)na + 1.0f;
+                const float r0f = -T0 * C.isa;          // t_j >= 0
+                if (ta > 0.0f) lo = fmaxf(lo, r0f);
+                else hi = fminf(hi, r0f);
+                if (C.isb != 0.0f) {                     // t_{j+1} < 0
+                    const float fx = fmaf((float)bx, R.dx, ok1.x), fy = fmaf((float)by, R.dx, ok1.y),
+                                fz = fmaf((float)bz, R.dx, ok1.z);
+                    const float T1 = fmaf(fz, pk.z, fmaf(fy, pk.y, fx * pk.x));
+                    const float r1f = -T1 * C.isb;
+                    if (C.isb > 0.0f) hi = fminf(hi, r1f);
+                    else lo = fmaxf(lo, r1f);
+                }
+                if (C.q2 > 0.0f) {                       // rho^2 < Rtube^2 about chord line j
+                    const float ea = a == 0 ? ex : (a == 1 ? ey : ez);
+                    const float e2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+                    const float Q1 = 2.0f * R.dx * (ea - T0 * ta);
+                    const float Q0 = e2 - T0 * T0;
+                    const float R2w = fmaf(R.chq[j].y, 1.002f, 1e-6f * e2);
+                    const float disc = Q1 * Q1 - 4.0f * C.q2 * (Q0 - R2w);
+                    if (disc < 0.0f) {
+                        hi = -3.0f;
+                    } else {
+                        const float sq = sqrtf(disc);
+                        lo = fmaxf(lo, (-Q1 - sq) * C.i2q);
+                        hi = fminf(hi, (-Q1 + sq) * C.i2q);
                     }
-                    sgn |= (tk >= 0.0f ? 1u : 0u) << kk;
                 }
-                uint32_t cand = sgn & ~(sgn >> 1) & ((1u << nch) - 1u);
-                while (cand) {
-                    const int j = __ffs(cand) - 1;
-                    cand &= cand - 1u;
-                    const float4 cp = R.po[j], cq = R.chq[j], pn = R.pl[j];
-                    const uint32_t blo = __float_as_uint(cq.z), bhi = __float_as_uint(cq.w);
-                    if (rx < unpack3(blo, 0) || rx > unpack3(bhi, 0) || ry < unpack3(blo, 1) || ry > unpack3(bhi, 1) ||
-                        rz < unpack3(blo, 2) || rz > unpack3(bhi, 2))
-                        continue;
-                    // distance to chord line j (tube.f90:806-818), in the chord's frame
-                    const float ex = fmaf((float)rx, R.dx, cp.x);
-                    const float ey = fmaf((float)ry, R.dx, cp.y);
-                    const float ez = fmaf((float)rz, R.dx, cp.z);
-                    const float t0 = fmaf(ez, pn.z, fmaf(ey, pn.y, ex * pn.x));
-                    const float r2 = fmaf(-t0, t0, fmaf(ez, ez, fmaf(ey, ey, ex * ex)));
-                    if (r2 < cq.y) amask |= 1u << j;
-                }
+                i = max(0, (int)ceilf(lo - 0.05f));
+                ihi = min(na - 1, (int)floorf(hi + 0.05f));
             }
-            // queue the accepted pairs (a point may pass for more than one chord)
-            while (__any_sync(0xffffffffu, amask != 0u)) {
-                const bool ok = amask != 0u;
+            while (__any_sync(0xffffffffu, i <= ihi)) {
+                const bool has = i <= ihi;
                 uint32_t code = 0u;
-                if (ok) {
-                    const int j = __ffs(amask) - 1;
-                    amask &= amask - 1u;
-                    code = (uint32_t)k | ((uint32_t)j << 3) | ((uint32_t)lx << 6) | ((uint32_t)ly << 10) |
-                           ((uint32_t)lz << 13);
+                if (has) {
+                    code = (uint32_t)c | ((uint32_t)(lx + (a == 0 ? i : 0)) << 5) |
+                           ((uint32_t)(ly + (a == 1 ? i : 0)) << 9) | ((uint32_t)(lz + (a == 2 ? i : 0)) << 12);
+                    ++i;
                 }
-                const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                if (ok) S.q[qn + __popc(bal & ((1u << lane) - 1u))] = code;
-                qn += __popc(bal);
+                const unsigned bal = __ballot_sync(0xffffffffu, has);
+                if (has) S.cq[cn + __popc(bal & ((1u << lane) - 1u))] = code;
+                cn += __popc(bal);
                 __syncwarp();
-                if (qn >= 32) drain_pieces<General>(S, acc, lane, 32, qn, fscale, fmaxq, err);
+                if (cn >= 32) test_candidates<General>(S, acc, lane, 32, cn, qn, fscale, fmaxq, err);
             }
         }
+        if (cn > 0) test_candidates<General>(S, acc, lane, cn, cn, qn, fscale, fmaxq, err);
         if (qn > 0) drain_pieces<General>(S, acc, lane, qn, qn, fscale, fmaxq, err);
         __syncwarp();   // the warp's stage is reused by its next chunk
         int nxt = 0;
