@@ -327,27 +327,39 @@ struct PBox {
 
 // Rows of one chord's box clipped to the tile, along the axis best aligned with the chord; the
 // box is in offsets from the piece's box origin (the piece kernel's rx, ry, rz).
-struct ChordRows {
-    int o[3];       // clipped box origin
-    int n[3];       // clipped box extent
-    int axis, nb;   // walk axis; rows per column (extent along (axis+1)%3)
-    float rnb;      // (1 + 1e-6) / nb
-    float isa;      // 1 / (dx n_j[axis])
-    float isb;      // 1 / (dx n_{j+1}[axis]), 0 when |n_{j+1}[axis]| <= 0.05 (no bound from it)
-    float q2, i2q;  // dx^2 (1 - n_j[axis]^2) (0: no cylinder bound) and 1 / (2 q2)
-    int pad[3];
+// The rows of a column (fixed offset along c = (axis+2)%3) are those inside the projection
+// along the axis of the part of chord j's cylinder that the chord can accept: points
+// S_j + t n + v with |v| < Rtube, v . n = 0 and 0 <= t < l + Rtube tan(theta) (theta: the
+// angle between planes j and j + 1; plane j + 1 passes through S_j + l n).  That projection is
+// the projected disk (semi-axes Rtube across n_bc and Rtube |n_a| along it) swept along n_bc,
+// inside the disk's ellipse about the sweep's midpoint scaled by 1 + sweep / (2 minor axis).
+constexpr int kMaxCol = 12;
+struct ChordRows {          // lane-major (one entry per chord lane): conflict-free stores
+    uint16_t o[3][32];      // clipped box origin
+    uint8_t n[3][32];       // clipped box extent (at most a tile's)
+    uint8_t axis[32], nb[32];   // walk axis; rows per column (extent along (axis+1)%3)
+    uint8_t ncol[32];       // columns with their own row ranges (0: every row of the box)
+    uint8_t pad[32];
+    float rnb[32];          // (1 + 1e-6) / nb  (every row of the box)
+    float isa[32];          // 1 / (dx n_j[axis])
+    float isb[32];          // 1 / (dx n_{j+1}[axis]), 0 when |n_{j+1}[axis]| <= 0.05 (no bound from it)
+    float q2[32], i2q[32];  // dx^2 (1 - n_j[axis]^2) (0: no cylinder bound) and 1 / (2 q2)
+    uint16_t col[kMaxCol][32];  // column jc: first row of the column | first b offset << 8
 };
 
 struct PieceStage {
     PieceRec rec[kPChunk];
     PBox box[kPChunk];
-    ChordRows cr[32];
+    ChordRows cr;
     uint32_t cq[kPQueue];  // candidate points: chord lane | x << 5 | y << 9 | z << 12 (tile-local)
     uint32_t q[kPQueue];   // piece | chord << 3 | x << 6 | y << 10 | z << 13 (tile-local)
     uint64_t bar;
     uint64_t pad;
 };
 constexpr size_t kPieceSmem = kAccBytes + sizeof(PieceStage) * kDepWarps;
+// three blocks per SM (the register budget allows three as well): the kernel hides the
+// latency of its record copies with the other blocks' warps
+static_assert(3 * (kPieceSmem + 1024) <= 228 * 1024, "deposit_piece_kernel: three blocks per SM");
 
 __device__ __forceinline__ void pclip(const PieceRec &R, uint32_t img, int N, int tx0, int ty0, int tz0, PBox &B)
 {
@@ -526,33 +538,83 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
                 const PieceRec &R = S.rec[k];
                 const PBox &B = S.box[k];
                 const uint32_t blo = __float_as_uint(R.chq[j].z), bhi = __float_as_uint(R.chq[j].w);
-                ChordRows C;
+                ChordRows &C = S.cr;
                 bool nonempty = true;
+                int co[3], cnn[3];
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     const int tlo = B.lo[d] + B.dl[d], thi = tlo + B.n[d] - 1;   // the tile part of the piece box
                     const int lo = max(tlo, unpack3(blo, d)), hi = min(thi, unpack3(bhi, d));
-                    C.o[d] = lo;
-                    C.n[d] = max(0, hi - lo + 1);
-                    nonempty = nonempty && C.n[d] > 0;
+                    co[d] = lo;
+                    cnn[d] = max(0, hi - lo + 1);
+                    C.o[d][lane] = (uint16_t)lo;
+                    C.n[d][lane] = (uint8_t)cnn[d];
+                    nonempty = nonempty && cnn[d] > 0;
                 }
                 const float4 pj = R.pl[j], pk = R.pl[j + 1];
                 const float ax = fabsf(pj.x), ay = fabsf(pj.y), az = fabsf(pj.z);
                 const int a = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
-                C.axis = a;
-                const int nbv = a == 0 ? C.n[1] : (a == 1 ? C.n[2] : C.n[0]);
-                const int ncv = a == 0 ? C.n[2] : (a == 1 ? C.n[0] : C.n[1]);
-                C.nb = nbv;
-                C.rnb = nonempty ? 1.000001f / (float)nbv : 0.0f;
+                C.axis[lane] = (uint8_t)a;
+                const int nbv = a == 0 ? cnn[1] : (a == 1 ? cnn[2] : cnn[0]);
+                const int ncv = a == 0 ? cnn[2] : (a == 1 ? cnn[0] : cnn[1]);
+                C.nb[lane] = (uint8_t)nbv;
+                C.rnb[lane] = nonempty ? 1.000001f / (float)nbv : 0.0f;
                 const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
                 const float tb = a == 0 ? pk.x : (a == 1 ? pk.y : pk.z);
-                C.isa = 1.0f / (R.dx * ta);
-                C.isb = fabsf(tb) > 0.05f ? 1.0f / (R.dx * tb) : 0.0f;
+                C.isa[lane] = 1.0f / (R.dx * ta);
+                C.isb[lane] = fabsf(tb) > 0.05f ? 1.0f / (R.dx * tb) : 0.0f;
                 const float q2 = R.dx * R.dx * (1.0f - ta * ta);
-                C.q2 = q2 > 0.01f * R.dx * R.dx ? q2 : 0.0f;
-                C.i2q = C.q2 > 0.0f ? 0.5f / C.q2 : 0.0f;
-                S.cr[lane] = C;
+                C.q2[lane] = q2 > 0.01f * R.dx * R.dx ? q2 : 0.0f;
+                C.i2q[lane] = q2 > 0.01f * R.dx * R.dx ? 0.5f / q2 : 0.0f;
+                C.ncol[lane] = 0;
                 nrows = nonempty ? nbv * ncv : 0;
+                const float cth = pj.x * pk.x + pj.y * pk.y + pj.z * pk.z;
+                if (nonempty && ncv <= kMaxCol && cth > 0.5f) {
+                    // the chord's sweep and the ellipse of its cross-section, in (b, c)
+                    const float4 oj = R.po[j], ok1 = R.po[j + 1];
+                    const float lx_ = oj.x - ok1.x, ly_ = oj.y - ok1.y, lz_ = oj.z - ok1.z;
+                    const float rt = sqrtf(R.chq[j].y);
+                    const float sweep = sqrtf(lx_ * lx_ + ly_ * ly_ + lz_ * lz_) +
+                                        rt * sqrtf(fmaxf(1.0f - cth * cth, 0.0f)) / cth;
+                    const int b = a == 2 ? 0 : a + 1, cc = a == 0 ? 2 : a - 1;
+                    const float nb_ = b == 0 ? pj.x : (b == 1 ? pj.y : pj.z);
+                    const float nc_ = cc == 0 ? pj.x : (cc == 1 ? pj.y : pj.z);
+                    const float nbc = sqrtf(nb_ * nb_ + nc_ * nc_);
+                    const float wb = nbc > 1e-4f ? nb_ / nbc : 1.0f, wc = nbc > 1e-4f ? nc_ / nbc : 0.0f;
+                    const float Bm = rt * fabsf(ta);
+                    const float f = 1.0f + sweep * nbc / (2.0f * Bm);
+                    const float Ae = fmaf(f * rt, 1.01f, 0.05f * R.dx), Be = fmaf(f * Bm, 1.01f, 0.05f * R.dx);
+                    const float ia2 = 1.0f / (Ae * Ae), ib2 = 1.0f / (Be * Be);
+                    // centre: S_j + (sweep / 2) n, with S_j = -po[j] (mesh-point offsets times dx)
+                    const float sb = -(b == 0 ? oj.x : (b == 1 ? oj.y : oj.z)), sc = -(cc == 0 ? oj.x : (cc == 1 ? oj.y : oj.z));
+                    const float Cb = fmaf(0.5f * sweep, nb_, sb), Cc = fmaf(0.5f * sweep, nc_, sc);
+                    const int ob = b == 0 ? co[0] : (b == 1 ? co[1] : co[2]);
+                    const int oc = cc == 0 ? co[0] : (cc == 1 ? co[1] : co[2]);
+                    const float al = fmaf(wc * wc, ia2, wb * wb * ib2);
+                    const float cross_ = 2.0f * wb * wc * (ib2 - ia2);
+                    const float g2 = fmaf(wb * wb, ia2, wc * wc * ib2);
+                    int rows = 0;
+                    const float idx = 1.0f / R.dx;
+#pragma unroll 1
+                    for (int jc = 0; jc < ncv; ++jc) {
+                        const float z = fmaf((float)(oc + jc), R.dx, -Cc);
+                        const float be = cross_ * z, ga = fmaf(g2 * z, z, -1.0f);
+                        const float disc = fmaf(be, be, -4.0f * al * ga);
+                        int jb0 = 0, nrow = 0;
+                        if (disc >= 0.0f) {
+                            const float sq = sqrtf(disc), i2a = 0.5f / al;
+                            const float y1 = (-be - sq) * i2a, y2 = (-be + sq) * i2a;
+                            const float u1 = fmaf(Cb + y1, idx, -(float)ob), u2 = fmaf(Cb + y2, idx, -(float)ob);
+                            jb0 = max(0, (int)ceilf(fmaxf(u1, -2.0f) - 0.05f));
+                            const int jb1 = min(nbv - 1, (int)floorf(fminf(u2, (float)nbv + 1.0f) + 0.05f));
+                            nrow = max(0, jb1 - jb0 + 1);
+                        }
+                        C.col[jc][lane] = (uint16_t)(rows | (jb0 << 8));
+                        rows += nrow;
+                    }
+                    C.ncol[lane] = (uint8_t)ncv;
+                    nrows = rows;
+                }
             }
         }
         int incl = nrows;
@@ -582,17 +644,29 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
             int i = 1, ihi = 0, a = 0, lx = 0, ly = 0, lz = 0;
             if (r < total) {
                 const int k = c >> 3, j = c & 7;
-                const ChordRows &C = S.cr[c];
+                const ChordRows &C = S.cr;
                 const PieceRec &R = S.rec[k];
                 const PBox &B = S.box[k];
-                a = C.axis;
+                a = C.axis[c];
                 const int rr = r - rc;
-                int jc = (int)((float)rr * C.rnb);
-                if (jc * C.nb > rr) --jc;
-                const int jb = rr - jc * C.nb;
-                const int bx = C.o[0] + (a == 0 ? 0 : (a == 1 ? jc : jb));
-                const int by = C.o[1] + (a == 0 ? jb : (a == 1 ? 0 : jc));
-                const int bz = C.o[2] + (a == 0 ? jc : (a == 1 ? jb : 0));
+                int jc, jb;
+                if (C.ncol[c] > 0) {
+                    // column of row rr: last column whose first row is <= rr (ncol <= 12)
+                    jc = 0;
+#pragma unroll
+                    for (int step = 8; step > 0; step >>= 1) {
+                        const int t = jc + step;
+                        if (t < C.ncol[c] && (int)(C.col[t][c] & 0xffu) <= rr) jc = t;
+                    }
+                    jb = (int)(C.col[jc][c] >> 8) + (rr - (int)(C.col[jc][c] & 0xffu));
+                } else {
+                    jc = (int)((float)rr * C.rnb[c]);
+                    if (jc * C.nb[c] > rr) --jc;
+                    jb = rr - jc * C.nb[c];
+                }
+                const int bx = C.o[0][c] + (a == 0 ? 0 : (a == 1 ? jc : jb));
+                const int by = C.o[1][c] + (a == 0 ? jb : (a == 1 ? 0 : jc));
+                const int bz = C.o[2][c] + (a == 0 ? jc : (a == 1 ? jb : 0));
                 lx = bx - B.dl[0];
                 ly = by - B.dl[1];
                 lz = bz - B.dl[2];
@@ -602,32 +676,32 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
                             ez = fmaf((float)bz, R.dx, oj.z);
                 const float T0 = fmaf(ez, pj.z, fmaf(ey, pj.y, ex * pj.x));
                 const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
-                const int na = a == 0 ? C.n[0] : (a == 1 ? C.n[1] : C.n[2]);
+                const int na = a == 0 ? C.n[0][c] : (a == 1 ? C.n[1][c] : C.n[2][c]);
                 float lo = -2.0f, hi = (float)na + 1.0f;
-                const float r0f = -T0 * C.isa;          // t_j >= 0
+                const float r0f = -T0 * C.isa[c];          // t_j >= 0
                 if (ta > 0.0f) lo = fmaxf(lo, r0f);
                 else hi = fminf(hi, r0f);
-                if (C.isb != 0.0f) {                     // t_{j+1} < 0
+                if (C.isb[c] != 0.0f) {                     // t_{j+1} < 0
                     const float fx = fmaf((float)bx, R.dx, ok1.x), fy = fmaf((float)by, R.dx, ok1.y),
                                 fz = fmaf((float)bz, R.dx, ok1.z);
                     const float T1 = fmaf(fz, pk.z, fmaf(fy, pk.y, fx * pk.x));
-                    const float r1f = -T1 * C.isb;
-                    if (C.isb > 0.0f) hi = fminf(hi, r1f);
+                    const float r1f = -T1 * C.isb[c];
+                    if (C.isb[c] > 0.0f) hi = fminf(hi, r1f);
                     else lo = fmaxf(lo, r1f);
                 }
-                if (C.q2 > 0.0f) {                       // rho^2 < Rtube^2 about chord line j
+                if (C.q2[c] > 0.0f) {                       // rho^2 < Rtube^2 about chord line j
                     const float ea = a == 0 ? ex : (a == 1 ? ey : ez);
                     const float e2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
                     const float Q1 = 2.0f * R.dx * (ea - T0 * ta);
                     const float Q0 = e2 - T0 * T0;
                     const float R2w = fmaf(R.chq[j].y, 1.002f, 1e-6f * e2);
-                    const float disc = Q1 * Q1 - 4.0f * C.q2 * (Q0 - R2w);
+                    const float disc = Q1 * Q1 - 4.0f * C.q2[c] * (Q0 - R2w);
                     if (disc < 0.0f) {
                         hi = -3.0f;
                     } else {
                         const float sq = sqrtf(disc);
-                        lo = fmaxf(lo, (-Q1 - sq) * C.i2q);
-                        hi = fminf(hi, (-Q1 + sq) * C.i2q);
+                        lo = fmaxf(lo, (-Q1 - sq) * C.i2q[c]);
+                        hi = fminf(hi, (-Q1 + sq) * C.i2q[c]);
                     }
                 }
                 i = max(0, (int)ceilf(lo - 0.05f));
