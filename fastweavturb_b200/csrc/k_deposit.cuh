@@ -421,6 +421,6 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out);
 // Lines whose truncation radius Rtube_ratio * sigma_max is at most this many grid spacings go
 // through the piece kernel; thicker tubes through the sub-segment kernel, whose analytic
 // row intervals skip most of a large box.
-constexpr double kPieceMaxRtCells = 2.5;
+constexpr double kPieceMaxRtCells = 8.0;
 
 }  // namespace fwt

@@ -333,7 +333,7 @@ struct PBox {
 // angle between planes j and j + 1; plane j + 1 passes through S_j + l n).  That projection is
 // the projected disk (semi-axes Rtube across n_bc and Rtube |n_a| along it) swept along n_bc,
 // inside the disk's ellipse about the sweep's midpoint scaled by 1 + sweep / (2 minor axis).
-constexpr int kMaxCol = 12;
+constexpr int kMaxCol = 16;   // a tile is at most 16 points wide
 struct ChordRows {          // lane-major (one entry per chord lane): conflict-free stores
     uint16_t o[3][32];      // clipped box origin
     uint8_t n[3][32];       // clipped box extent (at most a tile's)
@@ -344,7 +344,7 @@ struct ChordRows {          // lane-major (one entry per chord lane): conflict-f
     float isa[32];          // 1 / (dx n_j[axis])
     float isb[32];          // 1 / (dx n_{j+1}[axis]), 0 when |n_{j+1}[axis]| <= 0.05 (no bound from it)
     float q2[32], i2q[32];  // dx^2 (1 - n_j[axis]^2) (0: no cylinder bound) and 1 / (2 q2)
-    uint16_t col[kMaxCol][32];  // column jc: first row of the column | first b offset << 8
+    uint16_t col[kMaxCol][32];  // column jc: first row of the column | first b offset << 12
 };
 
 struct PieceStage {
@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
                             const int jb1 = min(nbv - 1, (int)floorf(fminf(u2, (float)nbv + 1.0f) + 0.05f));
                             nrow = max(0, jb1 - jb0 + 1);
                         }
-                        C.col[jc][lane] = (uint16_t)(rows | (jb0 << 8));
+                        C.col[jc][lane] = (uint16_t)(rows | (jb0 << 12));
                         rows += nrow;
                     }
                     C.ncol[lane] = (uint8_t)ncv;
@@ -651,14 +651,14 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
                 const int rr = r - rc;
                 int jc, jb;
                 if (C.ncol[c] > 0) {
-                    // column of row rr: last column whose first row is <= rr (ncol <= 12)
+                    // column of row rr: last column whose first row is <= rr (ncol <= 16)
                     jc = 0;
 #pragma unroll
                     for (int step = 8; step > 0; step >>= 1) {
                         const int t = jc + step;
-                        if (t < C.ncol[c] && (int)(C.col[t][c] & 0xffu) <= rr) jc = t;
+                        if (t < C.ncol[c] && (int)(C.col[t][c] & 0xfffu) <= rr) jc = t;
                     }
-                    jb = (int)(C.col[jc][c] >> 8) + (rr - (int)(C.col[jc][c] & 0xffu));
+                    jb = (int)(C.col[jc][c] >> 12) + (rr - (int)(C.col[jc][c] & 0xfffu));
                 } else {
                     jc = (int)((float)rr * C.rnb[c]);
                     if (jc * C.nb[c] > rr) --jc;

@@ -21,7 +21,7 @@ import numpy as np
 from .api import Context, Params, sp_exponents, sp_separations
 from .configs import build_workload
 
-TUNE_CANDIDATES = (0.0, 1.5, 2.5, 4.0)
+TUNE_CANDIDATES = (0.0, 2.5, 5.0, 8.0)
 
 
 class Ensemble:

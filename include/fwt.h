@@ -157,7 +157,7 @@ int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
 /* Tuning knobs of the context (no counterpart in the reference).  FWT_TUNE_PIECE_RT_CELLS:
  * lines whose truncation radius Rtube_ratio * sigma_max is at most `value` grid spacings are
  * deposited by the chord-piece kernel, thicker ones by the sub-segment kernel (value < 0
- * restores the default, 2.5).  Results agree within FP32 rounding either way; the choice is
+ * restores the default, 8).  Results agree within FP32 rounding either way; the choice is
  * speed only, and the ensemble autotuner sets it per grid size. */
 #define FWT_TUNE_PIECE_RT_CELLS 1
 int fwt_set_tuning(fwt_ctx *ctx, int key, double value);

@@ -49,11 +49,17 @@ def _masked_rel(a, b, mask):
     return rel_l2(a[m], b[m])
 
 
-@pytest.mark.parametrize("precision,mode,tol", [(32, 0, TOL32), (32, 1, TOL32), (64, 1, TOL64), (64, 0, TOL64)])
-def test_wt2_omega_matches_oracle(fwt, wt2, precision, mode, tol):
+@pytest.mark.parametrize("precision,mode,tol,piece_cells", [(32, 0, TOL32, None), (32, 0, TOL32, 0.0),
+                                                             (32, 1, TOL32, None), (64, 1, TOL64, None),
+                                                             (64, 0, TOL64, None)])
+def test_wt2_omega_matches_oracle(fwt, wt2, precision, mode, tol, piece_cells):
+    """piece_cells 0 sends every line through the sub-segment kernel (by default the WT2 tubes,
+    1.8-7.4 grid spacings thick at 64^3, all take the chord-piece kernel)."""
     p, cl, ref, vor_raw, cond = wt2
     ctx = fwt.Context(_params(fwt, p, precision, mode))
     ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T, p.if_filter)
+    if piece_cells is not None:
+        ctx.set_piece_radius_limit(piece_cells)
     ctx.deposit()
     vor = ctx.field(0)                 # raw (not yet normalised)
     good = cond <= COND_MAX
