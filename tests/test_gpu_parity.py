@@ -136,7 +136,7 @@ def test_partial_tiles(fwt, orc, N, piece_cells):
     sub-segment kernel (piece_cells = 0): omega matches the FP64 oracle on the well-conditioned
     points (curved-branch amplification <= 10) and the spectral path matches on the same omega."""
     from fastweavturb_b200.configs import small
-    w = small(N=N, seed=9, nlev=2, tubes0=2, nodes0=64, sigma0=0.3)
+    w = small(N=N, seed=9, nlev=2, tubes0=2, nodes0=64, sigma0=0.2)
     p, cl = oracle_inputs(orc, w)
     ctx = fwt.Context(gpu_params(fwt, w, precision=32, deposit_mode=0))
     ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
