@@ -53,6 +53,9 @@ class Workload:
     ntf_pre: int = 1000
     Rtube_ratio: float = 3.0
     dzeta_sup: float = 1e-4
+    # True: each level draws its tubes from its own stream (seed, level), so a level's tube
+    # count changes only that level's last tubes; False: one stream numbered across levels
+    level_streams: bool = False
     extra: dict = field(default_factory=dict)
 
     @property
@@ -117,6 +120,7 @@ def ensemble_member(seed, N=None, rng=None):
     w = Workload(f"ensemble member seed={seed}: N={N}, H={H:.3f}, levels={nlev}, density={dens:.2f}, "
                  f"Gamma exponent={gexp:.3f}", N, _levels(nlev, 0.4, 4, 256, H, gexp=gexp, density=dens), seed=seed)
     w.extra = {"H": H, "levels": nlev, "density": dens, "gexp": gexp, "sigma_ratio_levels": 2.0 ** (nlev - 1)}
+    w.level_streams = True
     return w
 
 
@@ -124,13 +128,17 @@ def surrogate_member(params, seed, N=64):
     """A realisation for the learned surrogate from its five inputs (H, sigma_max/sigma_min,
     density multiplier, levels, circulation exponent): the ensemble family of
     ensemble_member with 64 * 2^l nodes per tube (a quarter of the benchmark's, so thousands
-    of realisations fit the training budget) and sigma_max/sigma_min = 2^(levels - 1)."""
+    of realisations fit the training budget) and sigma_max/sigma_min = 2^(levels - 1).  Its
+    levels draw from separate streams, so with the seed fixed the statistics change gradually
+    with the density (tubes are added or removed at the end of a level) and continuously with
+    H and the circulation exponent."""
     H, _, dens, nlev, gexp = params
     nlev = int(round(nlev))
     w = Workload(f"surrogate member seed={seed}: N={N}, H={H:.3f}, levels={nlev}, density={dens:.2f}, "
                  f"Gamma exponent={gexp:.3f}", N, _levels(nlev, 0.4, 4, 64, float(H), gexp=float(gexp),
                                                            density=float(dens)), seed=seed)
     w.extra = {"H": H, "levels": nlev, "density": dens, "gexp": gexp, "sigma_ratio_levels": 2.0 ** (nlev - 1)}
+    w.level_streams = True
     return w
 
 
@@ -140,6 +148,11 @@ def small(N=32, seed=1, nlev=2, tubes0=2, nodes0=64, sigma0=0.4, H=0.7):
 
 
 CONFIGS = {"cfg0": cfg0, "cfg1": cfg1, "cfg2": cfg2}
+
+
+def level_seed(seed, level):
+    """Seed of one level's stream (level_streams workloads): a 64-bit mix of both."""
+    return (seed * 0x9E3779B97F4A7C15 + (level + 1) * 0xBF58476D1CE4E5B9) & 0xFFFFFFFFFFFFFFFF
 
 
 def build_workload(ctx, w: Workload):
@@ -155,8 +168,19 @@ def build_workload(ctx, w: Workload):
     n = w.nnodes
     xyz = torch.empty((3, n), dtype=torch.float64, device=dev)
     tubes, nodes, H, dB = w.gen_arrays()
-    ctx.fbb_generate(w.seed, tubes, nodes, H, dB, xyz[0].data_ptr(), xyz[1].data_ptr(), xyz[2].data_ptr())
-    signs = fbb_signs(w.seed, w.ntubes)
+    if w.level_streams:
+        off, signs = 0, []
+        for l in range(len(tubes)):
+            s = level_seed(w.seed, l)
+            if tubes[l] > 0:
+                ctx.fbb_generate(s, tubes[l:l + 1], nodes[l:l + 1], H[l:l + 1], dB[l:l + 1],
+                                 xyz[0, off:].data_ptr(), xyz[1, off:].data_ptr(), xyz[2, off:].data_ptr())
+                signs.append(fbb_signs(s, int(tubes[l])))
+            off += int(tubes[l]) * int(nodes[l])
+        signs = np.concatenate(signs) if signs else np.zeros(0, dtype=np.int32)
+    else:
+        ctx.fbb_generate(w.seed, tubes, nodes, H, dB, xyz[0].data_ptr(), xyz[1].data_ptr(), xyz[2].data_ptr())
+        signs = fbb_signs(w.seed, w.ntubes)
     npoint, sig, gam, nT = w.line_arrays(signs)
     ctx.set_centerlines_device(npoint, xyz[0].data_ptr(), xyz[1].data_ptr(), xyz[2].data_ptr(), sig, gam, nT)
     return xyz, (npoint, sig, gam, nT)
