@@ -22,6 +22,12 @@ int fail(int code, const std::string &msg)
 int buf_reserve(Ctx *c, DevBuf &b, size_t bytes)
 {
     if (bytes <= b.bytes && b.p) return 0;
+    // a buffer that grows takes 25 % headroom: cudaFree waits for the whole device, which
+    // would stall the other contexts' streams whenever a realisation is slightly larger
+    if (b.p && bytes < b.bytes + b.bytes / 4) {
+        const size_t grown = b.bytes + b.bytes / 4;
+        if (!c->p.mem_cap || c->mem_held - b.bytes + grown <= c->p.mem_cap) bytes = grown;
+    }
     if (b.p) {
         cudaFree(b.p);
         c->mem_held -= b.bytes;

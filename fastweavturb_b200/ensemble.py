@@ -1,10 +1,13 @@
 """Batched ensembles of woven fields on one GPU, and the autotuner of the deposition kernels.
 
 An ensemble is a list of workloads of uneven grid sizes and parameters (configs.
-ensemble_member, configs.surrogate_member).  Ensemble keeps one libfwt context per grid size,
-so the FFT plans and device buffers of a size are made once and reused by every realisation
-of that size; each realisation's centerlines are generated on the device, the field is built
-and its statistics stay on the device until read.
+ensemble_member, configs.surrogate_member).  Ensemble keeps `workers` libfwt contexts per grid
+size, each with its own CUDA stream, so the FFT plans and device buffers of a size are made
+once and reused by every realisation of that size, and up to `workers` realisations are in
+flight at once (one host thread each; the library releases the interpreter during its calls):
+small fields, whose kernels fill a fraction of the GPU and whose phases end in short host
+synchronisations, overlap on the device.  Each realisation's centerlines are generated on the
+device, the field is built and its statistics stay on the device until read.
 
 Autotuner: before the first realisation of a grid size, the deposition of a probe
 realisation is timed with the chord-piece kernel limit at each candidate value (the tube
@@ -14,7 +17,10 @@ field within FP32 rounding; only the speed differs.
 """
 from __future__ import annotations
 
+import queue
+import threading
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -25,19 +31,27 @@ TUNE_CANDIDATES = (0.0, 2.5, 5.0, 8.0)
 
 
 class Ensemble:
-    def __init__(self, device=0, tune=True, Sp_order=6):
+    def __init__(self, device=0, tune=True, Sp_order=6, workers=4):
         self.device = device
         self.tune = tune
         self.Sp_order = Sp_order
+        self.workers = max(1, int(workers))
         self.ctx = {}
         self.tuned = {}
         self.tune_log = {}
+        self._lock = threading.Lock()
 
-    def context(self, N):
-        if N not in self.ctx:
-            self.ctx[N] = Context(Params(N=N, N_downsample=N, line_s=1, line_e=0, sigma_ratio=1.0, device=self.device,
-                                         pdf_bins=201, Sp_order=self.Sp_order, vorticity_output=0))
-        return self.ctx[N]
+    def context(self, N, slot=0):
+        """Context `slot` of grid size N (created on first use, with its own stream)."""
+        with self._lock:
+            key = (N, slot)
+            if key not in self.ctx:
+                self.ctx[key] = Context(Params(N=N, N_downsample=N, line_s=1, line_e=0, sigma_ratio=1.0,
+                                               device=self.device, pdf_bins=201, Sp_order=self.Sp_order,
+                                               vorticity_output=0))
+                if N in self.tuned:
+                    self.ctx[key].set_piece_radius_limit(self.tuned[N])
+            return self.ctx[key]
 
     def _load(self, ctx, w):
         return build_workload(ctx, w)
@@ -57,29 +71,60 @@ class Ensemble:
             torch.cuda.synchronize()
             times[cells] = time.perf_counter() - t0
         best = min(times, key=times.get)
-        ctx.set_piece_radius_limit(best)
+        with self._lock:
+            for (n, _), c in self.ctx.items():
+                if n == w.N:
+                    c.set_piece_radius_limit(best)
         self.tuned[w.N] = best
         self.tune_log[w.N] = times
         del keep
         return best
 
+    def slots_for(self, N):
+        """Contexts kept for grid size N: every worker for small fields, fewer for large ones,
+        whose per-context buffers (records of up to 4 Mi nodes per batch, three N^3 fields)
+        run to gigabytes."""
+        cap = self.workers if N <= 96 else (4 if N <= 128 else 2)
+        return max(1, min(self.workers, cap))
+
     def run(self, members, stats=True):
-        """Build every member; returns (per-member statistics, device seconds, Mpts/s)."""
+        """Build every member, up to `workers` at once; returns (per-member statistics in
+        member order, wall seconds of the build, Mpts/s = sum N^3 / wall)."""
         import torch
-        out = []
-        t_total = 0.0
         for w in members:
-            ctx = self.context(w.N)
             if self.tune and w.N not in self.tuned:
                 self.autotune(w)
-            xyz = self._load(ctx, w)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            ctx.run()
-            torch.cuda.synchronize()
-            t_total += time.perf_counter() - t0
-            out.append(member_statistics(ctx, w.N, self.Sp_order) if stats else None)
-            del xyz
+        torch.cuda.synchronize(self.device)
+        slots = {}
+        for N in sorted({w.N for w in members}):
+            slots[N] = queue.Queue()
+            for k in range(self.slots_for(N)):
+                slots[N].put(k)
+
+        def build(w):
+            torch.cuda.set_device(self.device)
+            slot = slots[w.N].get()
+            try:
+                ctx = self.context(w.N, slot)
+                xyz = self._load(ctx, w)
+                ctx.run()
+                # the statistics are read back on the context's stream: after them no kernel
+                # of this realisation still uses xyz
+                res = member_statistics(ctx, w.N, self.Sp_order) if stats else ctx.cal_helicity()
+                del xyz
+                return res
+            finally:
+                slots[w.N].put(slot)
+
+        t0 = time.perf_counter()
+        if self.workers == 1:
+            out = [build(w) for w in members]
+        else:
+            with ThreadPoolExecutor(max_workers=self.workers) as ex:
+                out = list(ex.map(build, members))
+        t_total = time.perf_counter() - t0
+        if not stats:
+            out = [None] * len(out)
         pts = sum(w.N ** 3 for w in members)
         return out, t_total, pts / t_total / 1e6
 

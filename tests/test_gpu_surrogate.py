@@ -95,3 +95,26 @@ def test_surrogate_learns_the_generator_and_fits_held_out_targets(fwt):
         assert s["runs"] <= 16 and f["generator_only"]["runs"] <= 16
         assert s["wall_s_to_common"] <= s["wall_s"]
         assert s["err_logE"] + s["err_flat"] < m["err_logE"] + m["err_flat"], f
+
+
+def test_concurrent_ensemble_is_deterministic(fwt):
+    """Realisations built four at a time on separate streams give the statistics of the same
+    realisations built one at a time (integer fixed-point deposition, per-context buffers, no
+    shared state between contexts).  The FP64 shell and moment sums are atomics whose order
+    varies from run to run, hence 1e-12 rather than bit equality; a race would show as a
+    difference of order one."""
+    from fastweavturb_b200.configs import surrogate_member
+    from fastweavturb_b200.ensemble import Ensemble
+
+    params = [(0.4 + 0.05 * k, 2.0 ** (2 + k % 2), 1.0 + 0.3 * k, 3 + k % 2, 1.3) for k in range(8)]
+    members = [surrogate_member(p, 100 + k, N=64 if k % 3 else 96) for k, p in enumerate(params)]
+    outs = []
+    for workers in (1, 4):
+        ens = Ensemble(workers=workers, tune=False)
+        stats, secs, rate = ens.run(members)
+        outs.append(stats)
+        ens.close()
+    for a, b in zip(*outs):
+        assert rel_l2(a["Ek"], b["Ek"]) <= 1e-12
+        assert rel_l2(a["Sp"], b["Sp"]) <= 1e-12
+        assert abs(a["up"] - b["up"]) <= 1e-12 * abs(b["up"])
