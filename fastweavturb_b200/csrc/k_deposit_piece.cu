@@ -84,13 +84,17 @@ __global__ void piece_map_kernel(const LineParam *__restrict__ lp, const int *__
 // One thread per piece: FP64 samples, chords and boxes as the sub-segment set-up
 // (tube.f90:703-798), then the FP32 record in the piece's frame.  err bit 8: a piece box
 // wider than 1023 points (the 10-bit chord box offsets).
-__global__ void __launch_bounds__(128) piece_build_kernel(
+__global__ void __launch_bounds__(128, 3) piece_build_kernel(
     const LineParam *__restrict__ lp, const int *__restrict__ slot_line, const int *__restrict__ map, int64_t npieces,
     const double *__restrict__ X, const double *__restrict__ Y, const double *__restrict__ Z,
     const double *__restrict__ cze, int64_t node_base, const double *__restrict__ coe, const int *__restrict__ ntf,
     const double *__restrict__ dtf, const int64_t *__restrict__ poff, int N, double Rtube_ratio, double dzeta_sup,
     double eta, PieceRec *__restrict__ rec, int *__restrict__ err)
 {
+    // the section's 18 coefficients are read by every sample evaluation of both passes: one
+    // global read each into this thread's row of shared memory (rows of 19 doubles spread the
+    // banks), instead of about 20 x 18 global loads that throttled the load/store unit
+    __shared__ double s_cf[128][19];
     const int64_t pc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pc >= npieces) return;
     const int slot = map[pc];
@@ -107,7 +111,9 @@ __global__ void __launch_bounds__(128) piece_build_kernel(
     const double *czl = cze + (P.node_off - node_base);
     const double zl = cze_pl_at(czl, np, t), zl1 = cze_pl_at(czl, np, t + 1);
     const double d = dtf[slot];
-    const double *cf = coe + 18 * (size_t)slot;
+    double *cf = s_cf[threadIdx.x];
+#pragma unroll
+    for (int m = 0; m < 18; ++m) cf[m] = coe[18 * (size_t)slot + m];
     const int inext = (t + 1 < np) ? t + 1 : 0;
     // extended sample k of the section (as the sub-segment set-up: the endpoint copy and the
     // next section's first sample)
