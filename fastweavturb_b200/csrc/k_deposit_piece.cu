@@ -4,21 +4,22 @@
 // accepts a mesh point x when t_j(x) = (x - ci_j) . tci_j >= 0, t_{j+1}(x) < 0 (the next
 // chord's plane) and the distance to chord line j is below Rtube, inside chord j's box.
 // Consecutive chords share their planes (tube.f90:721-723,740-751), so a run of chords of one
-// section can be tested together: one scan of the run's planes per mesh point finds the
-// accepting chords as the sign changes of t_k.  For tubes a few grid spacings thick, where a
-// sub-segment holds only a handful of points but its box and rows cost far more, this cuts
-// the set-up, the binning and the per-point work by the run length.
+// section can share one record: the section's spline, the run's planes and per-sample frames.
+// For tubes up to a few grid spacings thick, where a sub-segment accepts only a handful of
+// points, this cuts the set-up, the binning and the record traffic by the run length.
 //
 // A piece is up to kPieceMax consecutive chords of one section.  Its record holds the
 // section's quintic Taylor-shifted to the piece start, the planes (normal, offset), per sample
 // the offset of the box origin in that sample's own frame, and per chord the spline slope,
 // Rtube^2 and the chord's own box.  Pieces are binned into tiles like sub-segments; the kernel
-// stages a warp's pieces with bulk asynchronous copies and gives each lane one chord: the rows
-// of the chord's box within the tile (along the axis best aligned with the chord) are spread
-// over the lanes, each row's index interval that can pass the chord's two planes and its
-// cylinder is solved in closed form, and only the points of that interval take the
-// reference's tests.  The accepted (point, chord) pairs are queued and evaluated 32 at a time
-// with the vorticity code of the sub-segment kernel, into the same int64 fixed-point cells.
+// stages a warp's pieces with bulk asynchronous copies and gives each lane one chord, whose
+// rows within the tile (along the axis best aligned with the chord) are limited, column by
+// column, to the projection of the part of the chord's cylinder it can accept; the rows are
+// spread over the lanes, each row's index interval that can pass the chord's two planes and
+// its cylinder is solved in closed form, and only the points of that interval take the
+// reference's tests, 32 candidates at a time.  The accepted (point, chord) pairs are queued
+// and evaluated 32 at a time with the vorticity code of the sub-segment kernel, into the same
+// int64 fixed-point cells.
 #include <cstdio>
 #include <cstdlib>
 
@@ -327,8 +328,7 @@ struct PBox {
     int n[3];       // clipped extent
     int dl[3];      // clipped origin relative to the piece's box_lo, minus lo
     int vol;
-    float inx, inxy;   // (1 + 1e-6) / n[0], (1 + 1e-6) / (n[0] n[1])
-    int pad[2];
+    int pad[3];
 };
 
 // Rows of one chord's box clipped to the tile, along the axis best aligned with the chord; the
@@ -357,7 +357,7 @@ struct PieceStage {
     PieceRec rec[kPChunk];
     PBox box[kPChunk];
     ChordRows cr;
-    uint32_t cq[kPQueue];  // candidate points: chord lane | x << 5 | y << 9 | z << 12 (tile-local)
+    uint32_t cq[kPQueue];  // candidates: chord lane (piece << 3 | chord) | x << 5 | y << 9 | z << 12 (tile-local)
     uint32_t q[kPQueue];   // piece | chord << 3 | x << 6 | y << 10 | z << 13 (tile-local)
     uint64_t bar;
     uint64_t pad;
@@ -382,8 +382,6 @@ __device__ __forceinline__ void pclip(const PieceRec &R, uint32_t img, int N, in
         nonempty = nonempty && B.n[d] > 0;
     }
     B.vol = nonempty ? B.n[0] * B.n[1] * B.n[2] : 0;
-    B.inx = nonempty ? 1.000001f / (float)B.n[0] : 0.0f;
-    B.inxy = nonempty ? 1.000001f / (float)(B.n[0] * B.n[1]) : 0.0f;
 }
 
 // The reference's acceptance of mesh point (rx, ry, rz) (offsets from the piece's box origin)
