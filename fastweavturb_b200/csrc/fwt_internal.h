@@ -99,7 +99,7 @@ struct Ctx {
     size_t fft_ws_bytes = 0;
 
     // scratch (centerline set-up, deposition, statistics)
-    DevBuf scratch[24];
+    DevBuf scratch[25];
 
     // state
     bool have_w = false, have_u = false, normalised = false;

@@ -137,7 +137,8 @@ __global__ void section_kernel(const LineParam *__restrict__ lp, const int *__re
                                const double *__restrict__ Z, const double *__restrict__ cze,
                                const double *__restrict__ ck, const double *__restrict__ ckk,
                                const double *__restrict__ Len, int64_t node_base, int ntf_times, int ntf_pre,
-                               double *__restrict__ coe_out, int *__restrict__ ntf_out, double *__restrict__ dtf_out)
+                               double *__restrict__ coe_out, int *__restrict__ ntf_out, double *__restrict__ dtf_out,
+                               unsigned *__restrict__ near)   // near[0]: count, near[4 + i]: marked slots
 {
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -204,52 +205,59 @@ __global__ void section_kernel(const LineParam *__restrict__ lp, const int *__re
     const bool near_step = fmin(fr, 1.0 - fr) < 1e-4 * (xr + 1.0) || !(xr == xr);
     if (lane == 0) {
         const int ntf = near_step ? 0 : (int)ceil(xr) + 1;
+        if (near_step) near[4 + atomicAdd(near, 1u)] = (unsigned)warp;
         ntf_out[warp] = ntf;
         dtf_out[warp] = near_step ? 0.0 : (zr_ - zl) / (1.0 * ntf);
     }
 }
 
-// FP64 turning angle of the sections section_kernel marked (ntf = 0): one warp per slot, the
-// reference's integrand (tube.f90:625-657) in FP64 from the stored coefficients.
+// FP64 turning angle of the sections section_kernel marked (ntf = 0), taken from its list of
+// them (a few per thousand): a fixed grid of warps strides over the list, one section per warp
+// at a time, with the reference's integrand (tube.f90:625-657) in FP64 from the stored
+// coefficients.
 __global__ void section_fp64_kernel(const LineParam *__restrict__ lp, const int *__restrict__ slot_line,
-                                    int64_t nslots, const double *__restrict__ cze, const double *__restrict__ Len,
+                                    const double *__restrict__ cze, const double *__restrict__ Len,
                                     int64_t node_base, int ntf_times, int ntf_pre, const double *__restrict__ coe_all,
-                                    int *__restrict__ ntf_out, double *__restrict__ dtf_out)
+                                    const unsigned *__restrict__ near, int *__restrict__ ntf_out,
+                                    double *__restrict__ dtf_out)
 {
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+    const unsigned count = near[0];
     const int lane = threadIdx.x & 31;
-    if (warp >= nslots || ntf_out[warp] != 0) return;
-    const int l = slot_line[warp];
-    const LineParam P = lp[l];
-    const int t = (int)(warp - P.slot_off);
-    const int np = P.n_sec;
-    const double L = Len[l];
-    const double *cz_line = cze + (P.node_off - node_base);
-    const double zl = cze_pl_at(cz_line, np, t), zr_ = cze_pl_at(cz_line, np, t + 1);
-    const double dtfp = (zr_ - zl) / (1.0 * ntf_pre);
-    const double *coe = coe_all + 18 * (size_t)warp;
-    double th = 0.0;
-    for (int tj = lane; tj <= ntf_pre; tj += 32) {
-        const double s = zl + dtfp * tj;
-        const double z = (s - zl) * L;
-        double dc[3], dd[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            const double *a = coe + 6 * d;
-            dc[d] = (((5.0 * a[5] * z + 4.0 * a[4]) * z + 3.0 * a[3]) * z + 2.0 * a[2]) * z + a[1];
-            dd[d] = ((20.0 * a[5] * z + 12.0 * a[4]) * z + 6.0 * a[3]) * z + 2.0 * a[2];
+    for (unsigned i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < count; i += nwarps) {
+        const int64_t warp = near[4 + i];
+        const int l = slot_line[warp];
+        const LineParam P = lp[l];
+        const int t = (int)(warp - P.slot_off);
+        const int np = P.n_sec;
+        const double L = Len[l];
+        const double *cz_line = cze + (P.node_off - node_base);
+        const double zl = cze_pl_at(cz_line, np, t), zr_ = cze_pl_at(cz_line, np, t + 1);
+        const double dtfp = (zr_ - zl) / (1.0 * ntf_pre);
+        const double *coe = coe_all + 18 * (size_t)warp;
+        double th = 0.0;
+        for (int tj = lane; tj <= ntf_pre; tj += 32) {
+            const double s = zl + dtfp * tj;
+            const double z = (s - zl) * L;
+            double dc[3], dd[3];
+    #pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double *a = coe + 6 * d;
+                dc[d] = (((5.0 * a[5] * z + 4.0 * a[4]) * z + 3.0 * a[3]) * z + 2.0 * a[2]) * z + a[1];
+                dd[d] = ((20.0 * a[5] * z + 12.0 * a[4]) * z + 6.0 * a[3]) * z + 2.0 * a[2];
+            }
+            const double x0 = dc[1] * dd[2] - dc[2] * dd[1];
+            const double x1 = dc[2] * dd[0] - dc[0] * dd[2];
+            const double x2 = dc[0] * dd[1] - dc[1] * dd[0];
+            const double ndc2 = dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2];
+            th += sqrt(x0 * x0 + x1 * x1 + x2 * x2) / ndc2 * dtfp * L;
         }
-        const double x0 = dc[1] * dd[2] - dc[2] * dd[1];
-        const double x1 = dc[2] * dd[0] - dc[0] * dd[2];
-        const double x2 = dc[0] * dd[1] - dc[1] * dd[0];
-        const double ndc2 = dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2];
-        th += sqrt(x0 * x0 + x1 * x1 + x2 * x2) / ndc2 * dtfp * L;
-    }
-    th = warp_sum(th);
-    if (lane == 0) {
-        const int ntf = (int)ceil(ntf_times * th / dev_pi2()) + 1;
-        ntf_out[warp] = ntf;
-        dtf_out[warp] = (zr_ - zl) / (1.0 * ntf);
+        th = warp_sum(th);
+        if (lane == 0) {
+            const int ntf = (int)ceil(ntf_times * th / dev_pi2()) + 1;
+            ntf_out[warp] = ntf;
+            dtf_out[warp] = (zr_ - zl) / (1.0 * ntf);
+        }
     }
 }
 
@@ -726,12 +734,16 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mo
     kt_end(c, km);
     const unsigned wblocks = (unsigned)((slots * 32 + 255) / 256);
     km = kt_begin(c, KT_SECTION);
+    FWT_TRY(buf_reserve(c, C.scratch[24], sizeof(unsigned) * (size_t)(slots + 4)));   // near-step list
+    unsigned *d_near = (unsigned *)C.scratch[24].p;
+    FWT_CUDA(cudaMemsetAsync(d_near, 0, sizeof(unsigned), c->stream));
     section_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, c->d_x, c->d_y, c->d_z, B.cze, B.ck,
                                                    B.ckk, B.Len, B.node_base, c->p.ntf_times, c->p.ntf_pre,
-                                                   B.coe, B.ntf, B.dtf);
-    section_fp64_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.cze, B.Len, B.node_base,
-                                                        c->p.ntf_times, c->p.ntf_pre, B.coe, B.ntf, B.dtf);
-    c->launches += 1;
+                                                   B.coe, B.ntf, B.dtf, d_near);
+    // a fixed grid: the list holds a few sections per thousand
+    section_fp64_kernel<<<4 * 148, 256, 0, c->stream>>>(B.lp, B.slot_line, B.cze, B.Len, B.node_base,
+                                                        c->p.ntf_times, c->p.ntf_pre, B.coe, d_near, B.ntf, B.dtf);
+    c->launches += 2;
     kt_end(c, km);
     km = kt_begin(c, KT_CENTERLINE);
     slot_counts_kernel<<<(unsigned)((slots + 255) / 256), 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf,
