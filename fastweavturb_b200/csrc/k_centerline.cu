@@ -10,6 +10,15 @@
 
 namespace fwt {
 
+// Slot -> batch-local line: block i fills line i's n_sec + 1 section slots.
+__global__ void slot_line_kernel(const LineParam *__restrict__ lp, int nlines, int *__restrict__ slot_line)
+{
+    const int i = blockIdx.x;
+    if (i >= nlines) return;
+    const LineParam &P = lp[i];
+    for (int t = threadIdx.x; t < P.n_sec + 1; t += blockDim.x) slot_line[P.slot_off + t] = i;
+}
+
 // ------------------------------------------------------------------ a2: line preprocessing
 // One block per line.  cze is an FP64 block scan of the wrapped node distances.
 __global__ void line_prep_kernel(const LineParam *__restrict__ lp, int nlines, const double *__restrict__ X,
@@ -676,7 +685,6 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mo
     B.node_base = c->node_off[la];
     int64_t nodes = 0, slots = 0;
     std::vector<LineParam> hp(nl);
-    std::vector<int> hslot_line;
     for (int i = 0; i < nl; ++i) {
         const int l = la + i;
         LineParam &P = hp[i];
@@ -694,9 +702,6 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mo
     }
     B.nodes = nodes;
     B.nslots = slots;
-    hslot_line.resize((size_t)slots);
-    for (int i = 0; i < nl; ++i)
-        for (int t = 0; t < hp[i].n_sec + 1; ++t) hslot_line[(size_t)(hp[i].slot_off + t)] = i;
 
     // buffers
     Ctx &C = *c;
@@ -725,12 +730,14 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mo
     B.qoff = (int64_t *)C.scratch[10].p;
     int64_t *d_misc = (int64_t *)C.scratch[11].p;
     FWT_CUDA(cudaMemcpyAsync(B.lp, hp.data(), sizeof(LineParam) * nl, cudaMemcpyHostToDevice, c->stream));
-    FWT_CUDA(cudaMemcpyAsync(B.slot_line, hslot_line.data(), sizeof(int) * (size_t)slots, cudaMemcpyHostToDevice,
-                             c->stream));
 
     int km = kt_begin(c, KT_CENTERLINE);
+    // slot -> line on the device (a host table of one int per slot, copied from pageable
+    // memory, cost milliseconds per batch)
+    slot_line_kernel<<<nl, 256, 0, c->stream>>>(B.lp, nl, B.slot_line);
     line_prep_kernel<<<nl, 256, 0, c->stream>>>(B.lp, nl, c->d_x, c->d_y, c->d_z, B.cze, B.ck, B.ckk, B.Len,
                                                 B.node_base);
+    c->launches += 1;
     kt_end(c, km);
     const unsigned wblocks = (unsigned)((slots * 32 + 255) / 256);
     km = kt_begin(c, KT_SECTION);
