@@ -186,7 +186,7 @@ __device__ __forceinline__ void clip_box(const SegRec &R, uint32_t img, int N, i
 // copy per record (cp.async.bulk, completion on the warp's mbarrier), flattens the chunk's
 // grid rows across its lanes, and adds into the CTA's fixed-point accumulators.  Only the
 // accumulator set-up and the epilogue synchronise the whole CTA.
-constexpr int kWarpChunk = 16;
+constexpr int kWarpChunk = 8;
 constexpr int kQueue = 64;       // accepted-point queue of a warp (< 32 left over + 32 new)
 struct WarpStage {
     SegRec rec[kWarpChunk];
