@@ -69,17 +69,17 @@ __global__ void piece_counts_kernel(const LineParam *__restrict__ lp, const int 
     poff[s] = real ? (ntf[s] + kPieceMax - 1) / kPieceMax : 0;
 }
 
-// slot of every piece (one warp per section slot)
+// slot of every piece (one thread per section slot: a slot has ceil(ntf / 8) pieces, mostly 1-3)
 __global__ void piece_map_kernel(const LineParam *__restrict__ lp, const int *__restrict__ slot_line, int64_t nslots,
                                  const int *__restrict__ ntf, const int64_t *__restrict__ poff, int *__restrict__ map)
 {
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= nslots) return;
-    const LineParam &P = lp[slot_line[warp]];
-    if ((int)(warp - P.slot_off) >= P.n_sec) return;
-    const int n = (ntf[warp] + kPieceMax - 1) / kPieceMax;
-    for (int j = lane; j < n; j += 32) map[poff[warp] + j] = (int)warp;
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const LineParam &P = lp[slot_line[s]];
+    if ((int)(s - P.slot_off) >= P.n_sec) return;
+    const int n = (ntf[s] + kPieceMax - 1) / kPieceMax;
+    const int64_t o = poff[s];
+    for (int j = 0; j < n; ++j) map[o + j] = (int)s;
 }
 
 // One thread per piece: FP64 samples, chords and boxes as the sub-segment set-up
@@ -766,8 +766,8 @@ int piece_setup(Ctx *c, CenterlineBatch &B)
     int *d_map = (int *)C.scratch[15].p;
     B.piece = (PieceRec *)C.scratch[18].p;
     km = kt_begin(c, KT_CENTERLINE);
-    piece_map_kernel<<<(unsigned)((slots * 32 + 255) / 256), 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf,
-                                                                                   d_poff, d_map);
+    piece_map_kernel<<<(unsigned)((slots + 255) / 256), 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf,
+                                                                              d_poff, d_map);
     if (np_ > 0)
         piece_build_kernel<<<(unsigned)((np_ + 127) / 128), 128, 0, c->stream>>>(
             B.lp, B.slot_line, d_map, np_, c->d_x, c->d_y, c->d_z, B.cze, B.node_base, B.coe, B.ntf, B.dtf, d_poff,
