@@ -55,7 +55,7 @@ class _Params(ctypes.Structure):
 EXPORTS = [
     "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_set_centerlines",
     "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
-    "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_copy_field",
+    "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_field_uw", "fwt_field_wd", "fwt_set_outputs", "fwt_copy_field",
     "fwt_write_outputs", "fwt_run_dir", "fwt_run",
     "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
     "fwt_set_tuning", "fwt_mlp_create", "fwt_mlp_destroy", "fwt_mlp_nparams", "fwt_mlp_get_params", "fwt_mlp_set_params",
@@ -93,6 +93,9 @@ def library(path: str | None = None):
         "fwt_sp": [vp, ip, ctypes.POINTER(ctypes.c_int), ip, dp],
         "fwt_sp_exponents": [dp, dp, ip, ip, dp, dp],
         "fwt_field_wh": [vp, ctypes.POINTER(ctypes.c_float)],
+        "fwt_field_uw": [vp, ctypes.POINTER(ctypes.c_float)],
+        "fwt_field_wd": [vp, ctypes.POINTER(ctypes.c_float)],
+        "fwt_set_outputs": [vp, ip, ip],
         "fwt_copy_field": [vp, ip, ip, dp],
         "fwt_write_outputs": [vp, ctypes.c_char_p],
         "fwt_run_dir": [ctypes.c_char_p, ctypes.POINTER(_Params)],
@@ -276,6 +279,25 @@ class Context:
         nd = self.params.N_downsample
         out = np.zeros(2 * nd ** 3, dtype=np.float32)
         _check(library().fwt_field_wh(self._h, _ptr(out, ctypes.c_float)))
+        return out.reshape(2, nd, nd, nd)
+
+    def set_outputs(self, u_out=False, d_out=False):
+        """The reference's u_out / d_out switches: write_outputs also writes field_uw.dat /
+        field_wd.dat."""
+        _check(library().fwt_set_outputs(self._h, int(bool(u_out)), int(bool(d_out))))
+
+    def field_uw(self):
+        """Downsampled ux, uy, uz, wx, wy, wz of the normalised fields: (6, nd, nd, nd) [k, j, i]."""
+        nd = self.params.N_downsample
+        out = np.zeros(6 * nd ** 3, dtype=np.float32)
+        _check(library().fwt_field_uw(self._h, _ptr(out, ctypes.c_float)))
+        return out.reshape(6, nd, nd, nd)
+
+    def field_wd(self):
+        """Downsampled |omega| and the dissipation S_ij S_ij: (2, nd, nd, nd) [k, j, i]."""
+        nd = self.params.N_downsample
+        out = np.zeros(2 * nd ** 3, dtype=np.float32)
+        _check(library().fwt_field_wd(self._h, _ptr(out, ctypes.c_float)))
         return out.reshape(2, nd, nd, nd)
 
     def copy_field(self, which, component):

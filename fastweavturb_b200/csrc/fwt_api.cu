@@ -258,6 +258,10 @@ int fwt_destroy(fwt_ctx *h)
     buf_free(c, c->b_u);
     buf_free(c, c->b_spec);
     buf_free(c, c->b_fftws);
+    buf_free(c, c->b_aux_spec);
+    buf_free(c, c->b_aux_real);
+    buf_free(c, c->b_aux_acc);
+    buf_free(c, c->b_aux_out);
     for (auto &b : c->scratch) buf_free(c, b);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -579,6 +583,31 @@ int fwt_set_tuning(fwt_ctx *h, int key, double value)
         return 0;
     }
     return fail(FWT_E_ARG, "unknown tuning key");
+}
+
+int fwt_set_outputs(fwt_ctx *h, int u_out, int d_out)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    c->u_out = u_out ? 1 : 0;
+    c->d_out = d_out ? 1 : 0;
+    return 0;
+}
+
+int fwt_field_uw(fwt_ctx *h, float *host_out)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !host_out) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    return stats_field_uw(c, host_out);
+}
+
+int fwt_field_wd(fwt_ctx *h, float *host_out)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !host_out) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    return stats_field_wd(c, host_out);
 }
 
 int fwt_counters(fwt_ctx *h, int64_t *v, int n)

@@ -94,6 +94,9 @@ struct Ctx {
     DevBuf b_u;       // u, 3 N^3
     DevBuf b_spec;    // spectral buffer, 3 N^2 (N/2+1) complex
     DevBuf b_fftws;   // cuFFT work area
+    // optional field outputs (field_uw.dat, field_wd.dat): the reference's u_out and d_out
+    int u_out = 0, d_out = 0;
+    DevBuf b_aux_spec, b_aux_real, b_aux_acc, b_aux_out;   // their buffers, made on first use
     cufftHandle plan_r2c = 0, plan_c2r = 0;
     bool plans = false;
     size_t fft_ws_bytes = 0;
@@ -165,6 +168,8 @@ int stats_normalise(Ctx *c);
 int stats_pdf(Ctx *c, int which, int comp, int nbins, float *val, float *pdf, uint64_t *counts);
 int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp);
 int stats_field_wh(Ctx *c, float *host_out);
+int stats_field_uw(Ctx *c, float *host_out);
+int stats_field_wd(Ctx *c, float *host_out);
 int stats_copy_field(Ctx *c, int which, int comp, double *host);
 
 // host I/O (fwt_io.cpp)

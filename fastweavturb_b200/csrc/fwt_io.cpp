@@ -341,6 +341,23 @@ int io_write_outputs(Ctx *c, const char *outdir)
         }
         fclose(f);
     }
+    // field_uw.dat (n_d^3 x 6: ux, uy, uz, wx, wy, wz) and field_wd.dat (n_d^3 x 2: |w|,
+    // S_ij S_ij), the same stream format, when the reference's u_out / d_out are set
+    // (tube.f90:1075-1120, inside its vorticity_output block)
+    const size_t nd3 = (size_t)c->p.N_downsample * c->p.N_downsample * c->p.N_downsample;
+    for (int which = 0; which < 2; ++which) {
+        if (!c->p.vorticity_output || !(which == 0 ? c->u_out : c->d_out)) continue;
+        const size_t n = (which == 0 ? 6 : 2) * nd3;
+        std::vector<float> box(n);
+        FWT_TRY(which == 0 ? stats_field_uw(c, box.data()) : stats_field_wd(c, box.data()));
+        const std::string name = which == 0 ? "/field_uw.dat" : "/field_wd.dat";
+        FWT_TRY(open_w(od + name, &f));
+        if (fwrite(box.data(), sizeof(float), n, f) != n) {
+            fclose(f);
+            return fail(FWT_E_IO, "short write of " + name.substr(1));
+        }
+        fclose(f);
+    }
     return 0;
 }
 

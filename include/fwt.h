@@ -150,6 +150,19 @@ int fwt_timings(fwt_ctx *ctx, double *t, int n);
  * binning, 3 deposition, 4 fused Biot-Savart, 5 cuFFT, 6 statistics, 7 generator.  (The
  * reference has no counterpart; it logs phase wall times to info.dat, tube.f90:519-953.) */
 int fwt_kernel_times(fwt_ctx *ctx, double *ms, int64_t *launches, int n);
+/* The reference's optional field outputs, switched off there by its compile-time flags u_out
+ * and d_out (tube.f90:55) and off by default here: with u_out, fwt_write_outputs also writes
+ * field_uw.dat (tube.f90:1075-1100), with d_out field_wd.dat (tube.f90:1102-1120), both in the
+ * raw float32 format of field_wh.dat and only when vorticity_output is set, as in the
+ * reference. */
+int fwt_set_outputs(fwt_ctx *ctx, int u_out, int d_out);
+/* The data boxes of those files after fwt_run: field_uw -> host_out[6 * n_d^3] (ux, uy, uz, wx,
+ * wy, wz, each n_d^3 in Fortran order), field_wd -> host_out[2 * n_d^3] (|omega| and the
+ * dissipation S_ij S_ij of dissipation_field, subroutine.f90:1086-1126), all of the normalised
+ * fields at the points i * N / n_d.  fwt_field_wd allocates, on first use, one extra half
+ * spectrum and three fields of the context's precision. */
+int fwt_field_uw(fwt_ctx *ctx, float *host_out);
+int fwt_field_wd(fwt_ctx *ctx, float *host_out);
 /* Counters of the last deposition: c[0] lines, c[1] sections, c[2] sub-segments,
  * c[3] candidate (tile, sub-segment) pairs, c[4] kernel launches of the last fwt_run. */
 int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);

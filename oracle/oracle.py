@@ -488,6 +488,48 @@ def field_wh(vor, vel, n_d):
     return np.stack([wm, h])  # (2, nz, ny, nx) == Fortran (nx, ny, nz, 2)
 
 
+def dx_dy_dz(phy, d):
+    """dx_dy_dz_dp_dm with switch_d = d (1, 2, 3: d/dx, d/dy, d/dz; subroutine.f90:1128-1163):
+    forward transform, times i k_d, backward transform, real part."""
+    N = phy.shape[0]
+    k = 1j * wavenumbers(N)
+    spec = fourier_forward(phy)
+    if d == 1:
+        spec = spec * k[None, None, :]
+    elif d == 2:
+        spec = spec * k[None, :, None]
+    else:
+        spec = spec * k[:, None, None]
+    return fourier_backward(spec)
+
+
+def dissipation_field(vel):
+    """sum_ij S_ij S_ij with S_ij = (du_i/dx_j + du_j/dx_i) / 2 (subroutine.f90:1086-1126)."""
+    dudx = [[dx_dy_dz(vel[i], j + 1) for j in range(3)] for i in range(3)]
+    disp = np.zeros_like(vel[0])
+    for i in range(3):
+        for j in range(3):
+            s = 0.5 * (dudx[i][j] + dudx[j][i])
+            disp += s * s
+    return disp
+
+
+def field_uw(vor, vel, n_d):
+    """Downsampled ux, uy, uz, wx, wy, wz as REAL(4) (tube.f90:1075-1100)."""
+    N = vor.shape[1]
+    s = slice(N // n_d - 1, N, N // n_d)
+    return np.concatenate([vel[:, s, s, s], vor[:, s, s, s]]).astype(np.float32)
+
+
+def field_wd(vor, vel, n_d):
+    """Downsampled |omega| and the dissipation field as REAL(4) (tube.f90:1102-1120)."""
+    N = vor.shape[1]
+    s = slice(N // n_d - 1, N, N // n_d)
+    w = vor[:, s, s, s]
+    wm = np.sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]).astype(np.float32)
+    return np.stack([wm, dissipation_field(vel)[s, s, s].astype(np.float32)])
+
+
 # ----------------------------------------------------------------------------- pipeline
 
 def run(params: Params, cl: Centerlines, nthreads=None, faithful_spectrum=False, sp_pmax=10):

@@ -151,3 +151,27 @@ def test_partial_tiles(fwt, orc, N, piece_cells):
     assert np.abs(vor).max() > 0
     assert rel_l2(vor[good], vor_o[good]) <= TOL32
     ctx.close()
+
+
+@pytest.mark.parametrize("precision,mode,tol_uw,tol_d", [(32, 0, 1e-5, 1e-4), (64, 1, 1e-6, 1e-6)])
+def test_optional_field_outputs_match_oracle(fwt, orc, small_case, precision, mode, tol_uw, tol_d, tmp_path):
+    """field_uw.dat and field_wd.dat (the reference's u_out / d_out outputs, tube.f90:1075-1120):
+    the downsampled u and omega, and the dissipation S_ij S_ij from spectral derivatives
+    (subroutine.f90:1086-1163), against the oracle's FP64 fields.  The boxes are REAL(4), so
+    the FP64 path is held to float32 rounding.  A second call gives the same box, and
+    write_outputs writes the same numbers when the switches are on."""
+    w, p, cl, ref = small_case
+    ctx = _gpu_run(fwt, w, cl, p, precision, mode)
+    uw, wd = ctx.field_uw(), ctx.field_wd()
+    uw_o = orc.field_uw(ref["vor"], ref["vel"], p.N_downsample)
+    wd_o = orc.field_wd(ref["vor"], ref["vel"], p.N_downsample)
+    assert uw.shape == uw_o.shape and wd.shape == wd_o.shape
+    assert rel_l2(uw[:3], uw_o[:3]) <= tol_uw and rel_l2(uw[3:], uw_o[3:]) <= tol_uw
+    assert rel_l2(wd[0], wd_o[0]) <= tol_uw
+    assert wd_o[1].max() > 0 and rel_l2(wd[1], wd_o[1]) <= tol_d
+    assert np.array_equal(ctx.field_wd(), wd)
+    ctx.set_outputs(u_out=True, d_out=True)
+    ctx.write_outputs(tmp_path / "output")
+    assert np.array_equal(np.fromfile(tmp_path / "output" / "field_uw.dat", dtype=np.float32), uw.ravel())
+    assert np.array_equal(np.fromfile(tmp_path / "output" / "field_wd.dat", dtype=np.float32), wd.ravel())
+    ctx.close()

@@ -416,3 +416,18 @@ def test_bf16_rounding_is_round_to_nearest_even():
     x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -9, 1.0 + 2 ** -9, -2.5, 3.0e38], dtype=np.float32)
     r = MO.bf16(x)
     assert list(r[:5]) == [1.0, 1.0, 1.0 + 2 ** -7, 1.0, -2.5]
+
+
+def test_dissipation_of_a_shear_and_a_strain(orc):
+    """dissipation_field (subroutine.f90:1086-1126) on fields with known strain: the shear
+    u = (sin y, 0, 0) has S_12 = S_21 = cos(y)/2, so S_ij S_ij = cos(y)^2 / 2; the strain
+    u = (sin x cos y, -cos x sin y, 0) has S_11 = -S_22 = cos x cos y and S_12 = 0, so
+    S_ij S_ij = 2 cos^2 x cos^2 y."""
+    N = 16
+    x = np.arange(N) * 2 * np.pi / N - np.pi
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")          # [k, j, i]
+    vel = np.stack([np.sin(Y), np.zeros_like(Y), np.zeros_like(Y)])
+    assert np.allclose(orc.dissipation_field(vel), 0.5 * np.cos(Y) ** 2, atol=1e-12)
+    vel = np.stack([np.sin(X) * np.cos(Y), -np.cos(X) * np.sin(Y), np.zeros_like(X)])
+    assert np.allclose(orc.dissipation_field(vel), 2.0 * np.cos(X) ** 2 * np.cos(Y) ** 2, atol=1e-12)
+    assert np.allclose(orc.dx_dy_dz(np.sin(2 * X), 1), 2 * np.cos(2 * X), atol=1e-12)
