@@ -81,8 +81,10 @@ module fwt_iface
          integer(c_int), value :: n
       end function
       ! the reference's u_out / d_out switches (tube.f90:55): field_uw.dat / field_wd.dat
-     integer(c_int) function fwt_set_outputs(ctx, u_out, d_out) bind(C)
-       import; type(c_ptr), value :: ctx; integer(c_int), value :: u_out, d_out
-     end function
+      integer(c_int) function fwt_set_outputs(ctx, u_out, d_out) bind(C, name="fwt_set_outputs")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: u_out, d_out
+      end function
   end interface
 end module fwt_iface
