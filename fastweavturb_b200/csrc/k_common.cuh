@@ -17,6 +17,18 @@ __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
 
+// cuFFT's complex type of a real precision
+template <typename Real>
+struct Cplx;
+template <>
+struct Cplx<float> {
+    using T = cufftComplex;
+};
+template <>
+struct Cplx<double> {
+    using T = cufftDoubleComplex;
+};
+
 // Quintic spline evaluation (subroutine.f90:490-560); coe layout [coord][6].
 __device__ __forceinline__ void spl_pos(const double *coe, double z, double *c3)
 {

@@ -19,17 +19,6 @@ namespace fwt {
 
 namespace {
 
-template <typename Real>
-struct CplxT;
-template <>
-struct CplxT<float> {
-    using T = cufftComplex;
-};
-template <>
-struct CplxT<double> {
-    using T = cufftDoubleComplex;
-};
-
 // data_box(i, j, k, :) = field(i*r_d, j*r_d, k*r_d, :), 1-based (tube.f90:1076-1087)
 __device__ __forceinline__ size_t box_point(size_t q, int N, int nd)
 {
@@ -56,10 +45,10 @@ __global__ void field_uw_kernel(const Real *__restrict__ w, const Real *__restri
 // pass 0: o_c = i k_c u^_c (S_11, S_22, S_33); pass 1: S_12, S_13, S_23 = i (k_j u^_i + k_i u^_j) / 2;
 // u^ is the unscaled R2C output, so every mode is also scaled by 1 / N^3
 template <typename Real>
-__global__ void strain_spec_kernel(const typename CplxT<Real>::T *__restrict__ ux,
-                                   const typename CplxT<Real>::T *__restrict__ uy,
-                                   const typename CplxT<Real>::T *__restrict__ uz, typename CplxT<Real>::T *__restrict__ o0,
-                                   typename CplxT<Real>::T *__restrict__ o1, typename CplxT<Real>::T *__restrict__ o2,
+__global__ void strain_spec_kernel(const typename Cplx<Real>::T *__restrict__ ux,
+                                   const typename Cplx<Real>::T *__restrict__ uy,
+                                   const typename Cplx<Real>::T *__restrict__ uz, typename Cplx<Real>::T *__restrict__ o0,
+                                   typename Cplx<Real>::T *__restrict__ o1, typename Cplx<Real>::T *__restrict__ o2,
                                    int N, int pass)
 {
     const int nh = N / 2 + 1;
@@ -72,9 +61,9 @@ __global__ void strain_spec_kernel(const typename CplxT<Real>::T *__restrict__ u
         const Real kx = (jx == N / 2) ? (Real)0 : (Real)jx;
         const Real ky = (jy == N / 2) ? (Real)0 : (Real)((jy + N / 2) % N - N / 2);
         const Real kz = (jz == N / 2) ? (Real)0 : (Real)((jz + N / 2) % N - N / 2);
-        const typename CplxT<Real>::T a = ux[id], b = uy[id], c = uz[id];
+        const typename Cplx<Real>::T a = ux[id], b = uy[id], c = uz[id];
         // i k (p + i q) = -k q + i k p
-        typename CplxT<Real>::T r0, r1, r2;
+        typename Cplx<Real>::T r0, r1, r2;
         if (pass == 0) {
             r0.x = -kx * a.y; r0.y = kx * a.x;
             r1.x = -ky * b.y; r1.y = ky * b.x;
@@ -135,7 +124,7 @@ int check_box(Ctx *c)
 template <typename Real>
 int field_wd_impl(Ctx *c, float *d_out)
 {
-    using C = typename CplxT<Real>::T;
+    using C = typename Cplx<Real>::T;
     const int N = c->p.N, nd = c->p.N_downsample;
     const size_t nh = (size_t)N * N * (N / 2 + 1), n3 = (size_t)N * N * N, m3 = (size_t)nd * nd * nd;
     FWT_TRY(spectral_init(c));

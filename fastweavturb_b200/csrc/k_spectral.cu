@@ -17,17 +17,6 @@
 
 namespace fwt {
 
-template <typename Real>
-struct Cplx;
-template <>
-struct Cplx<float> {
-    using T = cufftComplex;
-};
-template <>
-struct Cplx<double> {
-    using T = cufftDoubleComplex;
-};
-
 // segmented warp reduction of (shell, value) pairs whose shells are non-decreasing across
 // lanes; the last lane of each run adds the run total into sh[shell]
 __device__ __forceinline__ void shell_add(double *sh, int nek, int s, double v, bool valid)
