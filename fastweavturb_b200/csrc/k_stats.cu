@@ -318,11 +318,17 @@ int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp)
     const int64_t groups = (int64_t)N * N / W;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, (int64_t)sms * 4));
     const int mpw = (nr + 7) / 8;
+    // The dynamic shared-memory limit is a property of the kernel for the whole process: every
+    // context sets the same value, the device's opt-in maximum, so that contexts of different N
+    // on concurrent host threads never lower it under another's launch.
+    int optin = 0;
+    FWT_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
+    if (shb > (size_t)optin) return fail(FWT_E_RANGE, "Sp: N too large for one block's shared memory");
     const int km = kt_begin(c, KT_STATS);
 #define FWT_SP(REAL, MPW)                                                                                        \
     do {                                                                                                         \
         auto k = sp_kernel<REAL, 10, MPW>;                                                                       \
-        FWT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shb));               \
+        FWT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));                  \
         for (int ax = 0; ax < 3; ++ax)                                                                           \
             k<<<blocks, 256, shb, c->stream>>>((const REAL *)c->b_u.p + ax * n3, N, ax, s, d_r, nr, d_sp);        \
     } while (0)
