@@ -31,6 +31,12 @@ def test_header_declares_the_boundary():
         assert must in names
 
 
+def test_every_entry_point_is_documented_for_integrators():
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    undocumented = [n for n in declared_functions() if n not in doc]
+    assert not undocumented, undocumented
+
+
 def test_library_exports_every_declared_symbol(fwt):
     L = fwt.library()
     missing = [n for n in declared_functions() if not hasattr(L, n)]
