@@ -24,7 +24,7 @@ from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
-from .api import Context, Params, sp_exponents, sp_separations
+from .api import Context, Params, sp_exponents
 from .configs import build_workload
 
 TUNE_CANDIDATES = (0.0, 2.5, 5.0, 8.0)
