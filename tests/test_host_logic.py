@@ -70,3 +70,17 @@ def test_features_and_fit_error():
     z[:N_SHELLS] += 0.03
     eE, eF = fit_error(z, y)
     assert abs(eE - 0.03) < 1e-12 and eF == 0.0 and not within((eE, eF))
+
+
+def test_benchmark_workloads_follow_their_configurations():
+    """cfg0: 64^3, 3 levels, sigma_l = 0.3 2^-l, n_l = 4 4^l; cfg1: 256^3, 6 levels, 0.4 2^-l,
+    4 4^l; cfg2: 1024^3, 8 levels, 0.5 2^-l, 2 4^l; nodes 256 2^l, H = 0.7,
+    Gamma_l = (sigma_l / sigma_0)^(4/3) in all three."""
+    for w, N, nlev, s0, t0 in ((configs.cfg0(), 64, 3, 0.3, 4), (configs.cfg1(), 256, 6, 0.4, 4),
+                               (configs.cfg2(), 1024, 8, 0.5, 2)):
+        assert w.N == N and len(w.levels) == nlev and not w.level_streams
+        for l, L in enumerate(w.levels):
+            assert np.isclose(L.sigma, s0 * 2.0 ** -l) and L.tubes == t0 * 4 ** l and L.nodes == 256 * 2 ** l
+            assert L.H == 0.7 and np.isclose(L.Gamma, (L.sigma / s0) ** (4.0 / 3.0))
+    assert configs.cfg1().ntubes == 5460 and configs.cfg1().nnodes == 38347776
+    assert configs.cfg2().ntubes == 43690
