@@ -55,7 +55,8 @@ class _Params(ctypes.Structure):
 EXPORTS = [
     "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_set_centerlines",
     "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
-    "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_field_uw", "fwt_field_wd", "fwt_set_outputs", "fwt_copy_field",
+    "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_field_uw", "fwt_field_wd",
+    "fwt_set_outputs", "fwt_copy_field", "fwt_field_device",
     "fwt_write_outputs", "fwt_run_dir", "fwt_run",
     "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
     "fwt_set_tuning", "fwt_mlp_create", "fwt_mlp_destroy", "fwt_mlp_nparams", "fwt_mlp_get_params", "fwt_mlp_set_params",
@@ -97,6 +98,7 @@ def library(path: str | None = None):
         "fwt_field_wd": [vp, ctypes.POINTER(ctypes.c_float)],
         "fwt_set_outputs": [vp, ip, ip],
         "fwt_copy_field": [vp, ip, ip, dp],
+        "fwt_field_device": [vp, ip, ctypes.POINTER(vp)],
         "fwt_write_outputs": [vp, ctypes.c_char_p],
         "fwt_run_dir": [ctypes.c_char_p, ctypes.POINTER(_Params)],
         "fwt_run": [vp],
@@ -335,10 +337,27 @@ class Context:
         _check(library().fwt_set_tuning(self._h, 1, float(cells)))
 
     def counters(self):
-        v = np.zeros(5, dtype=np.int64)
-        library().fwt_counters(self._h, _ptr(v, ctypes.c_int64), 5)
+        v = np.zeros(7, dtype=np.int64)
+        library().fwt_counters(self._h, _ptr(v, ctypes.c_int64), 7)
         return {"lines": int(v[0]), "sections": int(v[1]), "subsegments": int(v[2]), "pairs": int(v[3]),
-                "launches": int(v[4])}
+                "launches": int(v[4]), "accepted": int(v[5]), "redone_fp64": int(v[6])}
+
+    def field_tensor(self, which):
+        """Zero-copy torch view (3, N, N, N), index [c, z, y, x], of the raw (unnormalised)
+        field on the device (which = 0: omega, 1: u), in the context's precision.  Valid until
+        the field is rebuilt or the context is closed."""
+        import torch
+
+        p = ctypes.c_void_p()
+        _check(library().fwt_field_device(self._h, which, ctypes.byref(p)))
+        N = self.N
+        dt = "<f4" if self.params.precision == 32 else "<f8"
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (3, N, N, N), "typestr": dt, "data": (p.value, False),
+                                        "version": 3, "strides": None}
+
+        return torch.as_tensor(_View(), device=torch.device("cuda", self.params.device))
 
     def fbb_generate(self, seed, tubes, nodes, H, dB, dx, dy, dz):
         tubes = np.ascontiguousarray(tubes, dtype=np.int32)

@@ -432,6 +432,17 @@ int fwt_field_wh(fwt_ctx *h, float *host_out)
     return stats_field_wh(c, host_out);
 }
 
+int fwt_field_device(fwt_ctx *h, int which, void **ptr)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !ptr) return fail(FWT_E_ARG, "null argument");
+    if (which != 0 && which != 1) return fail(FWT_E_ARG, "field_device: which must be 0 (omega) or 1 (u)");
+    if (which == 0 && !c->have_w) return fail(FWT_E_STATE, "omega not built");
+    if (which == 1 && !c->have_u) return fail(FWT_E_STATE, "u not built");
+    *ptr = which ? c->b_u.p : c->b_w.p;
+    return 0;
+}
+
 int fwt_copy_field(fwt_ctx *h, int which, int component, double *host)
 {
     Ctx *c = (Ctx *)h;
@@ -615,7 +626,7 @@ int fwt_counters(fwt_ctx *h, int64_t *v, int n)
     Ctx *c = (Ctx *)h;
     if (!c || !v) return fail(FWT_E_ARG, "null argument");
     int k = 0;
-    for (; k < n && k < 5; ++k) v[k] = c->counters[k];
+    for (; k < n && k < 7; ++k) v[k] = c->counters[k];
     return k;
 }
 

@@ -114,7 +114,7 @@ struct Ctx {
     std::vector<int64_t> line_ntf_sum, line_ntf_max;  // per deposited line
     std::vector<int> line_nsec;
     std::vector<double> line_len;
-    std::vector<float> wmin, wmax, umin, umax;   // per component, raw (unnormalised) fields
+    std::vector<double> wmin, wmax, umin, umax;  // per component, raw (unnormalised) fields, exact
 
     // statistics kept for file output
     std::vector<float> pdf_u_val, pdf_u, pdf_w_val, pdf_w;
@@ -126,7 +126,7 @@ struct Ctx {
     Timers tm;
     double t_ms[5] = {0, 0, 0, 0, 0};
     double t_deposit_wall_init = 0;
-    int64_t counters[5] = {0, 0, 0, 0, 0};
+    int64_t counters[7] = {0, 0, 0, 0, 0, 0, 0};   // see fwt_counters
     int64_t launches = 0;
     size_t mem_held = 0;
 

@@ -7,6 +7,7 @@
 //   chord_kernel       chords dci, |dci|, unit chords tci               tube.f90:740-751
 //   subseg_kernel      sub-segment records (unwrap, Rtube, box)          tube.f90:766-798
 #include "k_deposit.cuh"
+#include "k_tile_common.cuh"
 
 namespace fwt {
 
@@ -559,6 +560,23 @@ __global__ void __launch_bounds__(256) subseg_fused_kernel(
 }
 
 
+// FP64 sub-segment records of the FP64 tile path, one thread per sub-segment, built by the same
+// device code as the records of the FP64 redo (redo_subseg): the tile kernels decide their
+// candidate points in FP32 with a margin and then test and evaluate them in FP64 from these.
+__global__ void __launch_bounds__(256) subseg64_kernel(const RedoCtx R, const int *__restrict__ map,
+                                                       const int64_t *__restrict__ qoff, int64_t nsub, int line_base,
+                                                       SubSeg *__restrict__ out)
+{
+    const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nsub) return;
+    const int slot = map[q];
+    SubSeg S;
+    LineParam P;
+    redo_subseg(R, slot, (int)(q - qoff[slot]), S, P);
+    S.line = R.slot_line[slot] + line_base;
+    out[q] = S;
+}
+
 // ------------------------------------------------------------------ scan
 // Exclusive scan of n int64 values in place; out[n] receives the total.  Three launches:
 // block sums, a single-block scan of the block sums, and the per-block scan.
@@ -676,6 +694,35 @@ int scan_exclusive_i64(Ctx *c, int64_t *d_data, int64_t n, int64_t *d_total, Dev
 }
 
 // ------------------------------------------------------------------ driver
+// FP64 sub-segment records of every sub-segment of the batch (the FP64 tile path), after the
+// FP32 records: the sub-segment -> section map (built here for a piece batch), then the records.
+int subseg64_setup(Ctx *c, CenterlineBatch &B)
+{
+    Ctx &C = *c;
+    const int64_t nsub = std::max<int64_t>(B.nsub, 1);
+    const int *map = nullptr;
+    const unsigned wblocks = (unsigned)((B.nslots * 32 + 255) / 256);
+    int km = kt_begin(c, KT_CENTERLINE);
+    if (B.rec) {
+        map = B.rec_map;   // the sub-segment batch's own map
+    } else {
+        FWT_TRY(buf_reserve(c, C.scratch[16], sizeof(int) * (size_t)nsub));
+        int *m = (int *)C.scratch[16].p;
+        subseg_map_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, B.nslots, B.ntf, B.qoff, m);
+        c->launches += 1;
+        map = m;
+    }
+    FWT_TRY(buf_reserve(c, C.scratch[17], sizeof(SubSeg) * (size_t)nsub));
+    B.seg = (SubSeg *)C.scratch[17].p;
+    const RedoCtx R = redo_ctx(c, B, 1.0, B.rec == nullptr);
+    if (B.nsub > 0)
+        subseg64_kernel<<<(unsigned)((B.nsub + 255) / 256), 256, 0, c->stream>>>(R, map, B.qoff, B.nsub, B.la, B.seg);
+    kt_end(c, km);
+    c->launches += 1;
+    FWT_CUDA(cudaGetLastError());
+    return 0;
+}
+
 int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mode)
 {
     // la..lb-1: 0-based lines of this batch
@@ -781,7 +828,10 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mo
     FWT_CUDA(cudaMemcpyAsync(B.soff + slots, &B.nsamples, sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
     FWT_CUDA(cudaMemcpyAsync(B.qoff + slots, &B.nsub, sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
 
-    if (mode == BatchRecords::Pieces) return piece_setup(c, B);
+    if (mode == BatchRecords::Pieces) {
+        FWT_TRY(piece_setup(c, B));
+        return c->p.precision == 64 ? subseg64_setup(c, B) : 0;
+    }
     // the tile-owned FP32 kernel reads compact FP32 records built by one fused kernel; the box
     // walk reads FP64 records built from sample arrays
     const bool tile_mode = mode == BatchRecords::SubSeg;
@@ -791,6 +841,8 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mo
         B.rec = (SegRec *)C.scratch[18].p;
         FWT_TRY(buf_reserve(c, C.scratch[14], sizeof(int) * (size_t)std::max<int64_t>(B.nsub, 1)));
         int *d_map = (int *)C.scratch[14].p;
+        B.rec_map = d_map;
+        B.rec_first = B.qoff;
         km = kt_begin(c, KT_CENTERLINE);
         subseg_map_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf, B.qoff, d_map);
         if (B.nsub > 0)
@@ -800,7 +852,7 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mo
         kt_end(c, km);
         c->launches += 2;
         FWT_CUDA(cudaGetLastError());
-        return 0;
+        return c->p.precision == 64 ? subseg64_setup(c, B) : 0;
     }
     FWT_TRY(buf_reserve(c, C.scratch[14], sizeof(double) * (size_t)B.nsamples));        // s
     FWT_TRY(buf_reserve(c, C.scratch[15], sizeof(double) * 3 * (size_t)B.nsamples));    // ci

@@ -60,6 +60,8 @@ struct CenterlineBatch {
     SegRec *rec = nullptr;       // nsub FP32 records (tile-owned kernel)
     int64_t npieces = 0;         // chord pieces (piece kernel)
     PieceRec *piece = nullptr;   // npieces FP32 piece records
+    const int *rec_map = nullptr;        // record (sub-segment or piece) -> section slot
+    const int64_t *rec_first = nullptr;  // section slot -> its first record
     std::vector<int64_t> line_ntf_sum;  // 2 x nl: sum(ntf), max(ntf) per line
     std::vector<double> Lens;           // Len_Disc per line
 };
@@ -69,6 +71,7 @@ struct CenterlineBatch {
 enum class BatchRecords { SubSeg, Walk, Pieces };
 int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mode);
 int piece_setup(Ctx *c, CenterlineBatch &B);
+int subseg64_setup(Ctx *c, CenterlineBatch &B);
 int scan_exclusive_i64(Ctx *c, int64_t *d_data, int64_t n, int64_t *d_total, DevBuf &tmp);
 
 }  // namespace fwt

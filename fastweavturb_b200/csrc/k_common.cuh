@@ -79,7 +79,8 @@ __device__ __forceinline__ void spl_d2(const double *coe, double z, double *c3)
 
 __device__ __forceinline__ double sigma_func(double zeta, double length, double smax, double smin, int n_T)
 {
-    // subroutine.f90:164-173
+    // subroutine.f90:164-173; a constant core gives smin + 0 * (...) = smin exactly
+    if (smax == smin) return smin;
     const double omega = floor(length / dev_pi() + 0.5) * (double)n_T;
     return smin + (smax - smin) * (sin(omega * zeta) + 1.0) / 2.0;
 }
@@ -113,6 +114,24 @@ __host__ __device__ __forceinline__ float ord2f(uint32_t u)
 #else
     float f;
     __builtin_memcpy(&f, &v, 4);
+    return f;
+#endif
+}
+
+// double <-> order-preserving uint64 (bit-exact atomic min/max of FP64 values)
+__device__ __forceinline__ unsigned long long d2ord(double f)
+{
+    const unsigned long long u = (unsigned long long)__double_as_longlong(f);
+    return (u & 0x8000000000000000ull) ? ~u : (u | 0x8000000000000000ull);
+}
+__host__ __device__ __forceinline__ double ord2d(unsigned long long u)
+{
+    const unsigned long long v = (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)v);
+#else
+    double f;
+    __builtin_memcpy(&f, &v, 8);
     return f;
 #endif
 }

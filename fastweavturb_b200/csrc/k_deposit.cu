@@ -18,90 +18,6 @@
 
 namespace fwt {
 
-// ---------------------------------------------------------------------------- FP64 walk
-// Statement-for-statement the reference's inner body (tube.f90:806-892) at grid index
-// (ip, jp, kp) (1-based, unwrapped).  Returns true and the contribution if accepted.
-__device__ __forceinline__ bool point_ref_f64(const SubSeg &S, const LineParam &P, const double *coe, double dtf,
-                                              double dzeta_sup, double eta, double dx, int ip, int jp, int kp,
-                                              double out[3])
-{
-    const double xstart = -dev_pi();
-    const double m0 = dadd(dmul((double)ip - 1.0, dx), xstart);
-    const double m1 = dadd(dmul((double)jp - 1.0, dx), xstart);
-    const double m2 = dadd(dmul((double)kp - 1.0, dx), xstart);
-    const double a0 = dsub(m0, S.ci0[0]), a1 = dsub(m1, S.ci0[1]), a2 = dsub(m2, S.ci0[2]);
-    const double t0 = dadd(dadd(dmul(a0, S.tci0[0]), dmul(a1, S.tci0[1])), dmul(a2, S.tci0[2]));
-    if (!(t0 >= 0.0)) return false;
-    const double e0 = dsub(m0, S.ci1[0]), e1 = dsub(m1, S.ci1[1]), e2 = dsub(m2, S.ci1[2]);
-    double t1 = dadd(dadd(dmul(e0, S.tci1[0]), dmul(e1, S.tci1[1])), dmul(e2, S.tci1[2]));
-    if (!(t1 < 0.0)) return false;
-    double rho = sqrt(dsub(dadd(dadd(dmul(a0, a0), dmul(a1, a1)), dmul(a2, a2)), dmul(t0, t0)));
-    if (!(rho < S.Rt)) return false;
-    t1 = dadd(dadd(dmul(e0, S.tci0[0]), dmul(e1, S.tci0[1])), dmul(e2, S.tci0[2]));
-    const double zeta = (S.s1 * t0 - S.s0 * t1) / S.ndci0;
-    const double zsec = zeta - S.ssec;
-    const double L = P.Len;
-    double cz[3], dc[3], ddc[3];
-    spl_pos(coe, zsec * L, cz);
-    const double dzeta = fmin(dzeta_sup, 1.0 * dtf);
-    spl_d1(coe, zsec * L, dc);
-    const double ndc = sqrt(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]);
-    double T[3] = {dc[0] / ndc, dc[1] / ndc, dc[2] / ndc};
-    spl_d2(coe, zsec * L, ddc);
-    double X[3] = {dc[1] * ddc[2] - dc[2] * ddc[1], dc[2] * ddc[0] - dc[0] * ddc[2], dc[0] * ddc[1] - dc[1] * ddc[0]};
-    const double nX = sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
-    double xc[3];
-    const double m[3] = {m0, m1, m2};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        double v = m[d] - cz[d];
-        if (v > dev_pi()) v = v - dev_pi2();
-        if (v < -dev_pi()) v = v + dev_pi2();
-        xc[d] = v;
-    }
-    const double nxc = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
-    rho = nxc;
-    const double sigma = sigma_func(zeta, P.length, P.sigma_max, P.sigma_min, P.n_T);
-    const double s2 = sigma * sigma;
-    double tp = exp(-(rho * rho) / 2.0 / s2) / (dev_pi2() * s2);
-    const double ftd = -exp(-(S.Rt * S.Rt) / 2.0 / s2) / (dev_pi2() * s2);
-    tp = tp + ftd;
-    const double sl = sigma_func(zeta - dzeta, P.length, P.sigma_max, P.sigma_min, P.n_T);
-    const double sr = sigma_func(zeta + dzeta, P.length, P.sigma_max, P.sigma_min, P.n_T);
-    double dsds = (sr - sl) / (2.0 * dzeta);
-    dsds = dsds / ndc / L;
-    const double G = P.Gamma;
-    if (nX < 1.0e-8) {
-        double er[3], eth[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) er[d] = xc[d] / (nxc + 1.0e-15);
-        eth[0] = er[1] * T[2] - er[2] * T[1];
-        eth[1] = er[2] * T[0] - er[0] * T[2];
-        eth[2] = er[0] * T[1] - er[1] * T[0];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) out[d] = tp * G * (T[d] + eta * rho * eth[d] + (rho * dsds / sigma) * er[d]);
-    } else {
-        double B[3], Nv[3];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) B[d] = X[d] / nX;
-        Nv[0] = B[1] * T[2] - B[2] * T[1];
-        Nv[1] = B[2] * T[0] - B[0] * T[2];
-        Nv[2] = B[0] * T[1] - B[1] * T[0];
-        const double kap = nX / (ndc * ndc * ndc);
-        const double costh = (xc[0] * Nv[0] + xc[1] * Nv[1] + xc[2] * Nv[2]) / (nxc + 1.0e-15);
-        const double sinth = (xc[0] * B[0] + xc[1] * B[1] + xc[2] * B[2]) / (nxc + 1.0e-15);
-        const double den = 1.0 - kap * rho * costh;
-        const double t5 = -(sinth * rho) / den;
-        const double t6 = costh * rho / den;
-        const double t7 = costh * rho * dsds / sigma / den;
-        const double t8 = sinth * rho * dsds / sigma / den;
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-            out[d] = tp * G * (T[d] + eta * (t5 * Nv[d] + t6 * B[d]) + (t7 * Nv[d] + t8 * B[d]));
-    }
-    return true;
-}
-
 // Reference box walk: one warp per sub-segment; lanes stride the box points in the
 // reference's loop order (k outer, i inner); contributions added with global atomics.
 template <typename Real, bool General>
@@ -147,9 +63,19 @@ __global__ void __launch_bounds__(256) deposit_walk_kernel(const SubSeg *__restr
                 const int ii = (int)(idx % nx);
                 const int64_t r = idx / nx;
                 const int jj = (int)(r % ny), kk = (int)(r / ny);
-                float o[3];
-                if (!point_f32<General>(G, ii, jj, kk, o)) continue;
+                float o[3], cond;
+                if (!point_f32<General>(G, ii, jj, kk, o, cond)) continue;
                 const int ip = S.box_lo[0] + ii, jp = S.box_lo[1] + jj, kp = S.box_lo[2] + kk;
+                if (General && !(cond <= kRedoCond)) {
+                    // ill-conditioned curved-branch point: the reference's FP64 arithmetic
+                    double o64[3];
+                    if (!point_ref_f64(S, P, coe + 18 * (size_t)S.slot, dt, dzeta_sup, eta, dev_pi2() / N, ip, jp, kp,
+                                       o64))
+                        continue;
+                    o[0] = (float)o64[0];
+                    o[1] = (float)o64[1];
+                    o[2] = (float)o64[2];
+                }
                 const size_t id = (size_t)wrap_idx(ip - 1, N) +
                                   (size_t)N * ((size_t)wrap_idx(jp - 1, N) + (size_t)N * (size_t)wrap_idx(kp - 1, N));
                 atomicAdd((float *)wx + id, o[0]);
@@ -218,12 +144,16 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
     }
     c->have_u = false;
     c->normalised = false;
-    FWT_TRY(buf_reserve(c, c->scratch[19], 64));
+    // scratch[19]: [0, 8) accepted points of the box walk, [16, 64) the component range of a
+    // tile deposition, [64, 80) the tile kernels' tallies (accepted pairs, FP64 redone pairs)
+    FWT_TRY(buf_reserve(c, c->scratch[19], 128));
     unsigned long long *d_acc = (unsigned long long *)c->scratch[19].p;
-    FWT_CUDA(cudaMemsetAsync(d_acc, 0, sizeof(unsigned long long), c->stream));
+    FWT_CUDA(cudaMemsetAsync(d_acc, 0, 128, c->stream));
     int64_t sections = 0, subsegs = 0, pairs = 0;
     const int64_t cap = batch_node_cap(c);
-    const bool tile_path = c->p.precision == 32 && c->p.deposit_mode == 0;
+    // deposit_mode 0: the tile-owned kernels (FP32 evaluation, or in the FP64 path FP32
+    // candidate tests and the reference's FP64 tests and arithmetic); 1: the reference's box walk
+    const bool tile_path = c->p.deposit_mode == 0;
     const double dxg = kPi2 / c->p.N;
     // radius limit of the piece kernel in grid spacings: fwt_set_tuning, else the environment
     // variable FWT_PIECE_RT_CELLS, else the default
@@ -288,6 +218,13 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
     c->counters[1] = sections;
     c->counters[2] = subsegs;
     c->counters[3] = pairs;
+    unsigned long long tally[3];
+    FWT_CUDA(cudaMemcpyAsync(tally, d_acc, sizeof(tally), cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaMemcpyAsync(tally + 1, d_acc + 8, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    c->counters[5] = (int64_t)(tile_path ? tally[1] : tally[0]);
+    c->counters[6] = (int64_t)tally[2];
     return 0;
 }
 

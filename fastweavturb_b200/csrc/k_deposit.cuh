@@ -5,6 +5,253 @@
 
 namespace fwt {
 
+// ---------------------------------------------------------------------------- FP64 reference
+// The reference's inner body (tube.f90:806-892) split in two: the acceptance tests
+// (tube.f90:806-818) and the vorticity of an accepted point (tube.f90:819-892), statement for
+// statement in FP64.  m: mesh coordinates of the 1-based unwrapped grid index.
+__device__ __forceinline__ void ref_mesh_f64(double dx, int ip, int jp, int kp, double m[3])
+{
+    const double xstart = -dev_pi();
+    m[0] = dadd(dmul((double)ip - 1.0, dx), xstart);
+    m[1] = dadd(dmul((double)jp - 1.0, dx), xstart);
+    m[2] = dadd(dmul((double)kp - 1.0, dx), xstart);
+}
+
+// t0 = (x - ci0) . tci0 and t1' = (x - ci1) . tci0 (the projections ζ is interpolated from);
+// returns whether the point passes the three tests.
+__device__ __forceinline__ bool ref_tests_f64(const SubSeg &S, const double m[3], double &t0, double &t1p)
+{
+    const double a0 = dsub(m[0], S.ci0[0]), a1 = dsub(m[1], S.ci0[1]), a2 = dsub(m[2], S.ci0[2]);
+    t0 = dadd(dadd(dmul(a0, S.tci0[0]), dmul(a1, S.tci0[1])), dmul(a2, S.tci0[2]));
+    const double e0 = dsub(m[0], S.ci1[0]), e1 = dsub(m[1], S.ci1[1]), e2 = dsub(m[2], S.ci1[2]);
+    const double t1 = dadd(dadd(dmul(e0, S.tci1[0]), dmul(e1, S.tci1[1])), dmul(e2, S.tci1[2]));
+    t1p = dadd(dadd(dmul(e0, S.tci0[0]), dmul(e1, S.tci0[1])), dmul(e2, S.tci0[2]));
+    if (!(t0 >= 0.0) || !(t1 < 0.0)) return false;
+    const double rho = sqrt(dsub(dadd(dadd(dmul(a0, a0), dmul(a1, a1)), dmul(a2, a2)), dmul(t0, t0)));
+    return rho < S.Rt;
+}
+
+__device__ __forceinline__ void ref_value_f64(const SubSeg &S, const LineParam &P, const double *coe, double dtf,
+                                              double dzeta_sup, double eta, const double m[3], double t0,
+                                              double t1, double out[3])
+{
+    const double zeta = (S.s1 * t0 - S.s0 * t1) / S.ndci0;
+    const double zsec = zeta - S.ssec;
+    const double L = P.Len;
+    double cz[3], dc[3], ddc[3];
+    spl_pos(coe, zsec * L, cz);
+    const double dzeta = fmin(dzeta_sup, 1.0 * dtf);
+    spl_d1(coe, zsec * L, dc);
+    const double ndc = sqrt(dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2]);
+    double T[3] = {dc[0] / ndc, dc[1] / ndc, dc[2] / ndc};
+    spl_d2(coe, zsec * L, ddc);
+    double X[3] = {dc[1] * ddc[2] - dc[2] * ddc[1], dc[2] * ddc[0] - dc[0] * ddc[2], dc[0] * ddc[1] - dc[1] * ddc[0]};
+    const double nX = sqrt(X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+    double xc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double v = m[d] - cz[d];
+        if (v > dev_pi()) v = v - dev_pi2();
+        if (v < -dev_pi()) v = v + dev_pi2();
+        xc[d] = v;
+    }
+    const double nxc = sqrt(xc[0] * xc[0] + xc[1] * xc[1] + xc[2] * xc[2]);
+    const double rho = nxc;
+    const double sigma = sigma_func(zeta, P.length, P.sigma_max, P.sigma_min, P.n_T);
+    const double s2 = sigma * sigma;
+    double tp = exp(-(rho * rho) / 2.0 / s2) / (dev_pi2() * s2);
+    const double ftd = -exp(-(S.Rt * S.Rt) / 2.0 / s2) / (dev_pi2() * s2);
+    tp = tp + ftd;
+    const double sl = sigma_func(zeta - dzeta, P.length, P.sigma_max, P.sigma_min, P.n_T);
+    const double sr = sigma_func(zeta + dzeta, P.length, P.sigma_max, P.sigma_min, P.n_T);
+    double dsds = (sr - sl) / (2.0 * dzeta);
+    dsds = dsds / ndc / L;
+    const double G = P.Gamma;
+    if (nX < 1.0e-8) {
+        double er[3], eth[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) er[d] = xc[d] / (nxc + 1.0e-15);
+        eth[0] = er[1] * T[2] - er[2] * T[1];
+        eth[1] = er[2] * T[0] - er[0] * T[2];
+        eth[2] = er[0] * T[1] - er[1] * T[0];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) out[d] = tp * G * (T[d] + eta * rho * eth[d] + (rho * dsds / sigma) * er[d]);
+    } else {
+        double B[3], Nv[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) B[d] = X[d] / nX;
+        Nv[0] = B[1] * T[2] - B[2] * T[1];
+        Nv[1] = B[2] * T[0] - B[0] * T[2];
+        Nv[2] = B[0] * T[1] - B[1] * T[0];
+        const double kap = nX / (ndc * ndc * ndc);
+        const double costh = (xc[0] * Nv[0] + xc[1] * Nv[1] + xc[2] * Nv[2]) / (nxc + 1.0e-15);
+        const double sinth = (xc[0] * B[0] + xc[1] * B[1] + xc[2] * B[2]) / (nxc + 1.0e-15);
+        const double den = 1.0 - kap * rho * costh;
+        const double t5 = -(sinth * rho) / den;
+        const double t6 = costh * rho / den;
+        const double t7 = costh * rho * dsds / sigma / den;
+        const double t8 = sinth * rho * dsds / sigma / den;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            out[d] = tp * G * (T[d] + eta * (t5 * Nv[d] + t6 * B[d]) + (t7 * Nv[d] + t8 * B[d]));
+    }
+}
+
+// The reference's body at grid index (ip, jp, kp) (1-based, unwrapped): true and the
+// contribution if accepted.
+__device__ __forceinline__ bool point_ref_f64(const SubSeg &S, const LineParam &P, const double *coe, double dtf,
+                                              double dzeta_sup, double eta, double dx, int ip, int jp, int kp,
+                                              double out[3])
+{
+    double m[3], t0, t1;
+    ref_mesh_f64(dx, ip, jp, kp, m);
+    if (!ref_tests_f64(S, m, t0, t1)) return false;
+    ref_value_f64(S, P, coe, dtf, dzeta_sup, eta, m, t0, t1, out);
+    return true;
+}
+
+// FP64 data of a batch that the tile kernels read to redo a (point, sub-segment) pair in the
+// reference's arithmetic: the section's spline coefficients and sample spacing, the line's
+// constants, and the map from a record to its section.  A record is a sub-segment
+// (pieces = false: rec -> slot = map[rec], chord j = rec - first[slot]) or a chord piece
+// (pieces = true: rec -> slot = map[rec], chords j0.. of piece rec - first[slot]).
+struct RedoCtx {
+    const LineParam *lp;
+    const int *slot_line, *map, *ntf;
+    const int64_t *first;
+    const int64_t *qoff;       // section slot -> its first sub-segment
+    const SubSeg *seg;         // FP64 sub-segment records (the FP64 tile path), or null
+    unsigned long long *tally; // [0] accepted pairs evaluated, [1] pairs redone in FP64
+    const double *X, *Y, *Z, *cze, *coe, *dtf;
+    int64_t node_base;
+    int N, pieces;
+    double Rtube_ratio, dzeta_sup, eta, scale;
+};
+
+// Sub-segment j of section `slot` in FP64, built as the record builders build it
+// (tube.f90:703-798): samples j, j+1, j+2 of the section's extended sample list, chords, the
+// mark1 unwrap, Rtube and the box.
+__device__ __forceinline__ void redo_subseg(const RedoCtx &R, int slot, int j, SubSeg &S, LineParam &P)
+{
+    P = R.lp[R.slot_line[slot]];
+    const int t = slot - (int)P.slot_off;
+    const int np = P.n_sec;
+    const int n = R.ntf[slot];
+    const double L = P.Len;
+    const double *czl = R.cze + (P.node_off - R.node_base);
+    const double zl = cze_pl_at(czl, np, t), zl1 = cze_pl_at(czl, np, t + 1);
+    const double d = R.dtf[slot];
+    const double *cf = R.coe + 18 * (size_t)slot;
+    const int inext = (t + 1 < np) ? t + 1 : 0;
+    double c[3][3];
+#pragma unroll 1
+    for (int s = 0; s < 3; ++s) {
+        const int k = j + s;
+        if (k < n) {
+            spl_pos_fma(cf, (zl + d * k - zl) * L, c[s]);
+        } else if (k == n) {
+            c[s][0] = R.X[P.node_off + inext];
+            c[s][1] = R.Y[P.node_off + inext];
+            c[s][2] = R.Z[P.node_off + inext];
+        } else {
+            spl_pos_fma(R.coe + 18 * (size_t)(slot + 1), (zl1 + R.dtf[slot + 1] * 1 - zl1) * L, c[s]);
+        }
+    }
+    double ch0[3], ch1[3];
+    cminus3(c[1], c[0], ch0);
+    cminus3(c[2], c[1], ch1);
+    const double n0 = sqrt(ch0[0] * ch0[0] + ch0[1] * ch0[1] + ch0[2] * ch0[2]);
+    const double n1 = sqrt(ch1[0] * ch1[0] + ch1[1] * ch1[1] + ch1[2] * ch1[2]);
+    const double i0 = 1.0 / n0, i1 = 1.0 / n1;
+    const double s0 = zl + d * j, s1 = zl + d * (j + 1);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double a = c[0][k], b = c[1][k];
+        if (b - a > dev_pi()) a = a + dev_pi2();
+        else if (b - a < -dev_pi()) b = b + dev_pi2();
+        S.ci0[k] = a;
+        S.ci1[k] = b;
+        S.tci0[k] = ch0[k] * i0;
+        S.tci1[k] = ch1[k] * i1;
+    }
+    S.s0 = s0;
+    S.s1 = s1;
+    S.ndci0 = n0;
+    S.ssec = zl;
+    S.zs0 = s0 - zl;
+    double Rt;
+    if (P.sigma_max == P.sigma_min) {
+        Rt = R.Rtube_ratio * P.sigma_min;
+    } else {
+        Rt = R.Rtube_ratio * sigma_func(s0, P.length, P.sigma_max, P.sigma_min, P.n_T);
+        Rt = fmax(Rt, R.Rtube_ratio * sigma_func(s1, P.length, P.sigma_max, P.sigma_min, P.n_T));
+    }
+    S.Rt = Rt;
+    S.slot = slot;
+    S.line = 0;
+    const double inv_dx = (double)R.N / dev_pi2(), xstart = -dev_pi();
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double mn = fmin(S.ci0[k], S.ci1[k]), mx = fmax(S.ci0[k], S.ci1[k]);
+        S.box_lo[k] = (int)floor((mn - xstart - Rt) * inv_dx + 1.0);
+        S.box_hi[k] = (int)ceil((mx - xstart + Rt) * inv_dx + 1.0);
+    }
+}
+
+// Chord j of record `rec` (a sub-segment, or chord `ch` of a piece) and its section.
+__device__ __forceinline__ void redo_locate(const RedoCtx &R, uint32_t rec, int ch, int &slot, int &j)
+{
+    slot = R.map[rec];
+    const int i = (int)((int64_t)rec - R.first[slot]);
+    if (!R.pieces) {
+        j = i;
+        return;
+    }
+    // pieces split a section's ntf chords as evenly as possible (piece_build_kernel)
+    const int ns = R.ntf[slot];
+    const int npc = (ns + 7) / 8;
+    const int base = ns / npc, rem = ns % npc;
+    j = i * base + min(i, rem) + ch;
+}
+
+// The reference's FP64 vorticity of the pair (grid point g = wrapped 0-based indices,
+// record rec, chord ch), as a fixed-point contribution.  The tile kernel already accepted the
+// pair; the grid point's image inside the sub-segment's box is the one the reference visits.
+static __device__ __noinline__ bool redo_pair_f64(const RedoCtx &R, uint32_t rec, int ch, int gx, int gy, int gz,
+                                                  long long q[3])
+{
+    int slot, j;
+    redo_locate(R, rec, ch, slot, j);
+    SubSeg S;
+    LineParam P;
+    redo_subseg(R, slot, j, S, P);
+    const int g[3] = {gx, gy, gz};
+    int ix[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        int o = (g[k] + 1 - S.box_lo[k]) % R.N;
+        if (o < 0) o += R.N;
+        ix[k] = S.box_lo[k] + o;
+    }
+    double m[3], t0, t1, v[3];
+    ref_mesh_f64(dev_pi2() / R.N, ix[0], ix[1], ix[2], m);
+    ref_tests_f64(S, m, t0, t1);
+    ref_value_f64(S, P, R.coe + 18 * (size_t)slot, R.dtf[slot], R.dzeta_sup, R.eta, m, t0, t1, v);
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const double sv = v[k] * R.scale;
+        const bool in = fabs(sv) < 4.0e18;
+        q[k] = in ? __double2ll_rn(sv) : 0;
+        ok = ok && in;
+    }
+    return ok;
+}
+
+// Curved-branch amplification |1/(1 - kappa rho cos theta)| (tube.f90:876-879) above which an
+// FP32 evaluation cannot hold 1e-5: such pairs are redone in FP64 by redo_pair_f64.
+constexpr float kRedoCond = 4.0f;
+
 // FP32 view of one sub-segment, local to its start point ci0 and to a grid-index origin.
 struct SegF {
     float off[3];     // mesh point at the origin index minus ci0
@@ -91,8 +338,9 @@ __device__ __forceinline__ void seg_setup_f32(const SubSeg &S, const LineParam &
 // constant core (sigma_ratio = 1) and no twist (eta = 0), where the reference's vorticity
 // reduces to tp * Gamma * T.
 template <bool General>
-__device__ __forceinline__ bool point_f32(const SegF &G, int ii, int jj, int kk, float out[3])
+__device__ __forceinline__ bool point_f32(const SegF &G, int ii, int jj, int kk, float out[3], float &cond)
 {
+    cond = 1.0f;
     const float d0x = fmaf((float)ii, G.dx, G.off[0]);
     const float d0y = fmaf((float)jj, G.dx, G.off[1]);
     const float d0z = fmaf((float)kk, G.dx, G.off[2]);
@@ -166,6 +414,7 @@ __device__ __forceinline__ bool point_f32(const SegF &G, int ii, int jj, int kk,
             const float costh = (xc[0] * Nv[0] + xc[1] * Nv[1] + xc[2] * Nv[2]) * inr;
             const float sinth = (xc[0] * B[0] + xc[1] * B[1] + xc[2] * B[2]) * inr;
             const float iden = 1.0f / (1.0f - kap * rho * costh);
+            cond = fabsf(iden);
             const float t5 = -sinth * rho * iden, t6 = costh * rho * iden;
             const float t7 = costh * rho * dsds / sigma * iden, t8 = sinth * rho * dsds / sigma * iden;
 #pragma unroll
@@ -309,8 +558,9 @@ __device__ __forceinline__ bool rec_tests(const RecT &R, float d0x, float d0y, f
 // moved by rounding is undone by the final single wrap.
 template <bool General, bool Delta, typename RecT>
 __device__ __forceinline__ void vort_w(const RecT &R, float d0x, float d0y, float d0z, float zb, float w, float R2,
-                                       float out[3])
+                                       float out[3], float &cond)
 {
+    cond = 1.0f;
     const float W = Delta ? zb + w : w;
     float P[3], c1[3], Q[3];
 #pragma unroll
@@ -387,6 +637,7 @@ __device__ __forceinline__ void vort_w(const RecT &R, float d0x, float d0y, floa
             const float costh = (xc[0] * Nv[0] + xc[1] * Nv[1] + xc[2] * Nv[2]) * inr;
             const float sinth = (xc[0] * B[0] + xc[1] * B[1] + xc[2] * B[2]) * inr;
             const float iden = 1.0f / (1.0f - kap * rho * costh);
+            cond = fabsf(iden);
             const float t5 = -sinth * rho * iden, t6 = costh * rho * iden;
             const float t7 = costh * rho * dsds / sigma * iden, t8 = sinth * rho * dsds / sigma * iden;
 #pragma unroll
@@ -397,21 +648,12 @@ __device__ __forceinline__ void vort_w(const RecT &R, float d0x, float d0y, floa
 }
 
 // The vorticity of tube.f90:819-892 for a point that passed rec_tests with argument t0
-// (sub-segment record: W = t0 g).
+// (sub-segment record: W = t0 g), and its curved-branch amplification.
 template <bool General, typename RecT>
-__device__ __forceinline__ void rec_vorticity(const RecT &R, float d0x, float d0y, float d0z, float t0, float out[3])
+__device__ __forceinline__ void rec_vorticity(const RecT &R, float d0x, float d0y, float d0z, float t0, float out[3],
+                                              float &cond)
 {
-    vort_w<General, false>(R, d0x, d0y, d0z, 0.0f, t0 * R.g, R.R2, out);
-}
-
-// Predicate and vorticity together (tube.f90:806-892 in the local frame).
-template <bool General, typename RecT>
-__device__ __forceinline__ bool point_rec(const RecT &R, float d0x, float d0y, float d0z, float out[3])
-{
-    float t0;
-    if (!rec_tests(R, d0x, d0y, d0z, t0)) return false;
-    rec_vorticity<General>(R, d0x, d0y, d0z, t0, out);
-    return true;
+    vort_w<General, false>(R, d0x, d0y, d0z, 0.0f, t0 * R.g, R.R2, out, cond);
 }
 
 int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc);

@@ -359,6 +359,8 @@ struct PieceStage {
     ChordRows cr;
     uint32_t cq[kPQueue];  // candidates: chord lane (piece << 3 | chord) | x << 5 | y << 9 | z << 12 (tile-local)
     uint32_t q[kPQueue];   // piece | chord << 3 | x << 6 | y << 10 | z << 13 (tile-local)
+    RedoQueue redo;        // ill-conditioned pairs awaiting their FP64 evaluation
+    uint32_t id[kPChunk];  // global record ids of the staged pieces
     uint64_t bar;
     uint64_t pad;
 };
@@ -417,12 +419,56 @@ __device__ __forceinline__ bool piece_accepts(const PieceRec &R, int j, int rx, 
     return r2 < R.chq[j].y;
 }
 
-// Evaluate the first `cnt` queued (point, chord) pairs, one per lane, into the tile cells.
-template <bool General>
-__device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAccN], int lane, int cnt, int &qn,
-                                             float fscale, float fmaxq, int *__restrict__ err)
+// The candidate test of the FP64 path: piece_accepts with every test widened by far more than
+// its FP32 rounding (the guard band is that rounding), so that every point the reference's FP64
+// tests accept is queued; the FP64 tests then decide.
+__device__ __forceinline__ bool piece_accepts_wide(const PieceRec &R, int j, int rx, int ry, int rz)
 {
-    if (lane < cnt) {
+    const float dxv = fmaf((float)rx, R.dx, R.off[0]);
+    const float dyv = fmaf((float)ry, R.dx, R.off[1]);
+    const float dzv = fmaf((float)rz, R.dx, R.off[2]);
+    const float e = 10.0f * R.guard + 1e-3f * R.dx;
+    const float4 p0 = R.pl[j], p1 = R.pl[j + 1];
+    const float tj = fmaf(dzv, p0.z, fmaf(dyv, p0.y, fmaf(dxv, p0.x, -p0.w)));
+    const float tk = fmaf(dzv, p1.z, fmaf(dyv, p1.y, fmaf(dxv, p1.x, -p1.w)));
+    if (!(tj >= -e) || !(tk < e)) return false;
+    const float4 cp = R.po[j];
+    const float ex = fmaf((float)rx, R.dx, cp.x);
+    const float ey = fmaf((float)ry, R.dx, cp.y);
+    const float ez = fmaf((float)rz, R.dx, cp.z);
+    const float t0 = fmaf(ez, p0.z, fmaf(ey, p0.y, ex * p0.x));
+    const float e2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+    const float R2 = R.chq[j].y;
+    return fmaf(-t0, t0, e2) < R2 + 1e-5f * (e2 + R2) + e * e;
+}
+
+// Evaluate the first `cnt` queued (point, chord) pairs, one per lane, into the tile cells;
+// pairs whose curved-branch amplification exceeds kRedoCond go to the redo queue instead.
+template <bool General, bool F64>
+__device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAccN], int lane, int cnt, int &qn,
+                                             int &rn, unsigned &nacc, float fscale, float fmaxq, int *__restrict__ err,
+    const RedoCtx &redo, int x0, int y0, int z0)
+{
+    bool flag = false, ok64 = false;
+    uint32_t rrec = 0, rcode = 0;
+    if (F64 && lane < cnt) {
+        // FP64 path: the candidate passed the widened FP32 tests; the reference's FP64 tests
+        // decide, at the point's index in the chord's own box (the piece frame differs from it by
+        // whole periods)
+        const uint32_t e = S.q[lane];
+        const int k = (int)(e & 7u), j = (int)((e >> 3) & 7u);
+        const int lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)(e >> 13);
+        const PBox &B = S.box[k];
+        const PieceRec &R = S.rec[k];
+        int slot, jj;
+        redo_locate(redo, S.id[k] & ((1u << 26) - 1u), j, slot, jj);
+        const int64_t q = redo.qoff[slot] + jj;
+        const int *blo = redo.seg[q].box_lo;
+        ok64 = eval_pair_f64(redo, q, box_index(R.box_lo[0] + lx + B.dl[0], blo[0], redo.N),
+                      box_index(R.box_lo[1] + ly + B.dl[1], blo[1], redo.N),
+                      box_index(R.box_lo[2] + lz + B.dl[2], blo[2], redo.N),
+                      reinterpret_cast<double(*)[kAccN]>(acc), lx + kSY * ly + kSZ * lz);
+    } else if (lane < cnt) {
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 7u), j = (int)((e >> 3) & 7u);
         const int lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)(e >> 13);
@@ -433,18 +479,30 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
         const float ey = fmaf((float)(ly + B.dl[1]), R.dx, cp.y);
         const float ez = fmaf((float)(lz + B.dl[2]), R.dx, cp.z);
         const float t0 = fmaf(ez, pn.z, fmaf(ey, pn.y, ex * pn.x));
-        float vv[3];
-        vort_w<General, true>(R, ex, ey, ez, cp.w, t0 * cq.x, cq.y, vv);
+        float vv[3], cond;
+        vort_w<General, true>(R, ex, ey, ez, cp.w, t0 * cq.x, cq.y, vv, cond);
         const int p = lx + kSY * ly + kSZ * lz;
+        flag = General && !(cond <= kRedoCond);
+        if (flag) {
+            rrec = (S.id[k] & ((1u << 26) - 1u)) | ((uint32_t)j << 26);
+            rcode = redo_code(lx, ly, lz);
+        } else {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            float sv = vv[d] * fscale;
-            if (!(fabsf(sv) < fmaxq)) {
-                atomicOr(err, 4);
-                sv = sv != sv ? 0.0f : copysignf(fmaxq, sv);
+            for (int d = 0; d < 3; ++d) {
+                float sv = vv[d] * fscale;
+                if (!(fabsf(sv) < fmaxq)) {
+                    atomicOr(err, 4);
+                    sv = sv != sv ? 0.0f : copysignf(fmaxq, sv);
+                }
+                atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(sv));
             }
-            atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(sv));
         }
+    }
+    if constexpr (F64) nacc += __popc(__ballot_sync(0xffffffffu, ok64));
+    else nacc += cnt;
+    if constexpr (General && !F64) {
+        redo_push(S.redo, lane, flag, rrec, rcode, rn);
+        if (rn >= 32) redo_drain(S.redo, redo, acc, lane, 32, rn, x0, y0, z0, err);
     }
     __syncwarp();
     const int rem = qn - cnt;
@@ -457,9 +515,10 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
 
 // Test the first `cnt` candidate points, one per lane (piece_accepts), queue the accepted
 // (point, chord) pairs, drop the candidates and evaluate the queue when it holds 32 pairs.
-template <bool General>
+template <bool General, bool F64>
 __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[kAccN], int lane, int cnt, int &cn,
-                                                int &qn, float fscale, float fmaxq, int *__restrict__ err)
+                                                int &qn, int &rn, unsigned &nacc, float fscale, float fmaxq,
+                                                int *__restrict__ err, const RedoCtx &redo, int x0, int y0, int z0)
 {
     bool ok = false;
     uint32_t code = 0u;
@@ -468,7 +527,8 @@ __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[
         const int c = (int)(e & 31u), k = c >> 3, j = c & 7;
         const int lx = (int)((e >> 5) & 15u), ly = (int)((e >> 9) & 7u), lz = (int)(e >> 12);
         const PBox &B = S.box[k];
-        ok = piece_accepts(S.rec[k], j, lx + B.dl[0], ly + B.dl[1], lz + B.dl[2]);
+        ok = F64 ? piece_accepts_wide(S.rec[k], j, lx + B.dl[0], ly + B.dl[1], lz + B.dl[2])
+                 : piece_accepts(S.rec[k], j, lx + B.dl[0], ly + B.dl[1], lz + B.dl[2]);
         code = (uint32_t)k | ((uint32_t)j << 3) | ((uint32_t)lx << 6) | ((uint32_t)ly << 10) | ((uint32_t)lz << 13);
     }
     const unsigned bal = __ballot_sync(0xffffffffu, ok);
@@ -480,7 +540,7 @@ __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[
     if (lane < rem) S.cq[lane] = keep;
     __syncwarp();
     cn = rem;
-    if (qn >= 32) drain_pieces<General>(S, acc, lane, 32, qn, fscale, fmaxq, err);
+    if (qn >= 32) drain_pieces<General, F64>(S, acc, lane, 32, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
 }
 
 // One CTA per tile.  Each warp claims chunks of kPChunk pieces (32 chords), stages their
@@ -489,11 +549,11 @@ __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[
 // reference's tests (tube.f90:793-818: t_j >= 0, t_{j+1} < 0, distance to chord line j below
 // Rtube) with the plane tests in the piece frame and, within the rounding band of a plane, in
 // that sample's own frame.  Accepted pairs are queued and evaluated 32 at a time.
-template <bool General, bool Accumulate>
-__global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
+template <bool General, bool Accumulate, bool F64>
+__global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel(
     const PieceRec *__restrict__ rec, int N, int ntx, int nty, const int64_t *__restrict__ tile_off,
-    const uint32_t *__restrict__ list, double scale, float *__restrict__ wx, float *__restrict__ wy,
-    float *__restrict__ wz, uint32_t *__restrict__ mm, int *__restrict__ err)
+    const uint32_t *__restrict__ list, double scale, void *__restrict__ wx, void *__restrict__ wy,
+    void *__restrict__ wz, void *__restrict__ mm, int *__restrict__ err, const RedoCtx redo)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     long long(*acc)[kAccN] = reinterpret_cast<long long(*)[kAccN]>(dsm);
@@ -507,7 +567,11 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
     // next one, so the warps of a tile end close together at the epilogue's barrier
     __shared__ int next_chunk;
     if (threadIdx.x == 0) next_chunk = kDepWarps;
-    tile_acc_init<Accumulate>(acc, N, x0, y0, z0, scale, wx, wy, wz);
+    if constexpr (F64)
+        tile_acc_init_f64<Accumulate>(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, (const double *)wx,
+                                      (const double *)wy, (const double *)wz);
+    else
+        tile_acc_init<Accumulate>(acc, N, x0, y0, z0, scale, (const float *)wx, (const float *)wy, (const float *)wz);
     __syncthreads();
     const int64_t c0 = tile_off[tile], c1 = tile_off[tile + 1];
     const int nchunks = (int)((c1 - c0 + kPChunk - 1) / kPChunk);
@@ -516,10 +580,13 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
     uint32_t phase = 0;
     bool failed = false;
     int qn = 0;
+    int rn = 0;   // queued FP64 redo pairs of this warp (warp-uniform)
+    unsigned nacc = 0;   // pairs evaluated by this warp (warp-uniform)
     for (int ch = warp; ch < nchunks && !failed;) {
         const int64_t base = c0 + (int64_t)ch * kPChunk;
         const int nc = (c1 - base < kPChunk) ? (int)(c1 - base) : kPChunk;
         const uint32_t v = lane < nc ? __ldg(list + base + lane) : 0u;
+        if (lane < nc) S.id[lane] = v;
         if (lane == 0) mbar_expect(&S.bar, (uint32_t)(nc * sizeof(PieceRec)));
         __syncwarp();
         if (lane < nc) bulk_g2s(&S.rec[lane], rec + (v & ((1u << 26) - 1u)), (uint32_t)sizeof(PieceRec), &S.bar);
@@ -727,19 +794,26 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_piece_kernel(
                 if (has) S.cq[cn + __popc(bal & ((1u << lane) - 1u))] = code;
                 cn += __popc(bal);
                 __syncwarp();
-                if (cn >= 32) test_candidates<General>(S, acc, lane, 32, cn, qn, fscale, fmaxq, err);
+                if (cn >= 32) test_candidates<General, F64>(S, acc, lane, 32, cn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
             }
         }
-        if (cn > 0) test_candidates<General>(S, acc, lane, cn, cn, qn, fscale, fmaxq, err);
-        if (qn > 0) drain_pieces<General>(S, acc, lane, qn, qn, fscale, fmaxq, err);
+        if (cn > 0) test_candidates<General, F64>(S, acc, lane, cn, cn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+        if (qn > 0) drain_pieces<General, F64>(S, acc, lane, qn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
         __syncwarp();   // the warp's stage is reused by its next chunk
         int nxt = 0;
         if (lane == 0) nxt = atomicAdd(&next_chunk, 1);
         ch = __shfl_sync(0xffffffffu, nxt, 0);
     }
+    if constexpr (General && !F64)
+        if (rn > 0) redo_drain(S.redo, redo, acc, lane, rn, rn, x0, y0, z0, err);
     if (failed && lane == 0) atomicOr(err, 2);
+    if (lane == 0 && redo.tally) atomicAdd(redo.tally, (unsigned long long)nacc);
     __syncthreads();
-    tile_epilogue(acc, N, x0, y0, z0, scale, wx, wy, wz, mm);
+    if constexpr (F64)
+        tile_epilogue_f64(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, (double *)wx, (double *)wy,
+                          (double *)wz, (unsigned long long *)mm);
+    else
+        tile_epilogue(acc, N, x0, y0, z0, scale, (float *)wx, (float *)wy, (float *)wz, (uint32_t *)mm);
 }
 
 // ------------------------------------------------------------------------------ host
@@ -765,6 +839,8 @@ int piece_setup(Ctx *c, CenterlineBatch &B)
     FWT_TRY(buf_reserve(c, C.scratch[18], sizeof(PieceRec) * (size_t)std::max<int64_t>(np_, 1)));
     int *d_map = (int *)C.scratch[15].p;
     B.piece = (PieceRec *)C.scratch[18].p;
+    B.rec_map = d_map;
+    B.rec_first = d_poff;
     km = kt_begin(c, KT_CENTERLINE);
     piece_map_kernel<<<(unsigned)((slots + 255) / 256), 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf,
                                                                               d_poff, d_map);
@@ -835,47 +911,46 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     }
 
     const size_t n3 = field_elems(c);
-    float *w = (float *)c->b_w.p;
-    FWT_TRY(buf_reserve(c, C.scratch[19], 64));
-    uint32_t *d_mm = (uint32_t *)((char *)C.scratch[19].p + 16);
-    mm_init_kernel<<<1, 32, 0, c->stream>>>(d_mm, 6);
+    const bool f64 = c->p.precision == 64;
+    const size_t rb = f64 ? 8 : 4;
+    char *w = (char *)c->b_w.p;
+    void *wx = w, *wy = w + n3 * rb, *wz = w + 2 * n3 * rb;
+    FWT_TRY(buf_reserve(c, C.scratch[19], 128));   // deposit_lines cleared the tallies at 64
+    void *d_mm = (char *)C.scratch[19].p + 16;
+    if (f64) mm_init64_kernel<<<1, 32, 0, c->stream>>>((unsigned long long *)d_mm, 6);
+    else mm_init_kernel<<<1, 32, 0, c->stream>>>((uint32_t *)d_mm, 6);
     const bool general = !(c->p.sigma_ratio == 1.0 && c->p.eta_t == 0.0);
     const bool accumulate = c->w_written;
     const double scale = fixed_point_scale(c);
+    RedoCtx rctx = redo_ctx(c, B, scale, true);
+    rctx.tally = (unsigned long long *)((char *)C.scratch[19].p + 64);
     km = kt_begin(c, KT_DEPOSIT);
-#define FWT_PIECE_LAUNCH(G, A)                                                                              \
-    do {                                                                                                    \
-        FWT_CUDA(cudaFuncSetAttribute(deposit_piece_kernel<G, A>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                      (int)kPieceSmem));                                                    \
-        deposit_piece_kernel<G, A><<<(unsigned)ntiles, kDepThreads, kPieceSmem, c->stream>>>(              \
-            B.piece, N, ntx, nty, d_toff, d_list, scale, w, w + n3, w + 2 * n3, d_mm, d_err);                \
+#define FWT_PIECE_LAUNCH(G, A, D)                                                                          \
+    do {                                                                                                   \
+        FWT_CUDA(cudaFuncSetAttribute(deposit_piece_kernel<G, A, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                      (int)kPieceSmem));                                                   \
+        deposit_piece_kernel<G, A, D><<<(unsigned)ntiles, kDepThreads, kPieceSmem, c->stream>>>(          \
+            B.piece, N, ntx, nty, d_toff, d_list, scale, wx, wy, wz, d_mm, d_err, rctx);                    \
+        FWT_CUDA(cudaGetLastError());                                                                      \
     } while (0)
-    if (general) {
-        if (accumulate) FWT_PIECE_LAUNCH(true, true); else FWT_PIECE_LAUNCH(true, false);
+    if (f64) {
+        if (accumulate) FWT_PIECE_LAUNCH(true, true, true); else FWT_PIECE_LAUNCH(true, false, true);
+    } else if (general) {
+        if (accumulate) FWT_PIECE_LAUNCH(true, true, false); else FWT_PIECE_LAUNCH(true, false, false);
     } else {
-        if (accumulate) FWT_PIECE_LAUNCH(false, true); else FWT_PIECE_LAUNCH(false, false);
+        if (accumulate) FWT_PIECE_LAUNCH(false, true, false); else FWT_PIECE_LAUNCH(false, false, false);
     }
 #undef FWT_PIECE_LAUNCH
     kt_end(c, km);
     // algorithmic bytes: omega written once (read too when accumulating), one list entry and
     // one record per (tile, piece) pair
-    c->kbytes[KT_DEPOSIT] += (int64_t)(3 * n3 * 4 * (accumulate ? 2 : 1)) + npairs * (int64_t)(4 + sizeof(PieceRec));
+    c->kbytes[KT_DEPOSIT] += (int64_t)(3 * n3 * rb * (accumulate ? 2 : 1)) + npairs * (int64_t)(4 + sizeof(PieceRec));
     c->launches += 2;
-    FWT_CUDA(cudaGetLastError());
     c->w_written = true;
-    uint32_t hmm[6];
-    FWT_CUDA(cudaMemcpyAsync(hmm, d_mm, sizeof(hmm), cudaMemcpyDeviceToHost, c->stream));
     FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    FWT_TRY(read_dep_range(c, d_mm, f64));   // synchronises the stream
     if (herr & 2) return fail(FWT_E_TIMEOUT, "deposit: bulk copy wait ran out");
     if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
-    c->wmin.assign(3, 0.f);
-    c->wmax.assign(3, 0.f);
-    for (int d = 0; d < 3; ++d) {
-        c->wmin[d] = ord2f(hmm[2 * d]);
-        c->wmax[d] = ord2f(hmm[2 * d + 1]);
-    }
-    c->wmm_valid = true;
     return 0;
 }
 

@@ -192,6 +192,8 @@ struct WarpStage {
     SegRec rec[kWarpChunk];
     CandBox box[kWarpChunk];
     uint32_t q[kQueue];         // accepted points: candidate | x << 4 | y << 8 | z << 11 (tile-local)
+    RedoQueue redo;             // ill-conditioned pairs awaiting their FP64 evaluation
+    uint32_t id[kWarpChunk];    // global record ids of the staged candidates
     uint64_t bar;
     uint64_t pad;
 };
@@ -199,11 +201,27 @@ constexpr size_t kDepSmem = kAccBytes + sizeof(WarpStage) * kDepWarps;
 
 // Evaluate the first `cnt` queued points of the warp, one per lane (rec_tests again for t0,
 // then the vorticity), add them into the tile's fixed-point cells and drop them from the queue.
-template <bool General>
+// Pairs whose curved-branch amplification exceeds kRedoCond go to the warp's redo queue
+// instead, for an FP64 evaluation.
+template <bool General, bool F64>
 __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN], int lane, int cnt, int &qn,
-                                            float fscale, float fmaxq, int *__restrict__ err)
+                                            int &rn, unsigned &nacc, float fscale, float fmaxq, int *__restrict__ err,
+                                            const RedoCtx &redo, int x0, int y0, int z0)
 {
-    if (lane < cnt) {
+    bool flag = false, ok64 = false;
+    uint32_t rcode = 0, rrec = 0;
+    if (F64 && lane < cnt) {
+        // FP64 tile path: the candidate passed the widened FP32 tests; the reference's FP64
+        // tests decide, at its index in the sub-segment's own box
+        const uint32_t e = S.q[lane];
+        const int k = (int)(e & 15u);
+        const int lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)(e >> 11);
+        const CandBox &B = S.box[k];
+        const SegRec &R = S.rec[k];
+        ok64 = eval_pair_f64(redo, (int64_t)(S.id[k] & ((1u << 26) - 1u)), R.box_lo[0] + lx + B.dl[0],
+                      R.box_lo[1] + ly + B.dl[1], R.box_lo[2] + lz + B.dl[2], reinterpret_cast<double(*)[kAccN]>(acc),
+                      lx + kSY * ly + kSZ * lz);
+    } else if (lane < cnt) {
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 15u);
         const int lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)(e >> 11);
@@ -212,19 +230,31 @@ __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN
         const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
         const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
         const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
-        float t0, vv[3];
+        float t0, vv[3], cond;
         rec_tests(R, d0x, d0y, d0z, t0);
-        rec_vorticity<General>(R, d0x, d0y, d0z, t0, vv);
+        rec_vorticity<General>(R, d0x, d0y, d0z, t0, vv, cond);
         const int p = lx + kSY * ly + kSZ * lz;
+        flag = General && !(cond <= kRedoCond);
+        if (flag) {
+            rrec = S.id[k] & ((1u << 26) - 1u);
+            rcode = redo_code(lx, ly, lz);
+        } else {
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            float sv = vv[d] * fscale;
-            if (!(fabsf(sv) < fmaxq)) {
-                atomicOr(err, 4);
-                sv = sv != sv ? 0.0f : copysignf(fmaxq, sv);
+            for (int d = 0; d < 3; ++d) {
+                float sv = vv[d] * fscale;
+                if (!(fabsf(sv) < fmaxq)) {
+                    atomicOr(err, 4);
+                    sv = sv != sv ? 0.0f : copysignf(fmaxq, sv);
+                }
+                atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(sv));
             }
-            atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(sv));
         }
+    }
+    if constexpr (F64) nacc += __popc(__ballot_sync(0xffffffffu, ok64));
+    else nacc += cnt;
+    if constexpr (General && !F64) {
+        redo_push(S.redo, lane, flag, rrec, rcode, rn);
+        if (rn >= 32) redo_drain(S.redo, redo, acc, lane, 32, rn, x0, y0, z0, err);
     }
     __syncwarp();
     const int rem = qn - cnt;
@@ -235,11 +265,26 @@ __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN
     qn = rem;
 }
 
-template <bool General, bool Accumulate>
-__global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
+// The candidate test of the FP64 tile path: the three tests of tube.f90:806-818 widened by far
+// more than their FP32 rounding (about 1e-7 of the offsets), so that every point the
+// reference's FP64 tests accept is queued; the FP64 tests then decide.
+__device__ __forceinline__ bool rec_tests_wide(const SegRec &R, float d0x, float d0y, float d0z)
+{
+    const float e = 1e-3f * R.dx;
+    const float t0 = fmaf(d0z, R.tc0[2], fmaf(d0y, R.tc0[1], d0x * R.tc0[0]));
+    if (!(t0 >= -e)) return false;
+    const float ex = d0x - R.dci[0], ey = d0y - R.dci[1], ez = d0z - R.dci[2];
+    const float t1 = fmaf(ez, R.tc1[2], fmaf(ey, R.tc1[1], ex * R.tc1[0]));
+    if (!(t1 < e)) return false;
+    const float d2 = fmaf(d0z, d0z, fmaf(d0y, d0y, d0x * d0x));
+    return fmaf(-t0, t0, d2) < R.R2 + 1e-5f * (d2 + R.R2) + e * e;
+}
+
+template <bool General, bool Accumulate, bool F64>
+__global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
     const SegRec *__restrict__ rec, int N, int ntx, int nty, const int64_t *__restrict__ tile_off,
-    const uint32_t *__restrict__ list, double scale, float *__restrict__ wx, float *__restrict__ wy,
-    float *__restrict__ wz, uint32_t *__restrict__ mm, int *__restrict__ err)
+    const uint32_t *__restrict__ list, double scale, void *__restrict__ wx, void *__restrict__ wy,
+    void *__restrict__ wz, void *__restrict__ mm, int *__restrict__ err, const RedoCtx redo)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     long long(*acc)[kAccN] = reinterpret_cast<long long(*)[kAccN]>(dsm);
@@ -253,7 +298,11 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
     // next one, so the warps of a tile end close together at the epilogue's barrier
     __shared__ int next_chunk;
     if (threadIdx.x == 0) next_chunk = kDepWarps;
-    tile_acc_init<Accumulate>(acc, N, x0, y0, z0, scale, wx, wy, wz);
+    if constexpr (F64)
+        tile_acc_init_f64<Accumulate>(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, (const double *)wx,
+                                      (const double *)wy, (const double *)wz);
+    else
+        tile_acc_init<Accumulate>(acc, N, x0, y0, z0, scale, (const float *)wx, (const float *)wy, (const float *)wz);
     __syncthreads();
     const int64_t c0 = tile_off[tile], c1 = tile_off[tile + 1];
     const int nchunks = (int)((c1 - c0 + kWarpChunk - 1) / kWarpChunk);
@@ -262,10 +311,13 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
     uint32_t phase = 0;
     bool failed = false;
     int qn = 0;   // queued points of this warp (warp-uniform)
+    int rn = 0;   // queued FP64 redo pairs of this warp (warp-uniform)
+    unsigned nacc = 0;   // pairs evaluated by this warp (warp-uniform)
     for (int ch = warp; ch < nchunks && !failed;) {
         const int64_t base = c0 + (int64_t)ch * kWarpChunk;
         const int nc = (c1 - base < kWarpChunk) ? (int)(c1 - base) : kWarpChunk;
         const uint32_t v = lane < nc ? __ldg(list + base + lane) : 0u;
+        if (lane < nc) S.id[lane] = v;
         // stage the records: expect nc * sizeof(SegRec) bytes, then one bulk copy per record
         if (lane == 0) mbar_expect(&S.bar, (uint32_t)(nc * sizeof(SegRec)));
         __syncwarp();
@@ -340,8 +392,12 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
                     const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
                     const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
                     const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
-                    float t0;
-                    ok = rec_tests(R, d0x, d0y, d0z, t0);
+                    if constexpr (F64) {
+                        ok = rec_tests_wide(R, d0x, d0y, d0z);
+                    } else {
+                        float t0;
+                        ok = rec_tests(R, d0x, d0y, d0z, t0);
+                    }
                     code = (uint32_t)k | ((uint32_t)lx << 4) | ((uint32_t)ly << 8) | ((uint32_t)lz << 11);
                     ++i;
                 }
@@ -349,18 +405,25 @@ __global__ void __launch_bounds__(kDepThreads, 3) deposit_tile_kernel(
                 if (ok) S.q[qn + __popc(bal & ((1u << lane) - 1u))] = code;
                 qn += __popc(bal);
                 __syncwarp();
-                if (qn >= 32) drain_queue<General>(S, acc, lane, 32, qn, fscale, fmaxq, err);
+                if (qn >= 32) drain_queue<General, F64>(S, acc, lane, 32, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
             }
         }
-        if (qn > 0) drain_queue<General>(S, acc, lane, qn, qn, fscale, fmaxq, err);
+        if (qn > 0) drain_queue<General, F64>(S, acc, lane, qn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
         __syncwarp();   // the warp's stage is reused by its next chunk
         int nxt = 0;
         if (lane == 0) nxt = atomicAdd(&next_chunk, 1);
         ch = __shfl_sync(0xffffffffu, nxt, 0);
     }
+    if constexpr (General && !F64)
+        if (rn > 0) redo_drain(S.redo, redo, acc, lane, rn, rn, x0, y0, z0, err);
     if (failed && lane == 0) atomicOr(err, 2);
+    if (lane == 0 && redo.tally) atomicAdd(redo.tally, (unsigned long long)nacc);
     __syncthreads();
-    tile_epilogue(acc, N, x0, y0, z0, scale, wx, wy, wz, mm);
+    if constexpr (F64)
+        tile_epilogue_f64(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, (double *)wx, (double *)wy,
+                          (double *)wz, (unsigned long long *)mm);
+    else
+        tile_epilogue(acc, N, x0, y0, z0, scale, (float *)wx, (float *)wy, (float *)wz, (uint32_t *)mm);
 }
 
 
@@ -368,6 +431,56 @@ __global__ void mm_init_kernel(uint32_t *mm, int n)
 {
     const int i = threadIdx.x;
     if (i < n) mm[i] = (i & 1) ? 0u : 0xffffffffu;
+}
+
+__global__ void mm_init64_kernel(unsigned long long *mm, int n)
+{
+    const int i = threadIdx.x;
+    if (i < n) mm[i] = (i & 1) ? 0ull : ~0ull;
+}
+
+// Read back the deposition's component range (FP32 or FP64 words) into the context.
+int read_dep_range(Ctx *c, const void *d_mm, bool f64)
+{
+    unsigned long long h[6];
+    FWT_CUDA(cudaMemcpyAsync(h, d_mm, f64 ? 48 : 24, cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    const uint32_t *h32 = (const uint32_t *)h;
+    c->wmin.assign(3, 0.0);
+    c->wmax.assign(3, 0.0);
+    for (int d = 0; d < 3; ++d) {
+        c->wmin[d] = f64 ? ord2d(h[2 * d]) : (double)ord2f(h32[2 * d]);
+        c->wmax[d] = f64 ? ord2d(h[2 * d + 1]) : (double)ord2f(h32[2 * d + 1]);
+    }
+    c->wmm_valid = true;
+    return 0;
+}
+
+RedoCtx redo_ctx(const Ctx *c, const CenterlineBatch &B, double scale, bool pieces)
+{
+    RedoCtx r;
+    r.lp = B.lp;
+    r.slot_line = B.slot_line;
+    r.map = B.rec_map;
+    r.ntf = B.ntf;
+    r.first = B.rec_first;
+    r.qoff = B.qoff;
+    r.seg = B.seg;
+    r.tally = nullptr;
+    r.X = c->d_x;
+    r.Y = c->d_y;
+    r.Z = c->d_z;
+    r.cze = B.cze;
+    r.coe = B.coe;
+    r.dtf = B.dtf;
+    r.node_base = B.node_base;
+    r.N = c->p.N;
+    r.pieces = pieces ? 1 : 0;
+    r.Rtube_ratio = c->p.Rtube_ratio;
+    r.dzeta_sup = c->p.dzeta_sup;
+    r.eta = c->p.eta_t;
+    r.scale = scale;
+    return r;
 }
 
 double fixed_point_scale(const Ctx *c)
@@ -439,48 +552,47 @@ int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     }
 
     const size_t n3 = field_elems(c);
-    float *w = (float *)c->b_w.p;
-    FWT_TRY(buf_reserve(c, C.scratch[19], 64));
-    uint32_t *d_mm = (uint32_t *)((char *)C.scratch[19].p + 16);
-    mm_init_kernel<<<1, 32, 0, c->stream>>>(d_mm, 6);
+    const bool f64 = c->p.precision == 64;
+    const size_t rb = f64 ? 8 : 4;
+    char *w = (char *)c->b_w.p;
+    void *wx = w, *wy = w + n3 * rb, *wz = w + 2 * n3 * rb;
+    FWT_TRY(buf_reserve(c, C.scratch[19], 128));   // deposit_lines cleared the tallies at 64
+    void *d_mm = (char *)C.scratch[19].p + 16;
+    if (f64) mm_init64_kernel<<<1, 32, 0, c->stream>>>((unsigned long long *)d_mm, 6);
+    else mm_init_kernel<<<1, 32, 0, c->stream>>>((uint32_t *)d_mm, 6);
     const bool general = !(c->p.sigma_ratio == 1.0 && c->p.eta_t == 0.0);
     const bool accumulate = c->w_written;
     const double scale = fixed_point_scale(c);
+    RedoCtx rctx = redo_ctx(c, B, scale, false);
+    rctx.tally = (unsigned long long *)((char *)C.scratch[19].p + 64);
     km = kt_begin(c, KT_DEPOSIT);
-#define FWT_TILE_LAUNCH(G, A)                                                                              \
-    do {                                                                                                   \
-        FWT_CUDA(cudaFuncSetAttribute(deposit_tile_kernel<G, A>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                      (int)kDepSmem));                                                     \
-        deposit_tile_kernel<G, A><<<(unsigned)ntiles, kDepThreads, kDepSmem, c->stream>>>(                \
-            B.rec, N, ntx, nty, d_toff, d_list, scale, w, w + n3, w + 2 * n3, d_mm, d_err);                 \
+#define FWT_TILE_LAUNCH(G, A, D)                                                                          \
+    do {                                                                                                  \
+        FWT_CUDA(cudaFuncSetAttribute(deposit_tile_kernel<G, A, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                      (int)kDepSmem));                                                    \
+        deposit_tile_kernel<G, A, D><<<(unsigned)ntiles, kDepThreads, kDepSmem, c->stream>>>(             \
+            B.rec, N, ntx, nty, d_toff, d_list, scale, wx, wy, wz, d_mm, d_err, rctx);                     \
+        FWT_CUDA(cudaGetLastError());                                                                     \
     } while (0)
-    if (general) {
-        if (accumulate) FWT_TILE_LAUNCH(true, true); else FWT_TILE_LAUNCH(true, false);
+    if (f64) {
+        // the FP64 path evaluates every pair in FP64: the General distinction is only the FP32 one
+        if (accumulate) FWT_TILE_LAUNCH(true, true, true); else FWT_TILE_LAUNCH(true, false, true);
+    } else if (general) {
+        if (accumulate) FWT_TILE_LAUNCH(true, true, false); else FWT_TILE_LAUNCH(true, false, false);
     } else {
-        if (accumulate) FWT_TILE_LAUNCH(false, true); else FWT_TILE_LAUNCH(false, false);
+        if (accumulate) FWT_TILE_LAUNCH(false, true, false); else FWT_TILE_LAUNCH(false, false, false);
     }
 #undef FWT_TILE_LAUNCH
     kt_end(c, km);
     // algorithmic bytes: omega written once (read too when accumulating), one candidate id
     // and one record per (tile, sub-segment) pair
-    c->kbytes[KT_DEPOSIT] += (int64_t)(3 * n3 * 4 * (accumulate ? 2 : 1)) + npairs * (int64_t)(4 + sizeof(SegRec));
+    c->kbytes[KT_DEPOSIT] += (int64_t)(3 * n3 * rb * (accumulate ? 2 : 1)) + npairs * (int64_t)(4 + sizeof(SegRec));
     c->launches += 2;
-    FWT_CUDA(cudaGetLastError());
     c->w_written = true;
-    uint32_t hmm[6];
-    FWT_CUDA(cudaMemcpyAsync(hmm, d_mm, sizeof(hmm), cudaMemcpyDeviceToHost, c->stream));
     FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    FWT_TRY(read_dep_range(c, d_mm, f64));   // synchronises the stream
     if (herr & 2) return fail(FWT_E_TIMEOUT, "deposit: bulk copy wait ran out");
     if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
-    // every tile is rewritten in every batch, so the last batch's range is the field's range
-    c->wmin.assign(3, 0.f);
-    c->wmax.assign(3, 0.f);
-    for (int d = 0; d < 3; ++d) {
-        c->wmin[d] = ord2f(hmm[2 * d]);
-        c->wmax[d] = ord2f(hmm[2 * d + 1]);
-    }
-    c->wmm_valid = true;
     return 0;
 }
 

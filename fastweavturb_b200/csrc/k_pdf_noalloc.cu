@@ -14,13 +14,18 @@
 // (two streams, two host threads on one device) race on the array and give wrong results;
 // serialise them.
 //
-// Set-up: the array's host-side name is only a stand-in, not a device address.  The first
-// call on each device, with that device current, looks its address up once with
-// cudaGetSymbolAddress and caches it; that first call should come before any stream capture.
+// Set-up: the array's host-side name is only a stand-in, not a device address.  Every call,
+// with the caller's device current, looks the address up with cudaGetSymbolAddress (a lookup in
+// the already loaded module, so a context made anew after cudaDeviceReset gets its own array).
+// The first call in each CUDA context also loads every kernel of this entry point (CUDA loads
+// kernels lazily, and a load allocates device memory) and sets their shared-memory limit once,
+// so that later calls -- FP32 or FP64, any bin count -- allocate nothing; that first call
+// should come before any stream capture.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdint>
+#include <algorithm>
 #include <mutex>
 
 #include "k_common.cuh"
@@ -119,28 +124,63 @@ __global__ void __launch_bounds__(256) na_hist_kernel(const Real *__restrict__ a
         if (s_cnt[i]) atomicAdd(S->cnt + i, (unsigned long long)s_cnt[i]);
 }
 
-// device address of g_pdf_scratch, looked up once per device with that device current
-static PdfScratch *scratch_addr(int dev, int *rc)
+constexpr int kPdfNoAllocShmem = (int)(sizeof(float) * 2 + sizeof(uint32_t)) * kPdfNoAllocMaxBins;   // 96 KB
+
+// The current CUDA context (the driver's cuCtxGetCurrent, reached through the runtime so that
+// the library needs no link to libcuda); null if it cannot be had.
+static void *current_context()
+{
+    using GetCtx = int (*)(void **);
+    static GetCtx fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (GetCtx)f;
+        cudaGetLastError();
+    });
+    void *ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
+// Load every kernel of the entry point and set the histogram kernels' shared-memory limit to
+// the fixed maximum, once per context.
+static int prepare_context()
 {
     static std::mutex mu;
-    static PdfScratch *addr[256] = {nullptr};
-    *rc = 0;
-    if (dev < 0 || dev >= 256) {
-        *rc = fail(FWT_E_RANGE, "device ordinal above 255");
+    static void *done[64] = {nullptr};
+    static int ndone = 0;
+    void *ctx = current_context();
+    std::lock_guard<std::mutex> lk(mu);
+    for (int i = 0; i < ndone; ++i)
+        if (ctx && done[i] == ctx) return 0;
+    cudaFuncAttributes fa;
+    FWT_CUDA(cudaFuncGetAttributes(&fa, na_init_kernel));
+    FWT_CUDA(cudaFuncGetAttributes(&fa, na_edges_kernel));
+    FWT_CUDA(cudaFuncGetAttributes(&fa, na_clear_minmax_kernel<float>));
+    FWT_CUDA(cudaFuncGetAttributes(&fa, na_clear_minmax_kernel<double>));
+    FWT_CUDA(cudaFuncSetAttribute(na_hist_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPdfNoAllocShmem));
+    FWT_CUDA(cudaFuncSetAttribute(na_hist_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPdfNoAllocShmem));
+    if (ctx && ndone < 64) done[ndone++] = ctx;
+    return 0;
+}
+
+// device address of g_pdf_scratch in the current context
+static PdfScratch *scratch_addr(int *rc)
+{
+    *rc = prepare_context();
+    if (*rc) return nullptr;
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_pdf_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        *rc = fail(FWT_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         return nullptr;
     }
-    std::lock_guard<std::mutex> lk(mu);
-    if (!addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_pdf_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            *rc = fail(FWT_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            return nullptr;
-        }
-        addr[dev] = (PdfScratch *)p;
-    }
-    return addr[dev];
+    return (PdfScratch *)p;
 }
 
 }  // namespace fwt
@@ -160,7 +200,7 @@ extern "C" int fwt_pdf_noalloc(const void *d_data, int precision, int nx, int ny
     int dev = 0;
     FWT_CUDA(cudaGetDevice(&dev));
     int rc = 0;
-    PdfScratch *S = scratch_addr(dev, &rc);
+    PdfScratch *S = scratch_addr(&rc);
     if (!S) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     const size_t n = (size_t)nx * ny * nz;
@@ -172,22 +212,17 @@ extern "C" int fwt_pdf_noalloc(const void *d_data, int precision, int nx, int ny
     if (precision == 64) {
         na_clear_minmax_kernel<double><<<blocks, 256, 0, st>>>((const double *)d_data, n, scale, nbins, S);
         na_edges_kernel<<<(nbins + 255) / 256, 256, 0, st>>>(nbins, S);
-        FWT_CUDA(cudaFuncSetAttribute(na_hist_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shb));
         na_hist_kernel<double><<<blocks, 256, shb, st>>>((const double *)d_data, n, scale, nbins, S);
     } else {
         na_clear_minmax_kernel<float><<<blocks, 256, 0, st>>>((const float *)d_data, n, scale, nbins, S);
         na_edges_kernel<<<(nbins + 255) / 256, 256, 0, st>>>(nbins, S);
-        FWT_CUDA(cudaFuncSetAttribute(na_hist_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shb));
         na_hist_kernel<float><<<blocks, 256, shb, st>>>((const float *)d_data, n, scale, nbins, S);
     }
     FWT_CUDA(cudaGetLastError());
     // results to the caller's host arrays (plain copies, no staging buffers of ours)
     float rng[3];
     FWT_CUDA(cudaMemcpyAsync(rng, &S->vmin, sizeof(rng), cudaMemcpyDeviceToHost, st));
-    uint64_t *hc = counts;
-    uint64_t local[kPdfNoAllocMaxBins];
-    if (!hc) hc = local;
-    FWT_CUDA(cudaMemcpyAsync(hc, S->cnt, sizeof(uint64_t) * nbins, cudaMemcpyDeviceToHost, st));
+    if (counts) FWT_CUDA(cudaMemcpyAsync(counts, S->cnt, sizeof(uint64_t) * nbins, cudaMemcpyDeviceToHost, st));
     FWT_CUDA(cudaStreamSynchronize(st));
     // val and pdf in the reference's REAL(4) arithmetic (subroutine.f90:19,38)
     const float vmin = rng[0], bsz = rng[2];
@@ -195,12 +230,24 @@ extern "C" int fwt_pdf_noalloc(const void *d_data, int precision, int nx, int ny
     den = (float)(den * (float)nx);
     den = (float)(den * (float)ny);
     den = (float)(den * (float)nz);
-    for (int l = 0; l < nbins; ++l) {
-        if (val) {
+    if (val)
+        for (int l = 0; l < nbins; ++l) {
             const float prod = (float)((float)l * bsz);
             val[l] = (float)((double)vmin + 0.5 * (double)bsz + (double)prod);
         }
-        if (pdf) pdf[l] = (float)((float)hc[l] / den);
+    if (pdf) {
+        // the counts pass through a small stack chunk when the caller wants no count array
+        constexpr int kChunk = 256;
+        uint64_t chunk[kChunk];
+        for (int l0 = 0; l0 < nbins; l0 += kChunk) {
+            const int m = std::min(kChunk, nbins - l0);
+            const uint64_t *hc = counts ? counts + l0 : chunk;
+            if (!counts) {
+                FWT_CUDA(cudaMemcpyAsync(chunk, S->cnt + l0, sizeof(uint64_t) * m, cudaMemcpyDeviceToHost, st));
+                FWT_CUDA(cudaStreamSynchronize(st));
+            }
+            for (int i = 0; i < m; ++i) pdf[l0 + i] = (float)((float)hc[i] / den);
+        }
     }
     return 0;
 }

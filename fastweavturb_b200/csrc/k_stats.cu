@@ -12,23 +12,36 @@
 
 namespace fwt {
 
+// Component range, exact in the field's precision: FP32 values through order-preserving
+// 32-bit atomics, FP64 values through 64-bit ones (mm: two words of the value's width).
 template <typename Real>
-__global__ void minmax_kernel(const Real *__restrict__ a, size_t n, uint32_t *__restrict__ mm)
+__global__ void minmax_kernel(const Real *__restrict__ a, size_t n, void *__restrict__ mm)
 {
-    float mn = 3.4e38f, mx = -3.4e38f;
+    Real mn = (Real)3.4e38f, mx = (Real)-3.4e38f;
+    if (sizeof(Real) == 8) {
+        mn = (Real)1.7e308;
+        mx = (Real)-1.7e308;
+    }
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const float v = (float)a[i];
-        mn = fminf(mn, v);
-        mx = fmaxf(mx, v);
+        const Real v = a[i];
+        mn = fmin(mn, v);
+        mx = fmax(mx, v);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     }
     if ((threadIdx.x & 31) == 0) {
-        atomicMin(mm, f2ord(mn));
-        atomicMax(mm + 1, f2ord(mx));
+        if constexpr (sizeof(Real) == 8) {
+            unsigned long long *m = (unsigned long long *)mm;
+            atomicMin(m, d2ord((double)mn));
+            atomicMax(m + 1, d2ord((double)mx));
+        } else {
+            uint32_t *m = (uint32_t *)mm;
+            atomicMin(m, f2ord((float)mn));
+            atomicMax(m + 1, f2ord((float)mx));
+        }
     }
 }
 
@@ -63,16 +76,25 @@ __global__ void __launch_bounds__(256) pdf_kernel(const Real *__restrict__ a, si
         if (s_cnt[i]) atomicAdd(counts + i, (unsigned long long)s_cnt[i]);
 }
 
-// Structure functions along one axis.  A block stages W = min(32, N) lines of length N in
-// shared memory as [pos][line] (padded), then warp w accumulates, for its separations,
-// sum (du * s)^p for p = 1..PMAX in registers.  axis 0: u_x along x; 1: u_y along y;
+// Structure functions along one axis.  A block stages W lines of length N in shared memory
+// as [pos][line] (padded), in the field's own precision, then warp w accumulates, for its
+// separations, sum (du * s)^p for p = 1..PMAX in registers.  W = 32 lines for FP32 fields and
+// 16 for FP64 (a 1024-point FP64 group still fits one block's shared memory); groups at the end
+// of an axis may hold fewer lines, so any N works.  axis 0: u_x along x; 1: u_y along y;
 // 2: u_z along z.
+template <typename Real>
+__host__ __device__ constexpr int sp_lines(int N)
+{
+    return N < (sizeof(Real) == 8 ? 16 : 32) ? N : (sizeof(Real) == 8 ? 16 : 32);
+}
+
 template <typename Real, int PMAX, int MPW>
 __global__ void __launch_bounds__(256) sp_kernel(const Real *__restrict__ u, int N, int axis, double s,
                                                  const int *__restrict__ rs, int nr, double *__restrict__ Sp)
 {
-    extern __shared__ float tile[];   // N x (W + 1)
-    const int W = N < 32 ? N : 32;
+    extern __shared__ __align__(16) unsigned char sp_smem[];
+    Real *tile = reinterpret_cast<Real *>(sp_smem);   // N x (W + 1)
+    const int W = sp_lines<Real>(N);
     const int ld = W + 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     double acc[MPW][PMAX];
@@ -86,31 +108,35 @@ __global__ void __launch_bounds__(256) sp_kernel(const Real *__restrict__ u, int
         const int m = warp + a * nwarps;
         rr[a] = m < nr ? rs[m] % N : -1;
     }
-    const int64_t ngroups = (int64_t)N * N / W;
+    // axis 0: groups of W consecutive x-rows (row = y + N z); axes 1, 2: groups of W
+    // consecutive x at fixed z (axis 1) or fixed y (axis 2)
+    const int xgroups = (N + W - 1) / W;
+    const int64_t ngroups = axis == 0 ? ((int64_t)N * N + W - 1) / W : (int64_t)xgroups * N;
     for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
         __syncthreads();
-        // stage
+        int nl;   // lines of this group
         if (axis == 0) {
-            // lines are x-rows y0..y0+W-1 at fixed z
-            const int64_t row0 = g * W;   // row index = y + N z
-            for (int e = threadIdx.x; e < N * W; e += blockDim.x) {
+            const int64_t row0 = g * W;
+            nl = (int)min((int64_t)W, (int64_t)N * N - row0);
+            for (int e = threadIdx.x; e < N * nl; e += blockDim.x) {
                 const int x = e % N, l = e / N;
-                tile[x * ld + l] = (float)u[(size_t)(row0 + l) * N + x];
+                tile[x * ld + l] = u[(size_t)(row0 + l) * N + x];
             }
         } else {
-            // lines along y (fixed z) or z (fixed y), at x0..x0+W-1
-            const int xg = (int)(g % (N / W)), o = (int)(g / (N / W));
+            const int xg = (int)(g % xgroups), o = (int)(g / xgroups);
             const int x0 = xg * W;
+            nl = min(W, N - x0);
             for (int e = threadIdx.x; e < N * W; e += blockDim.x) {
                 const int l = e % W, pos = e / W;
+                if (l >= nl) continue;
                 size_t gi;
                 if (axis == 1) gi = (size_t)(x0 + l) + (size_t)N * ((size_t)pos + (size_t)N * o);
                 else gi = (size_t)(x0 + l) + (size_t)N * ((size_t)o + (size_t)N * pos);
-                tile[pos * ld + l] = (float)u[gi];
+                tile[pos * ld + l] = u[gi];
             }
         }
         __syncthreads();
-        if (lane < W) {
+        if (lane < nl) {
 #pragma unroll
             for (int a = 0; a < MPW; ++a) {
                 const int r = rr[a];
@@ -159,10 +185,12 @@ __global__ void field_wh_kernel(const Real *__restrict__ w, const Real *__restri
     }
 }
 
-__global__ void mm_init2(uint32_t *mm, int n)
+__global__ void mm_init2(void *mm, int n, int wide)
 {
     const int i = threadIdx.x;
-    if (i < n) mm[i] = (i & 1) ? 0u : 0xffffffffu;
+    if (i >= n) return;
+    if (wide) ((unsigned long long *)mm)[i] = (i & 1) ? 0ull : ~0ull;
+    else ((uint32_t *)mm)[i] = (i & 1) ? 0u : 0xffffffffu;
 }
 
 static unsigned grid_for(Ctx *c, size_t n, int per_sm = 8)
@@ -172,33 +200,35 @@ static unsigned grid_for(Ctx *c, size_t n, int per_sm = 8)
     return (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)sms * per_sm));
 }
 
-// raw component ranges of u (which = 1) or omega (which = 0)
+// raw component ranges of u (which = 1) or omega (which = 0), exact in the field's precision
 int stats_minmax(Ctx *c, int which)
 {
     const size_t n3 = field_elems(c);
     void *f = which ? c->b_u.p : c->b_w.p;
-    FWT_TRY(buf_reserve(c, c->scratch[19], 64));
-    uint32_t *mm = (uint32_t *)((char *)c->scratch[19].p + 16);
+    const bool wide = c->p.precision == 64;
+    FWT_TRY(buf_reserve(c, c->scratch[19], 128));
+    char *mm = (char *)c->scratch[19].p + 16;
     const int km = kt_begin(c, KT_STATS);
-    mm_init2<<<1, 32, 0, c->stream>>>(mm, 6);
+    mm_init2<<<1, 32, 0, c->stream>>>(mm, 6, wide ? 1 : 0);
     for (int d = 0; d < 3; ++d) {
-        if (c->p.precision == 64)
-            minmax_kernel<double><<<grid_for(c, n3), 256, 0, c->stream>>>((const double *)f + d * n3, n3, mm + 2 * d);
+        if (wide)
+            minmax_kernel<double><<<grid_for(c, n3), 256, 0, c->stream>>>((const double *)f + d * n3, n3, mm + 16 * d);
         else
-            minmax_kernel<float><<<grid_for(c, n3), 256, 0, c->stream>>>((const float *)f + d * n3, n3, mm + 2 * d);
+            minmax_kernel<float><<<grid_for(c, n3), 256, 0, c->stream>>>((const float *)f + d * n3, n3, mm + 8 * d);
     }
     kt_end(c, km);
     c->launches += 4;
     FWT_CUDA(cudaGetLastError());
-    uint32_t h[6];
-    FWT_CUDA(cudaMemcpyAsync(h, mm, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    unsigned long long h[6];
+    FWT_CUDA(cudaMemcpyAsync(h, mm, wide ? 48 : 24, cudaMemcpyDeviceToHost, c->stream));
     FWT_CUDA(cudaStreamSynchronize(c->stream));
-    std::vector<float> &mn = which ? c->umin : c->wmin, &mx = which ? c->umax : c->wmax;
-    mn.assign(3, 0.f);
-    mx.assign(3, 0.f);
+    std::vector<double> &mn = which ? c->umin : c->wmin, &mx = which ? c->umax : c->wmax;
+    mn.assign(3, 0.0);
+    mx.assign(3, 0.0);
+    const uint32_t *h32 = (const uint32_t *)h;
     for (int d = 0; d < 3; ++d) {
-        mn[d] = ord2f(h[2 * d]);
-        mx[d] = ord2f(h[2 * d + 1]);
+        mn[d] = wide ? ord2d(h[2 * d]) : (double)ord2f(h32[2 * d]);
+        mx[d] = wide ? ord2d(h[2 * d + 1]) : (double)ord2f(h32[2 * d + 1]);
     }
     if (which) c->umm_valid = true;
     else c->wmm_valid = true;
@@ -242,16 +272,17 @@ int stats_pdf(Ctx *c, int which, int comp, int nbins, float *val, float *pdf, ui
     const bool is_u = which == 0;
     if (is_u && !c->umm_valid) FWT_TRY(stats_minmax(c, 1));
     if (!is_u && !c->wmm_valid) FWT_TRY(stats_minmax(c, 0));
-    const std::vector<float> &mn = is_u ? c->umin : c->wmin, &mx = is_u ? c->umax : c->wmax;
+    const std::vector<double> &mn = is_u ? c->umin : c->wmin, &mx = is_u ? c->umax : c->wmax;
     const double s = 1.0 / c->up;
-    float rmin = 3.4e38f, rmax = -3.4e38f;
+    double rmin = 1.7e308, rmax = -1.7e308;
     for (int d = 0; d < 3; ++d) {
         if (comp >= 0 && d != comp) continue;
         rmin = std::min(rmin, mn[d]);
         rmax = std::max(rmax, mx[d]);
     }
-    // range of the scaled REAL(4) values: rounding is monotone, so it is the scaled range
-    const float vmin = (float)((double)rmin * s), vmax = (float)((double)rmax * s);
+    // range of the scaled REAL(4) values (float)(x s): rounding is monotone, so it is the
+    // rounded scaled range of the exact raw values
+    const float vmin = (float)(rmin * s), vmax = (float)(rmax * s);
     std::vector<float> hval, hlo, hhi;
     float bsz;
     pdf_layout(vmin, vmax, nbins, hval, hlo, hhi, bsz);
@@ -264,6 +295,16 @@ int stats_pdf(Ctx *c, int which, int comp, int nbins, float *val, float *pdf, ui
     const size_t n3 = field_elems(c);
     const void *f = is_u ? c->b_u.p : c->b_w.p;
     const size_t shb = sizeof(float) * 2 * nbins + sizeof(uint32_t) * nbins;
+    // 8192 bins take 96 KB of shared memory, above the default 48 KB: the limit is raised to
+    // the device's opt-in maximum, the same value for every context (the attribute belongs to
+    // the kernel, for the whole process)
+    int optin = 0;
+    FWT_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
+    if (shb > (size_t)optin) return fail(FWT_E_RANGE, "pdf: bins exceed one block's shared memory");
+    if (c->p.precision == 64)
+        FWT_CUDA(cudaFuncSetAttribute(pdf_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    else
+        FWT_CUDA(cudaFuncSetAttribute(pdf_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     const int km = kt_begin(c, KT_STATS);
     for (int d = 0; d < 3; ++d) {
         if (comp >= 0 && d != comp) continue;
@@ -301,8 +342,8 @@ int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp)
     if (pmax < 1 || pmax > 10) return fail(FWT_E_ARG, "Sp: pmax must be 1..10");
     if (nr < 1 || nr > 64) return fail(FWT_E_ARG, "Sp: nr must be 1..64");
     const int N = c->p.N;
-    const int W = N < 32 ? N : 32;
-    if (N % W) return fail(FWT_E_ARG, "Sp: N must be a multiple of 32 (or below 32)");
+    const bool f64 = c->p.precision == 64;
+    const int W = f64 ? sp_lines<double>(N) : sp_lines<float>(N);
     for (int m = 0; m < nr; ++m)
         if (r[m] < 0) return fail(FWT_E_ARG, "Sp: negative separation");
     FWT_TRY(buf_reserve(c, c->scratch[9], sizeof(int) * 64 + sizeof(double) * 10 * 64 + 64));
@@ -312,10 +353,10 @@ int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp)
     FWT_CUDA(cudaMemsetAsync(d_sp, 0, sizeof(double) * 10 * nr, c->stream));
     const size_t n3 = field_elems(c);
     const double s = 1.0 / c->up;
-    const size_t shb = sizeof(float) * (size_t)N * (W + 1);
+    const size_t shb = (f64 ? sizeof(double) : sizeof(float)) * (size_t)N * (W + 1);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
-    const int64_t groups = (int64_t)N * N / W;
+    const int64_t groups = ((int64_t)N * N + W - 1) / W;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, (int64_t)sms * 4));
     const int mpw = (nr + 7) / 8;
     // The dynamic shared-memory limit is a property of the kernel for the whole process: every

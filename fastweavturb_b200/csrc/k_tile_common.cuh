@@ -4,7 +4,7 @@
 // accumulator (set-up and the coalesced epilogue).
 #pragma once
 
-#include "k_common.cuh"
+#include "k_deposit.cuh"
 
 namespace fwt {
 
@@ -239,6 +239,171 @@ __device__ __forceinline__ void tile_epilogue(long long (*acc)[kAccN], int N, in
         }
     }
 }
+
+// FP64 tile cells (the FP64 tile path): load the tile's current values or zero them.
+template <bool Accumulate>
+__device__ __forceinline__ void tile_acc_init_f64(double (*acc)[kAccN], int N, int x0, int y0, int z0,
+                                                  const double *__restrict__ wx, const double *__restrict__ wy,
+                                                  const double *__restrict__ wz)
+{
+    for (int p = threadIdx.x; p < TP; p += blockDim.x) {
+        const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
+        const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        if (Accumulate && gx < N && gy < N && gz < N) {
+            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
+            a0 = wx[g];
+            a1 = wy[g];
+            a2 = wz[g];
+        }
+        const int pa = lx + kSY * ly + kSZ * lz;
+        acc[0][pa] = a0;
+        acc[1][pa] = a1;
+        acc[2][pa] = a2;
+    }
+}
+
+// FP64 tile store (coalesced double2 stores) and the exact component min/max (64-bit ordered
+// atomics, mm: 6 words).
+__device__ __forceinline__ void tile_epilogue_f64(double (*acc)[kAccN], int N, int x0, int y0, int z0,
+                                                  double *__restrict__ wx, double *__restrict__ wy,
+                                                  double *__restrict__ wz, unsigned long long *__restrict__ mm)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    double mn[3] = {1.7e308, 1.7e308, 1.7e308}, mx[3] = {-1.7e308, -1.7e308, -1.7e308};
+    const bool full = (x0 + TX <= N) && (y0 + TY <= N) && (z0 + TZ <= N);
+    if (full) {
+        for (int q2 = tid; q2 < TP / 2; q2 += blockDim.x) {
+            const int p = 2 * q2;
+            const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
+            const size_t g = (size_t)(x0 + lx) + (size_t)N * ((size_t)(y0 + ly) + (size_t)N * (z0 + lz));
+            const int pa = lx + kSY * ly + kSZ * lz;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double2 v2;
+                v2.x = acc[d][pa];
+                v2.y = acc[d][pa + 1];
+                double *w = d == 0 ? wx : (d == 1 ? wy : wz);
+                *reinterpret_cast<double2 *>(w + g) = v2;
+                mn[d] = fmin(mn[d], fmin(v2.x, v2.y));
+                mx[d] = fmax(mx[d], fmax(v2.x, v2.y));
+            }
+        }
+    } else {
+        for (int p = tid; p < TP; p += blockDim.x) {
+            const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
+            const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
+            if (gx >= N || gy >= N || gz >= N) continue;
+            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const double v1 = acc[d][lx + kSY * ly + kSZ * lz];
+                double *w = d == 0 ? wx : (d == 1 ? wy : wz);
+                w[g] = v1;
+                mn[d] = fmin(mn[d], v1);
+                mx[d] = fmax(mx[d], v1);
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        for (int o2 = 16; o2 > 0; o2 >>= 1) {
+            mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o2));
+            mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o2));
+        }
+        if (lane == 0) {
+            atomicMin(mm + 2 * d, d2ord(mn[d]));
+            atomicMax(mm + 2 * d + 1, d2ord(mx[d]));
+        }
+    }
+}
+
+// The FP64 tile path's evaluation of a candidate pair: the reference's FP64 tests of
+// tube.f90:806-818 at the 1-based unwrapped grid index (ip, jp, kp) of sub-segment q's own box,
+// and, if it passes, the reference's FP64 vorticity (tube.f90:819-892) added into the double
+// cell p.
+__device__ __forceinline__ bool eval_pair_f64(const RedoCtx &R, int64_t q, int ip, int jp, int kp,
+                                              double (*acc)[kAccN], int p)
+{
+    const SubSeg &S = R.seg[q];
+    double m[3], t0, t1;
+    ref_mesh_f64(dev_pi2() / R.N, ip, jp, kp, m);
+    if (!ref_tests_f64(S, m, t0, t1)) return false;
+    const int slot = S.slot;
+    const LineParam P = R.lp[R.slot_line[slot]];
+    double v[3];
+    ref_value_f64(S, P, R.coe + 18 * (size_t)slot, R.dtf[slot], R.dzeta_sup, R.eta, m, t0, t1, v);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) atomicAdd(&acc[d][p], v[d]);
+    return true;
+}
+
+// Index along one axis in the box of a sub-segment whose lower corner is lo, of the grid
+// point with unwrapped index i in another frame (the two differ by whole periods).
+__device__ __forceinline__ int box_index(int i, int lo, int N)
+{
+    int o = (i - lo) % N;
+    if (o < 0) o += N;
+    return lo + o;
+}
+
+__global__ void mm_init64_kernel(unsigned long long *mm, int n);
+int read_dep_range(Ctx *c, const void *d_mm, bool f64);
+
+
+// ---------------------------------------------------------------- FP64 redo of ill-conditioned pairs
+// A warp queues the accepted (point, chord) pairs whose curved-branch amplification
+// |1/(1 - kappa rho cos theta)| exceeds kRedoCond (tube.f90:876-879: the FP32 value carries the
+// amplified rounding of kappa, rho and cos theta) and evaluates them 32 at a time, one per
+// lane, in the reference's FP64 arithmetic from the batch's FP64 spline data (redo_pair_f64),
+// adding the fixed-point result into the same tile cells.  Only tubes with a varying core or
+// a twist reach this path: with a constant core and no twist the vorticity has no curvature
+// term.
+struct RedoQueue {
+    uint2 e[64];   // x: record id | chord << 26; y: tile-local point x | y << 4 | z << 7
+};
+
+__device__ __forceinline__ uint32_t redo_code(int lx, int ly, int lz)
+{
+    return (uint32_t)lx | ((uint32_t)ly << 4) | ((uint32_t)lz << 7);
+}
+
+// Append the lanes' flagged pairs (at most 32) to the queue; rn is warp-uniform and stays
+// below 64 when the caller drains at 32.
+__device__ __forceinline__ void redo_push(RedoQueue &Q, int lane, bool flag, uint32_t rec, uint32_t code, int &rn)
+{
+    const unsigned bal = __ballot_sync(0xffffffffu, flag);
+    if (flag) Q.e[rn + __popc(bal & ((1u << lane) - 1u))] = make_uint2(rec, code);
+    rn += __popc(bal);
+    __syncwarp();
+}
+
+// Evaluate the first cnt queued pairs in FP64 and drop them from the queue.
+__device__ __forceinline__ void redo_drain(RedoQueue &Q, const RedoCtx &R, long long (*acc)[kAccN], int lane, int cnt,
+                                           int &rn, int x0, int y0, int z0, int *__restrict__ err)
+{
+    if (lane < cnt) {
+        const uint2 e = Q.e[lane];
+        const int lx = (int)(e.y & 15u), ly = (int)((e.y >> 4) & 7u), lz = (int)(e.y >> 7);
+        long long q[3];
+        if (!redo_pair_f64(R, e.x & ((1u << 26) - 1u), (int)(e.x >> 26), x0 + lx, y0 + ly, z0 + lz, q))
+            atomicOr(err, 4);
+        const int p = lx + kSY * ly + kSZ * lz;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)q[d]);
+    }
+    if (lane == 0 && R.tally) atomicAdd(R.tally + 1, (unsigned long long)cnt);
+    __syncwarp();
+    const int rem = rn - cnt;
+    const uint2 keep = lane < rem ? Q.e[cnt + lane] : make_uint2(0u, 0u);
+    __syncwarp();
+    if (lane < rem) Q.e[lane] = keep;
+    __syncwarp();
+    rn = rem;
+}
+
+// The redo context of a batch (records: sub-segments, or chord pieces when `pieces`).
+RedoCtx redo_ctx(const Ctx *c, const CenterlineBatch &B, double scale, bool pieces);
 
 // Shared kernels of the binning (defined in k_deposit_tile.cu).
 __global__ void tile_scatter_kernel(const uint32_t *__restrict__ key, const uint32_t *__restrict__ val, int64_t n,

@@ -129,6 +129,12 @@ int fwt_field_wh(fwt_ctx *ctx, float *host_out);
 /* Copy a normalised (after fwt_normalize) or raw field to the host as doubles,
  * column-major.  which = 0: omega, 1: u; component 0..2. */
 int fwt_copy_field(fwt_ctx *ctx, int which, int component, double *host_colmajor);
+/* Device address of a field held by the context: three N^3 arrays (components x, y, z, each
+ * column-major, x fastest) of the context's precision (float or double), raw (unnormalised:
+ * divide by u' of fwt_normalize for the normalised field).  Valid until the next call that
+ * rebuilds the field or fwt_destroy; the caller must not free it.  (No counterpart in the
+ * reference, whose fields are Fortran arrays of the caller; this gives zero-copy access.) */
+int fwt_field_device(fwt_ctx *ctx, int which, void **ptr);
 /* Write the reference's output tree under outdir: parameters_output.dat,
  * centerline_output.dat, info.dat, test_data.dat, field_wh.dat, stat/spectrum_vor_temp.dat,
  * stat/spectrum.dat, stat/pdf_um.dat, stat/pdf_wm.dat, stat/Sp.dat (tube.f90:171,226-258,
@@ -164,7 +170,9 @@ int fwt_set_outputs(fwt_ctx *ctx, int u_out, int d_out);
 int fwt_field_uw(fwt_ctx *ctx, float *host_out);
 int fwt_field_wd(fwt_ctx *ctx, float *host_out);
 /* Counters of the last deposition: c[0] lines, c[1] sections, c[2] sub-segments,
- * c[3] candidate (tile, sub-segment) pairs, c[4] kernel launches of the last fwt_run. */
+ * c[3] candidate (tile, record) pairs, c[4] kernel launches of the last fwt_run, c[5] accepted
+ * (grid point, sub-segment) pairs, i.e. vorticity evaluations, c[6] of those, the pairs the
+ * FP32 path evaluated in FP64 because of their curved-branch amplification. */
 int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
 
 /* Tuning knobs of the context (no counterpart in the reference).  FWT_TUNE_PIECE_RT_CELLS:

@@ -22,9 +22,11 @@ def oracle_inputs(O, w, line_e=None):
 
 
 def gpu_params(F, w, precision=32, deposit_mode=0, **kw):
-    return F.Params(N=w.N, N_downsample=w.N, line_s=1, line_e=w.ntubes, sigma_ratio=w.sigma_ratio, eta_t=w.eta_t,
-                    ntf_times=w.ntf_times, ntf_pre=w.ntf_pre, Rtube_ratio=w.Rtube_ratio, dzeta_sup=w.dzeta_sup,
-                    precision=precision, deposit_mode=deposit_mode, **kw)
+    a = dict(N=w.N, N_downsample=w.N, line_s=1, line_e=w.ntubes, sigma_ratio=w.sigma_ratio, eta_t=w.eta_t,
+             ntf_times=w.ntf_times, ntf_pre=w.ntf_pre, Rtube_ratio=w.Rtube_ratio, dzeta_sup=w.dzeta_sup,
+             precision=precision, deposit_mode=deposit_mode)
+    a.update(kw)
+    return F.Params(**a)
 
 
 def rel_l2(a, b):

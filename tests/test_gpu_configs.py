@@ -1,0 +1,124 @@
+"""Parity on the benchmark workloads themselves, against the FP64 oracle.
+
+* cfg0 whole (64^3, 3 levels, 84 tubes, 74,752 nodes): omega, u, E(k) of omega and u, the
+  normalisation, S_p for p = 2..6 on the reference's separations, the downsampled field
+  output and the numbers of info.dat; FP32 tile path <= 1e-5, FP64 path <= 1e-12.
+* cfg1 (256^3, 6 levels) bounded to the first two tubes of every level (the oracle walks the
+  whole box of every sub-segment; the full 5,460 tubes take it about an hour): omega through
+  both tile kernels, FP32 <= 1e-5 and FP64 <= 1e-12.
+
+Tolerances are relative L2 norms over every grid point (S_p: relative error per entry).
+"""
+import numpy as np
+import pytest
+
+from helpers import gpu_params, oracle_inputs, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 1e-5
+TOL64 = 1e-12
+
+
+@pytest.fixture(scope="module")
+def cfg0_case(orc):
+    from fastweavturb_b200.configs import cfg0
+
+    w = cfg0(seed=0)
+    p, cl = oracle_inputs(orc, w)
+    p.N_downsample = w.N // 4
+    return w, p, cl, orc.run(p, cl)
+
+
+@pytest.mark.parametrize("precision,mode,tol", [(32, 0, TOL32), (64, 0, TOL64), (64, 1, TOL64)])
+def test_cfg0_whole_field_matches_oracle(fwt, orc, cfg0_case, precision, mode, tol):
+    w, p, cl, ref = cfg0_case
+    ctx = fwt.Context(gpu_params(fwt, w, precision=precision, deposit_mode=mode, N_downsample=w.N // 4))
+    ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+    ctx.run()
+    assert ctx.counters()["lines"] == 84
+    assert rel_l2(ctx.field(0), ref["vor"]) <= tol
+    assert rel_l2(ctx.field(1), ref["vel"]) <= tol
+    s = ctx.cal_helicity()
+    assert s["up"] == pytest.approx(ref["up"], rel=tol)
+    assert s["Enstrophy"] == pytest.approx(ref["Enstrophy"], rel=tol)
+    assert s["Etot"] == pytest.approx(1.5, rel=tol)      # Etot / u'^2 = 3/2 after normalisation
+    assert rel_l2(ctx.spectrum(0), ref["spectrum_vor"]) <= tol
+    assert rel_l2(ctx.spectrum(1), ref["spectrum"]) <= tol
+    r, Sp = ctx.Sp_calculate(pmax=10)
+    assert np.array_equal(r, ref["Sp_r"])
+    for q in range(1, 6):   # S_2 .. S_6
+        np.testing.assert_allclose(Sp[q], ref["Sp"][q], rtol=tol * 10 if q >= 3 else tol)
+    # the downsampled field output (N_downsample = N / 4): REAL(4) values of FP64 or FP32 fields
+    fw = ctx.output_v()
+    assert fw.shape == ref["field_wh"].shape == (2, 16, 16, 16)
+    assert rel_l2(fw[0], ref["field_wh"][0]) <= max(tol, 1e-7)
+    assert rel_l2(fw[1], ref["field_wh"][1]) <= max(tol, 1e-7)
+    ctx.close()
+
+
+def test_cfg0_sp_fp64_to_fp64_rounding(fwt, orc, cfg0_case):
+    """The FP64 path's S_p from its own u: the oracle applied to that same u agrees to FP64
+    rounding (the increments are staged in FP64)."""
+    w, p, cl, ref = cfg0_case
+    ctx = fwt.Context(gpu_params(fwt, w, precision=64, deposit_mode=0))
+    ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+    ctx.run()
+    ctx.cal_helicity()
+    vel = ctx.field(1)
+    r, Sp = ctx.Sp_calculate(pmax=10)
+    r_o, Sp_o = orc.structure_functions(vel, pmax=10, nthreads=4)
+    assert np.array_equal(r, r_o)
+    for q in range(10):
+        scale = np.abs(Sp_o[q]).max()
+        assert np.abs(Sp[q] - Sp_o[q]).max() <= 1e-12 * scale, q
+    ctx.close()
+
+
+def test_cfg0_info_dat_numbers(fwt, orc, cfg0_case, tmp_path):
+    """info.dat carries the run's numbers (tube.f90:1193-1210): N, the total centerline length,
+    Gamma_1 / u', the twist, Etot / u'^2 and the enstrophy."""
+    w, p, cl, ref = cfg0_case
+    ctx = fwt.Context(gpu_params(fwt, w, precision=32, deposit_mode=0, N_downsample=w.N // 4))
+    ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+    ctx.run()
+    ctx.write_outputs(tmp_path / "output")
+    rows = {}
+    for ln in (tmp_path / "output" / "info.dat").read_text().splitlines():
+        if "=" in ln:
+            k, v = ln.split("=", 1)
+            if v.strip():
+                rows[k.strip()] = float(v.replace("D", "E").replace("d", "e"))
+    length = sum(2 * np.pi * orc.line_prep(cl.line(i))[3] for i in range(len(cl.npoint)))
+    assert rows["N"] == w.N
+    assert rows["Total length of curve"] == pytest.approx(length, rel=1e-12)
+    assert rows["Gamma_1"] == pytest.approx(p.Gamma[0] / ref["up"], rel=TOL32)
+    assert rows["twist eta"] == 0.0
+    assert rows["Etot"] == pytest.approx(1.5, rel=TOL32)
+    assert rows["Enstrophy"] == pytest.approx(ref["Enstrophy"], rel=TOL32)
+    assert rows["up_temp"] == pytest.approx(ref["up"], rel=TOL32)
+    ctx.close()
+
+
+@pytest.fixture(scope="module")
+def cfg1_bounded(orc):
+    from fastweavturb_b200.configs import cfg1
+
+    w = cfg1(seed=0)
+    for L in w.levels:
+        L.tubes = min(L.tubes, 2)
+    p, cl = oracle_inputs(orc, w)
+    vor, _ = orc.deposit(p, cl)
+    return w, p, cl, vor
+
+
+@pytest.mark.parametrize("precision,mode,tol", [(32, 0, TOL32), (64, 0, TOL64)])
+def test_cfg1_first_tubes_of_every_level(fwt, cfg1_bounded, precision, mode, tol):
+    """Levels 0-2 (truncation radius 12-49 grid spacings) take the sub-segment kernel, levels
+    3-5 (1.5-6.1 grid spacings) the chord-piece kernel."""
+    w, p, cl, vor = cfg1_bounded
+    ctx = fwt.Context(gpu_params(fwt, w, precision=precision, deposit_mode=mode))
+    ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+    ctx.deposit()
+    assert rel_l2(ctx.field(0), vor) <= tol
+    ctx.close()

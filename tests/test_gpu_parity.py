@@ -32,7 +32,7 @@ def _gpu_run(F, w, cl, p, precision, mode):
     return ctx
 
 
-@pytest.mark.parametrize("precision,mode,tol", [(32, 0, TOL32), (32, 1, TOL32), (64, 1, TOL64)])
+@pytest.mark.parametrize("precision,mode,tol", [(32, 0, TOL32), (32, 1, TOL32), (64, 1, TOL64), (64, 0, TOL64)])
 def test_fields_match_oracle(fwt, small_case, precision, mode, tol):
     w, p, cl, ref = small_case
     ctx = _gpu_run(fwt, w, cl, p, precision, mode)
@@ -43,12 +43,12 @@ def test_fields_match_oracle(fwt, small_case, precision, mode, tol):
     assert e_w <= tol, f"omega rel L2 {e_w:.3e}"
     assert e_u <= tol, f"u rel L2 {e_u:.3e}"
     norm = ctx.cal_helicity()
-    assert abs(norm["up"] - ref["up"]) <= tol * ref["up"] * 10
-    assert abs(norm["Enstrophy"] - ref["Enstrophy"]) <= tol * ref["Enstrophy"] * 10
+    assert abs(norm["up"] - ref["up"]) <= tol * ref["up"]
+    assert abs(norm["Enstrophy"] - ref["Enstrophy"]) <= tol * ref["Enstrophy"]
     ew = ctx.spectrum(0)
     eu = ctx.spectrum(1)
-    assert rel_l2(ew, ref["spectrum_vor"]) <= tol * 10
-    assert rel_l2(eu, ref["spectrum"]) <= tol * 10
+    assert rel_l2(ew, ref["spectrum_vor"]) <= tol
+    assert rel_l2(eu, ref["spectrum"]) <= tol
     ctx.close()
 
 
@@ -106,50 +106,49 @@ def test_ntf_bit_exact_across_curvatures(fwt, orc, H, dB_over_sigma):
 def test_piece_and_subsegment_kernels_agree(fwt, orc):
     """Thin tubes (Rtube 1.2-1.9 grid spacings on 64^3) deposited by the chord-piece kernel and
     by the sub-segment kernel: the same accepted points, evaluated by two forms of the same
-    vorticity, agree to FP32 rounding; both match the FP64 oracle on the well-conditioned
-    points."""
+    vorticity, agree to FP32 rounding; both match the FP64 oracle on every point, and so do
+    both kernels of the FP64 tile path at FP64 rounding."""
     from fastweavturb_b200.configs import small
     w = small(N=64, seed=5, nlev=2, tubes0=3, nodes0=128, sigma0=0.04)
     p, cl = oracle_inputs(orc, w)
     fields = {}
-    for cells in (0.0, 8.0):
-        ctx = fwt.Context(gpu_params(fwt, w, precision=32, deposit_mode=0))
-        ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
-        ctx.set_piece_radius_limit(cells)
-        ctx.deposit(1, w.ntubes)
-        fields[cells] = ctx.field(0).copy()
-        ctx.close()
-    assert np.abs(fields[8.0]).max() > 0
-    assert rel_l2(fields[8.0], fields[0.0]) <= 1e-6
-    cond = np.zeros((w.N,) * 3)
-    vor, _ = orc.deposit(p, cl, cond=cond)
-    good = np.broadcast_to(cond <= 10.0, fields[8.0].shape)
-    assert good.mean() > 0.99
-    assert rel_l2(np.where(good, fields[8.0], 0), np.where(good, vor, 0)) <= TOL32
+    for precision in (32, 64):
+        for cells in (0.0, 8.0):
+            ctx = fwt.Context(gpu_params(fwt, w, precision=precision, deposit_mode=0))
+            ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+            ctx.set_piece_radius_limit(cells)
+            ctx.deposit(1, w.ntubes)
+            fields[precision, cells] = ctx.field(0).copy()
+            ctx.close()
+    assert np.abs(fields[32, 8.0]).max() > 0
+    assert rel_l2(fields[32, 8.0], fields[32, 0.0]) <= 1e-6
+    vor, _ = orc.deposit(p, cl)
+    assert rel_l2(fields[32, 8.0], vor) <= TOL32
+    assert rel_l2(fields[32, 0.0], vor) <= TOL32
+    assert rel_l2(fields[64, 8.0], vor) <= TOL64
+    assert rel_l2(fields[64, 0.0], vor) <= TOL64
 
 
 @pytest.mark.parametrize("N", [36, 40])
 @pytest.mark.parametrize("piece_cells", [None, 0.0])
-def test_partial_tiles(fwt, orc, N, piece_cells):
+@pytest.mark.parametrize("precision,tol", [(32, TOL32), (64, TOL64)])
+def test_partial_tiles(fwt, orc, N, piece_cells, precision, tol):
     """Grids that are not a multiple of the 16 x 8 x 8 deposition tile (N = 36: partial tiles
     along every axis; N = 40: along x only), through the chord-piece kernel (default) and the
-    sub-segment kernel (piece_cells = 0): omega matches the FP64 oracle on the well-conditioned
-    points (curved-branch amplification <= 10) and the spectral path matches on the same omega."""
+    sub-segment kernel (piece_cells = 0), in FP32 and in the FP64 tile path: omega matches the
+    FP64 oracle on every point."""
     from fastweavturb_b200.configs import small
     w = small(N=N, seed=9, nlev=2, tubes0=2, nodes0=64, sigma0=0.2)
     p, cl = oracle_inputs(orc, w)
-    ctx = fwt.Context(gpu_params(fwt, w, precision=32, deposit_mode=0))
+    ctx = fwt.Context(gpu_params(fwt, w, precision=precision, deposit_mode=0))
     ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
     if piece_cells is not None:
         ctx.set_piece_radius_limit(piece_cells)
     ctx.deposit(1, w.ntubes)
     vor = ctx.field(0).copy()
-    cond = np.zeros((N,) * 3)
-    vor_o, _ = orc.deposit(p, cl, cond=cond)
-    good = np.broadcast_to(cond <= 10.0, vor.shape)
-    assert good.mean() > 0.99
+    vor_o, _ = orc.deposit(p, cl)
     assert np.abs(vor).max() > 0
-    assert rel_l2(vor[good], vor_o[good]) <= TOL32
+    assert rel_l2(vor, vor_o) <= tol
     ctx.close()
 
 

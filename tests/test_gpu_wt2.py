@@ -2,9 +2,10 @@
 general deposition branch with a varying core and twisted tubes) through the CUDA path, at
 N = 64, against the FP64 oracle and the committed golden fixture.
 
-Tolerances: FP32 path <= 1e-5 relative L2 on omega and u, FP64 path <= 1e-12, both on the
-well-conditioned points (see the wt2 fixture); the spectral path and the statistics are
-compared on the GPU's own fields (PDF counts bit-exact, S_p to FP64 rounding).
+Tolerances: FP32 path <= 1e-5 relative L2 on omega and u over every grid point; FP64 path
+<= 1e-7 over every grid point (see the wt2 fixture for why FP64 cannot do better on this
+input); the spectral path and the statistics are compared on the GPU's own fields (PDF counts
+bit-exact, S_p to FP64 rounding).
 """
 import os
 
@@ -17,7 +18,8 @@ from test_golden import GOLD, write_reference_inputs, wt2_inputs
 pytestmark = pytest.mark.gpu
 
 TOL32 = 1e-5
-TOL64 = 1e-10    # FP64: operation order and contraction differ from the oracle's (observed ~1e-12)
+TOL64 = 1e-10    # FP64 spectral path on the same omega: operation order differs from the oracle's
+TOL64_DEPOSIT = 1e-7   # FP64 deposition on every point of this ill-conditioned input (see wt2)
 
 
 def _params(F, p, precision, mode, N=64):
@@ -26,47 +28,38 @@ def _params(F, p, precision, mode, N=64):
                     precision=precision, deposit_mode=mode)
 
 
-COND_MAX = 10.0
-
-
 @pytest.fixture(scope="module")
 def wt2(orc):
     """Inputs, the oracle's whole run, its raw omega and the curved-branch amplification
     cond = max |1/(1 - kappa rho cos theta)| per point (tube.f90:876-879).  Near the centre of
     curvature of bends tighter than the tube radius the reference's FP64 value itself is
-    ill-conditioned (the error of any evaluation grows as cond^2): at N = 64 the 819 points
-    with cond > 10 (0.3 %) hold 87 % of the enstrophy, and no FP32 evaluation can agree with
-    FP64 there.  Parity is therefore measured on the points with cond <= 10, and the FP64
-    path is also held to 1e-7 on all points."""
+    ill-conditioned: at N = 64 the 819 points with cond > 10 (0.3 %) hold 87 % of the
+    enstrophy.  The FP32 path evaluates the pairs with cond > 4 in the reference's FP64
+    arithmetic, so it is held to 1e-5 on every point; two FP64 evaluations that differ only in
+    operation order already differ by ~1e-8 there, hence TOL64_DEPOSIT."""
     p, cl = wt2_inputs(orc)
     cond = np.zeros((p.N,) * 3)
     vor_raw, _ = orc.deposit(p, cl, cond=cond)
     return p, cl, orc.run(p, cl), vor_raw, cond
 
 
-def _masked_rel(a, b, mask):
-    m = np.broadcast_to(mask, a.shape)
-    return rel_l2(a[m], b[m])
-
-
 @pytest.mark.parametrize("precision,mode,tol,piece_cells", [(32, 0, TOL32, None), (32, 0, TOL32, 0.0),
-                                                             (32, 1, TOL32, None), (64, 1, TOL64, None),
-                                                             (64, 0, TOL64, None)])
+                                                             (32, 1, TOL32, None), (64, 1, TOL64_DEPOSIT, None),
+                                                             (64, 0, TOL64_DEPOSIT, None),
+                                                             (64, 0, TOL64_DEPOSIT, 0.0)])
 def test_wt2_omega_matches_oracle(fwt, wt2, precision, mode, tol, piece_cells):
-    """piece_cells 0 sends every line through the sub-segment kernel (by default the WT2 tubes,
-    1.8-7.4 grid spacings thick at 64^3, all take the chord-piece kernel)."""
+    """Every grid point, the ill-conditioned ones included.  piece_cells 0 sends every line
+    through the sub-segment kernel (by default the WT2 tubes, 1.8-7.4 grid spacings thick at
+    64^3, all take the chord-piece kernel)."""
     p, cl, ref, vor_raw, cond = wt2
+    assert (cond > 10).sum() > 100        # the ill-conditioned points are there
     ctx = fwt.Context(_params(fwt, p, precision, mode))
     ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T, p.if_filter)
     if piece_cells is not None:
         ctx.set_piece_radius_limit(piece_cells)
     ctx.deposit()
     vor = ctx.field(0)                 # raw (not yet normalised)
-    good = cond <= COND_MAX
-    assert good.mean() > 0.99
-    assert _masked_rel(vor, vor_raw, good) <= tol
-    if precision == 64:
-        assert rel_l2(vor, vor_raw) <= 1e-7        # all points, ill-conditioned ones included
+    assert rel_l2(vor, vor_raw) <= tol
     ctx.close()
 
 
@@ -89,11 +82,11 @@ def test_wt2_spectral_path_matches_oracle_on_the_same_omega(fwt, orc, wt2, preci
     w_o = w.copy()
     s_o = orc.normalise(w_o, u_o.copy())
     assert rel_l2(u, u_o) <= tol
-    assert rel_l2(ew, ew_o) <= 10 * tol
-    assert s["up"] == pytest.approx(s_o["up"], rel=10 * tol)
-    assert s["Etot"] == pytest.approx(s_o["Etot"], rel=10 * tol)
-    assert s["Enstrophy"] == pytest.approx(s_o["Enstrophy"], rel=10 * tol)
-    assert rel_l2(eu, orc.spectrum(u_o / s_o["up"])) <= 10 * tol
+    assert rel_l2(ew, ew_o) <= tol
+    assert s["up"] == pytest.approx(s_o["up"], rel=tol)
+    assert s["Etot"] == pytest.approx(s_o["Etot"], rel=tol)
+    assert s["Enstrophy"] == pytest.approx(s_o["Enstrophy"], rel=tol)
+    assert rel_l2(eu, orc.spectrum(u_o / s_o["up"])) <= tol
     ctx.close()
 
 
@@ -104,8 +97,7 @@ def test_wt2_fp64_matches_golden_fixture(fwt, orc, wt2):
     ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T, p.if_filter)
     ctx.run()
     vor = ctx.field(0)[:, ::4, ::4, ::4]
-    good = np.broadcast_to(cond[::4, ::4, ::4] <= COND_MAX, vor.shape)
-    np.testing.assert_allclose(vor[good], g["vor_sample"][good], rtol=1e-7, atol=1e-9)
+    assert rel_l2(vor, g["vor_sample"]) <= TOL64_DEPOSIT
     s = ctx.cal_helicity()
     np.testing.assert_allclose([s["up"], s["Etot"], s["Enstrophy"]], g["scalars"], rtol=1e-7)
     ctx.close()
