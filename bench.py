@@ -5,23 +5,26 @@ One step = one woven field built from centerlines already on the device: centerl
 (periodic arc length, quintic splines, adaptive sub-segmentation), Burgers-tube deposition,
 spectral Biot-Savart omega -> u with E(k), normalisation, PDFs, S_p(r) and the downsampled
 field output, i.e. the reference program's tube.f90:392-1188 (its file writing excluded).
+The default workload is the 1024^3, 8-level field (cfg2).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config cfg1] [--precision 32]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config cfg2] [--precision 32]
     python bench.py --impl reference ...      # the CPU implementation of the path (see below)
 
 metric  "woven Mpts/s": N^3 grid points per step / step time, summed over ranks.
-value   device time (CUDA events on the library's stream), centerline nodes resident in HBM.
+value   FP32 device time (CUDA events on the library's stream), centerline nodes resident in HBM.
 e2e     the same metric through the public C-ABI from pinned host memory: the host->device
         copy of the nodes, the whole path, and the device->host copy of the statistics and of
-        the downsampled field each step.
+        the downsampled field each step (min(K, 3) steps unless --e2e-steps).
+fp64    the same workload through the FP64 tile path (--fp64-steps fields): its Mpts/s, the
+        FP32 / FP64 ratio and the FP32 errors against it (relative L2 of omega, u and E(k),
+        relative errors of S_2..S_6).
 Multi-GPU: the path does not shard (one field per GPU); each rank builds its own
 realisation (seed = rank) -- replicas, weak scaling.  No data-path collective.
 
 The reference arm (--impl reference) times the FP64 CPU restatement of the reference
-(oracle/, the Fortran reference cannot be compiled in this image) on the host cores: each
-step deposits a bounded sample of the workload's lines (the first tube of every level),
-scales each level by its tube count, and adds the full-size spectral path and statistics
-(S_p on two separations scaled to all), giving an estimated whole-field time.
+(oracle/; the Fortran reference cannot be compiled in this image) on the host cores: each
+step is a bounded sample (the first tube of every level on a reduced grid, the spectral path
+and statistics at <= 256^3), scaled to an estimated whole-field time.
 """
 from __future__ import annotations
 
@@ -118,10 +121,46 @@ def whole_job_rate(world, steps, N, ms):
 
 
 # --------------------------------------------------------------------------- CPU sample
+# Algorithmic bytes of the path (per grid point, FP32): omega written 12; R2C reads 12, writes the
+# half spectrum 12; the fused Biot-Savart / spectra / energy pass reads and writes it (24); C2R
+# reads 12, writes 12; statistics and the field output read u and omega (24) and write <= 8:
+# 116 B per point (232 in FP64).  Deposition adds the centerline data: about 200 B per node
+# (coordinates, arc length, derivatives, the section's spline and sub-segment set-up).
+PATH_BYTES_PER_POINT = {32: 116, 64: 232}
+DEPOSIT_BYTES_PER_POINT = {32: 12, 64: 24}
+BYTES_PER_NODE = 200
+
+
+def level_sample_grid(w, L):
+    """Grid of the CPU sample of level L: the box walk of the reference costs (box points per
+    sub-segment) x (sub-segments), and its boxes span 2 Rtube + a chord, so on a grid N' with
+    Rtube >= 4 grid spacings the cost of a tube scales as (N / N')^3.  The smallest such grid
+    (at least 64) bounds the sample; levels thinner than that keep the workload's grid."""
+    Rt = w.Rtube_ratio * L.sigma * w.sigma_ratio
+    n = 64
+    while n < w.N and Rt * n / (2 * np.pi) < 4.0:
+        n *= 2
+    return min(n, w.N)
+
+
+_SAMPLE_GRIDS = {}
+
+
+def _sample_field(n):
+    """One (3, n, n, n) FP64 array per sample grid, kept across samples: the deposition only adds
+    into it, so its contents do not matter to the timing, and allocating 26 GB per 1024^3 sample
+    would cost more than the deposition."""
+    if n not in _SAMPLE_GRIDS:
+        _SAMPLE_GRIDS[n] = np.zeros((3, n, n, n))
+    return _SAMPLE_GRIDS[n]
+
+
 def cpu_sample_estimate(w, nthreads=None):
-    """Estimated FP64 CPU time (s) of one whole woven field of workload `w` with the oracle:
-    deposition of the first tube of each level scaled by the level's tube count, plus the
-    full-size spectral path, PDFs and S_p (two separations scaled to all)."""
+    """Estimated FP64 CPU time (s) of one whole woven field of workload `w` with the oracle,
+    from a bounded sample: the first tube of every level deposited on the level's sample grid
+    (level_sample_grid) and scaled by (N / N')^3 and the level's tube count; the spectral path,
+    the PDFs and S_p (two separations, scaled to all) on a grid of at most 256^3, scaled by the
+    FFT's N^3 log N or the statistics' N^3."""
     from oracle import oracle as O
 
     O.build()
@@ -129,39 +168,48 @@ def cpu_sample_estimate(w, nthreads=None):
     O.set_fft_workers(nthreads)
     N = w.N
     t_dep = 0.0
-    vor = np.zeros((3, N, N, N))
     t0 = 0
     for L in w.levels:
+        n = level_sample_grid(w, L)
         xyz = O.fbb_tube(w.seed, t0, L.nodes, L.H, L.dB)
-        p = O.Params(N=N, N_downsample=N, line_s=1, line_e=1, sigma_ratio=w.sigma_ratio, eta_t=w.eta_t,
+        p = O.Params(N=n, N_downsample=n, line_s=1, line_e=1, sigma_ratio=w.sigma_ratio, eta_t=w.eta_t,
                      ntf_times=w.ntf_times, ntf_pre=w.ntf_pre, Rtube_ratio=w.Rtube_ratio, dzeta_sup=w.dzeta_sup,
                      sigma=np.array([L.sigma]), Gamma=np.array([L.Gamma]), n_T=np.array([1], dtype=np.int32),
                      if_filter=np.zeros(1, dtype=np.int32))
         cl = O.Centerlines(npoint=np.array([L.nodes]), xyz=xyz)
         t = time.perf_counter()
-        O.deposit(p, cl, nthreads=nthreads, vor=vor)
-        t_dep += (time.perf_counter() - t) * L.tubes
+        O.deposit(p, cl, nthreads=nthreads, vor=_sample_field(n))
+        t_dep += (time.perf_counter() - t) * L.tubes * (N / n) ** 3
         t0 += L.tubes
+    ns = min(N, 256)
+    rng = np.random.default_rng(0)
+    vor = rng.standard_normal((3, ns, ns, ns))
     t = time.perf_counter()
     O.spectrum(vor)
     vel = O.biot_savart(vor)
     O.normalise(vor, vel)
     O.spectrum(vel)
-    t_spec = time.perf_counter() - t
+    t_spec = (time.perf_counter() - t) * (N / ns) ** 3 * np.log(N ** 3) / np.log(ns ** 3)
     t = time.perf_counter()
-    O.pdf(vel.astype(np.float32).reshape(3 * N, N, N))
-    O.pdf(vor.astype(np.float32).reshape(3 * N, N, N))
-    t_pdf = time.perf_counter() - t
-    rr = O.sp_separations(N)
+    O.pdf(vel.astype(np.float32).reshape(3 * ns, ns, ns))
+    O.pdf(vor.astype(np.float32).reshape(3 * ns, ns, ns))
+    t_pdf = (time.perf_counter() - t) * (N / ns) ** 3
+    rr = O.sp_separations(ns)
     t = time.perf_counter()
     O.structure_functions(vel, pmax=10, r=rr[:2], nthreads=nthreads)
-    t_sp = (time.perf_counter() - t) * len(rr) / 2.0   # cost is linear in the number of separations
+    t_sp = (time.perf_counter() - t) / 2.0 * len(O.sp_separations(N)) * (N / ns) ** 3
     est = t_dep + t_spec + t_pdf + t_sp
-    return est, {"deposit_s": t_dep, "spectral_s": t_spec, "stats_s": t_pdf + t_sp, "threads": nthreads}
+    grids = [level_sample_grid(w, L) for L in w.levels]
+    return est, {"deposit_s": t_dep, "spectral_s": t_spec, "stats_s": t_pdf + t_sp, "threads": nthreads,
+                 "sample": f"FP64 oracle: the first tube of every level deposited on grids {grids} and scaled by "
+                           f"(N/N')^3 x tubes; spectral path, PDFs and S_p (2 separations) at {ns}^3 scaled to "
+                           f"{N}^3 (N^3 log N, N^3, separations); estimated whole field {est:.1f} s"}
 
 
 def run_reference(args):
-    """The reference arm: the oracle's FP64 CPU path on the host cores (rank 0 only)."""
+    """The reference arm: the oracle's FP64 CPU path on the host cores (rank 0 only).  Each
+    step is one bounded sample (cpu_sample_estimate); ms_per_step is its measured wall time and
+    value the whole-field throughput estimated from it."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -169,26 +217,24 @@ def run_reference(args):
 
     w = CONFIGS[args.config](seed=0)
     nthreads = os.cpu_count() or 1
-    # one untimed sample warms the caches and builds the oracle; more would only cost minutes
-    for _ in range(min(args.warmup, 1)):
+    for _ in range(min(args.warmup, 1)):   # builds the oracle and warms the caches
         cpu_sample_estimate(w, nthreads)
-    ests = []
-    t0 = time.perf_counter()
+    ests, walls = [], []
     for _ in range(args.steps):
-        e, _ = cpu_sample_estimate(w, nthreads)
+        t = time.perf_counter()
+        e, parts = cpu_sample_estimate(w, nthreads)
+        walls.append(time.perf_counter() - t)
         ests.append(e)
-    wall = time.perf_counter() - t0
     est = float(np.mean(ests))
     val = w.N ** 3 / est / 1e6
     line = {
         "impl": "reference", "metric": "woven Mpts/s", "value": val, "unit": "Mpts/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": est * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded fBb centerlines)",
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(walls)) * 1e3,
+        "estimated_field_ms": est * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded fBb centerlines)",
         "config": {"workload": w.name, "N": w.N, "lines": w.ntubes, "nodes": w.nnodes},
         "cpu_baseline": {"value": val, "unit": "Mpts/s", "cores": nthreads, "kind": "port",
-                         "sample": "first tube of every level deposited and scaled by tube count; full-size FFT "
-                                   "path, PDFs, S_p at 2 separations scaled; estimated whole-field seconds "
-                                   f"{est:.2f}, sample wall {wall / max(args.steps, 1):.1f} s/step"},
+                         "sample": parts["sample"] + "; ms_per_step is the sample's wall time"},
         "e2e": {"value": val, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -196,15 +242,55 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------------------- GPU arm
+def timed_runs(ctx, stream, steps, torch):
+    """Device ms of `steps` whole runs (CUDA events on the library's stream), the summed
+    per-category kernel times, and the launches of this library's kernels."""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ktimes, launches = {}, 0
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.run()
+        for k, (ms, n) in ctx.kernel_times().items():
+            a = ktimes.setdefault(k, [0.0, 0])
+            a[0] += ms
+            a[1] += n
+        launches += ctx.counters()["launches"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), ktimes, launches
+
+
+def rel_l2_device(a, b, torch):
+    """||a - b|| / ||b|| of two device fields (3, N, N, N) of any precision, in FP64, by z-slabs."""
+    num = den = 0.0
+    for c in range(3):
+        for z in range(0, a.shape[1], 64):
+            x = a[c, z:z + 64].double()
+            y = b[c, z:z + 64].double()
+            num += float(torch.sum((x - y) ** 2))
+            den += float(torch.sum(y * y))
+    return (num / den) ** 0.5 if den > 0 else float("nan")
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fwt", choices=["fwt", "reference"])
-    ap.add_argument("--config", default="cfg1")
+    ap.add_argument("--config", default="cfg2")
     ap.add_argument("--precision", type=int, default=32)
     ap.add_argument("--deposit-mode", type=int, default=0)
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="steps of the end-to-end leg (default: min(steps, 3))")
+    ap.add_argument("--fp64-steps", type=int, default=1,
+                    help="fields of the FP64 leg (FP64 tile path, same workload): its Mpts/s and the FP32 "
+                         "errors against it; 0 skips the leg")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--level", type=int, default=None,
@@ -232,22 +318,30 @@ def main():
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    w = CONFIGS[args.config](seed=rank)
-    if args.level is not None:
-        w.levels = [w.levels[args.level]]
-        w.name += f" -- level {args.level} only (profiling case)"
-        if args.lines:
-            w.levels[0].tubes = min(w.levels[0].tubes, args.lines)
-            w.name += f", first {w.levels[0].tubes} lines"
-    stream = torch.cuda.current_stream()
-    params = F.Params(N=w.N, N_downsample=w.N, line_s=1, line_e=w.ntubes, sigma_ratio=w.sigma_ratio,
-                      eta_t=w.eta_t, ntf_times=w.ntf_times, ntf_pre=w.ntf_pre, Rtube_ratio=w.Rtube_ratio,
-                      dzeta_sup=w.dzeta_sup, precision=args.precision, deposit_mode=args.deposit_mode,
-                      device=local, stream=stream.cuda_stream)
-    ctx = F.Context(params)
-    xyz, (npoint, sig, gam, nT) = build_workload(ctx, w)
-    torch.cuda.synchronize()
+    def workload():
+        w = CONFIGS[args.config](seed=rank)
+        if args.level is not None:
+            w.levels = [w.levels[args.level]]
+            w.name += f" -- level {args.level} only (profiling case)"
+            if args.lines:
+                w.levels[0].tubes = min(w.levels[0].tubes, args.lines)
+                w.name += f", first {w.levels[0].tubes} lines"
+        return w
 
+    w = workload()
+    stream = torch.cuda.current_stream()
+
+    def make_ctx(precision, mode):
+        prm = F.Params(N=w.N, N_downsample=w.N, line_s=1, line_e=w.ntubes, sigma_ratio=w.sigma_ratio,
+                       eta_t=w.eta_t, ntf_times=w.ntf_times, ntf_pre=w.ntf_pre, Rtube_ratio=w.Rtube_ratio,
+                       dzeta_sup=w.dzeta_sup, precision=precision, deposit_mode=mode, device=local,
+                       stream=stream.cuda_stream)
+        ctx = F.Context(prm)
+        xyz, arrs = build_workload(ctx, w)
+        torch.cuda.synchronize()
+        return prm, ctx, xyz, arrs
+
+    params, ctx, xyz, (npoint, sig, gam, nT) = make_ctx(args.precision, args.deposit_mode)
     for _ in range(args.warmup):
         ctx.run()
     clocks = ClockSampler(local)
@@ -256,44 +350,40 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ktimes = {}
-    launches = 0
-    e0.record(stream)
-    for _ in range(args.steps):
-        ctx.run()
-        for k, (ms, n) in ctx.kernel_times().items():
-            a = ktimes.setdefault(k, [0.0, 0])
-            a[0] += ms
-            a[1] += n
-        launches += ctx.counters()["launches"]
-    e1.record(stream)
-    torch.cuda.synchronize()
+    ms, ktimes, launches = timed_runs(ctx, stream, args.steps, torch)
     if dist:
         dist.barrier()
     clocks.stop()
-    ms = e0.elapsed_time(e1)
     t_max = max_over_ranks(ms, dist, "cuda")
     ms_step = t_max / args.steps
     value = whole_job_rate(world, args.steps, w.N, t_max)
     counters = ctx.counters()
 
-    # dominant kernel and its roofline
+    # dominant kernel and its roofline (algorithmic bytes: deposition writes omega, 12 B per
+    # point, and reads the centerline data, about 200 B per node)
     peaks, pk_kind = measured_peaks()
-    dom = max(ktimes.items(), key=lambda kv: kv[1][0])
-    dom_name, (dom_ms, dom_n) = dom
-    dep_launches = ktimes.get("deposit", [0.0, 0])[1] // args.steps
-    kb = _kernel_bytes(ctx, w, counters, args.precision, dep_launches)
-    dom_bytes = kb.get(dom_name)
+    dom_name, (dom_ms, dom_n) = max(ktimes.items(), key=lambda kv: kv[1][0])
+    rb = 4 if args.precision == 32 else 8
+    step_bytes = {"deposit": DEPOSIT_BYTES_PER_POINT[args.precision] * w.N ** 3 + BYTES_PER_NODE * w.nnodes}
     roofline = None
     if dom_n:
+        launches_per_step = dom_n / args.steps
         avg_ms = dom_ms / dom_n
-        per_launch_bytes = (dom_bytes / max(1, ktimes[dom_name][1] // args.steps)) if dom_bytes else None
-        achieved = per_launch_bytes / (avg_ms / 1e3) / 1e9 if per_launch_bytes else None
+        per_launch = step_bytes.get(dom_name, 0) / launches_per_step if dom_name in step_bytes else None
+        achieved = per_launch / (avg_ms / 1e3) / 1e9 if per_launch else None
         roofline = {"kernel": dom_name, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
                     "unit": "GB/s", "frac": (achieved / peaks["hbm_gbs"]) if achieved else None,
-                    "traffic": None, "peak_kind": pk_kind, "avg_launch_ms": avg_ms,
-                    "share_of_step": dom_ms / max(ms, 1e-9)}
+                    "traffic": deposit_traffic(w, counters, launches_per_step) if dom_name == "deposit" else None,
+                    "peak_kind": pk_kind, "avg_launch_ms": avg_ms, "launches_per_step": launches_per_step,
+                    "algorithmic_bytes_per_launch": per_launch, "share_of_step": dom_ms / max(ms, 1e-9),
+                    "bytes_model": "12 B per grid point (omega) + 200 B per centerline node, per step"}
+        acc = counters.get("accepted", 0)
+        if dom_name == "deposit" and acc:
+            roofline["accepted_pairs_per_step"] = acc
+            roofline["accepted_pairs_per_s"] = acc / (dom_ms / args.steps / 1e3)
+    whole_path = {"bytes_per_step": PATH_BYTES_PER_POINT[args.precision] * w.N ** 3 + BYTES_PER_NODE * w.nnodes}
+    whole_path["achieved_gbs"] = whole_path["bytes_per_step"] / (ms_step / 1e3) / 1e9
+    whole_path["frac"] = whole_path["achieved_gbs"] / peaks["hbm_gbs"]
 
     # end to end through the public API from pinned host memory
     e2e = None
@@ -301,12 +391,13 @@ def main():
         host = xyz.T.contiguous().cpu().pin_memory()
         hx = host.numpy()
         nd = params.N_downsample
+        ne = args.e2e_steps or min(args.steps, 3)
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(ne):
             ctx.set_centerlines(npoint, hx, sig, gam, nT)
             ctx.run()
             ctx.output_v()
@@ -316,16 +407,46 @@ def main():
         h2d = int(hx.nbytes)
         d2h = int(2 * nd ** 3 * 4 + 2 * (w.N // 2) * 8 + 2 * params.pdf_bins * 8 * 2
                   + 10 * len(F.sp_separations(w.N)) * 8)
-        e2e = {"value": whole_job_rate(world, args.steps, w.N, ems), "unit": "Mpts/s",
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ems / args.steps}
+        e2e = {"value": whole_job_rate(world, ne, w.N, ems), "unit": "Mpts/s", "steps": ne,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ems / ne}
+        del host
+
+    # the FP64 leg: the same workload through the FP64 tile path; FP32 errors against it
+    fp64 = None
+    if args.fp64_steps > 0 and args.precision == 32 and world == 1:
+        ctx.run()
+        ew32, eu32 = ctx.spectrum(0), ctx.spectrum(1)
+        ctx.cal_helicity()
+        _, sp32 = ctx.Sp_calculate(pmax=10)
+        w32 = ctx.field_tensor(0).clone()
+        u32 = ctx.field_tensor(1).clone()
+        ctx.close()
+        del xyz
+        torch.cuda.synchronize()
+        _, ctx64, xyz64, _ = make_ctx(64, 0)
+        ms64, kt64, _ = timed_runs(ctx64, stream, args.fp64_steps, torch)
+        ew64, eu64 = ctx64.spectrum(0), ctx64.spectrum(1)
+        ctx64.cal_helicity()
+        _, sp64 = ctx64.Sp_calculate(pmax=10)
+        err = {"omega_rel_l2": rel_l2_device(w32, ctx64.field_tensor(0), torch),
+               "u_rel_l2": rel_l2_device(u32, ctx64.field_tensor(1), torch),
+               "Ek_omega_rel_l2": rel_l2(ew32, ew64), "Ek_u_rel_l2": rel_l2(eu32, eu64)}
+        for q in range(1, 6):
+            err[f"S{q + 1}_rel"] = float(np.max(np.abs(sp32[q] - sp64[q]) / np.abs(sp64[q])))
+        v64 = whole_job_rate(1, args.fp64_steps, w.N, ms64)
+        fp64 = {"value": v64, "unit": "Mpts/s", "steps": args.fp64_steps, "ms_per_step": ms64 / args.fp64_steps,
+                "path": "FP64 tile path (FP32 candidate tests, the reference's FP64 tests and arithmetic)",
+                "fp32_over_fp64": value / v64, "errors_fp32_vs_fp64": err,
+                "kernel_ms_per_step": {k: v[0] / args.fp64_steps for k, v in kt64.items()}}
+        ctx64.close()
+        del w32, u32, xyz64
+        ctx = None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         est, parts = cpu_sample_estimate(w)
         cpu = {"value": w.N ** 3 / est / 1e6, "unit": "Mpts/s", "cores": parts["threads"], "kind": "port",
-               "sample": "FP64 oracle: first tube of every level deposited and scaled by the level's tube count, "
-                         "full-size spectral path and statistics (S_p on 2 separations scaled to all); "
-                         f"estimated whole-field {est:.1f} s"}
+               "sample": parts["sample"]}
 
     if rank == 0:
         line = {
@@ -335,46 +456,45 @@ def main():
             "data": "synthetic (seeded fBb centerlines generated on the GPU)",
             "config": {"workload": w.name, "N": w.N, "lines": w.ntubes, "nodes": w.nnodes,
                        "sections": counters["sections"], "subsegments": counters["subsegments"],
-                       "cell_pairs": counters["pairs"], "precision": args.precision,
+                       "cell_pairs": counters["pairs"], "accepted_pairs": counters["accepted"],
+                       "precision": args.precision,
                        "deposit": "tile-owned cell lists" if args.deposit_mode == 0 else "reference box walk",
                        "l2": "inputs larger than L2 (omega, u, spectra, sub-segment records >> 126 MB)",
                        "parallelism": f"replicas x{world}"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks.summary(),
+            "roofline": roofline, "whole_path_roofline": whole_path, "cpu_baseline": cpu, "e2e": e2e,
+            "fp64": fp64, "gpu_launches": launches, "clocks": clocks.summary(),
             "kernel_ms_per_step": {k: v[0] / args.steps for k, v in ktimes.items()},
         }
         print(json.dumps(line))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
-    ctx.close()
+    if ctx is not None:
+        ctx.close()
     return 0
 
 
-def _kernel_bytes(ctx, w, counters, precision, dep_launches):
-    """Algorithmic bytes per step of each kernel category: section presampling reads the node
-    data and writes coefficients; the deposition writes omega in its first launch, reads and
-    writes it in each later launch (one launch per batch of lines), and reads one 224-byte
-    sub-segment record plus a 4-byte cell-list entry per (tile, sub-segment) pair; the fused
-    Biot-Savart reads and writes the half spectrum once."""
-    N = w.N
-    rb = 4 if precision == 32 else 8
-    n3 = N ** 3
-    nh = N * N * (N // 2 + 1)
-    secs = counters["sections"] + counters["lines"]
-    subseg_record = 224
-    field = 3 * n3 * rb * (1 + 2 * max(0, dep_launches - 1))
-    return {
-        "section_presample": secs * (3 * 8 + 6 * 8 + 8) + secs * (18 * 8 + 4 + 8),
-        "deposit": field + counters["pairs"] * (4 + subseg_record) if counters["pairs"]
-        else counters["subsegments"] * subseg_record + field,
-        "biot_savart": 2 * 3 * nh * 2 * rb,
-        "cufft": 6 * 3 * n3 * rb * 2,
-        "statistics": 3 * n3 * rb * 4,
-        "centerline_setup": counters["subsegments"] * (subseg_record + 8 * 8),
-        "binning": counters["pairs"] * 8 * 3 + counters["subsegments"] * subseg_record,
-        "generator": 0,
-    }
+def deposit_traffic(w, counters, launches_per_step):
+    """DRAM bytes per deposition launch from the ncu capture summarised in
+    profiles/deposit_traffic.txt (bytes per accepted pair and per grid point of a bounded case,
+    scaled to this workload's per-launch counts), or None without that summary."""
+    path = os.path.join(ROOT, "profiles", "deposit_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    vals = {}
+    with open(path) as f:
+        for ln in f:
+            if ":" in ln and not ln.startswith("#"):
+                k, v = ln.split(":", 1)
+                try:
+                    vals[k.strip()] = float(v.split()[0])
+                except (ValueError, IndexError):
+                    pass
+    if "bytes_per_accepted_pair" not in vals or "bytes_per_grid_point" not in vals:
+        return None
+    per_step = vals["bytes_per_accepted_pair"] * counters.get("accepted", 0) + \
+        vals["bytes_per_grid_point"] * w.N ** 3
+    return per_step / max(launches_per_step, 1)
 
 
 if __name__ == "__main__":

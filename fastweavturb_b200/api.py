@@ -56,7 +56,7 @@ EXPORTS = [
     "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_set_centerlines",
     "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
     "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_field_uw", "fwt_field_wd",
-    "fwt_set_outputs", "fwt_copy_field", "fwt_field_device",
+    "fwt_set_outputs", "fwt_copy_field", "fwt_field_device", "fwt_vsf_deviation", "fwt_helicity",
     "fwt_write_outputs", "fwt_run_dir", "fwt_run",
     "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
     "fwt_set_tuning", "fwt_mlp_create", "fwt_mlp_destroy", "fwt_mlp_nparams", "fwt_mlp_get_params", "fwt_mlp_set_params",
@@ -99,6 +99,8 @@ def library(path: str | None = None):
         "fwt_set_outputs": [vp, ip, ip],
         "fwt_copy_field": [vp, ip, ip, dp],
         "fwt_field_device": [vp, ip, ctypes.POINTER(vp)],
+        "fwt_vsf_deviation": [vp, vp, dp],
+        "fwt_helicity": [vp, dp],
         "fwt_write_outputs": [vp, ctypes.c_char_p],
         "fwt_run_dir": [ctypes.c_char_p, ctypes.POINTER(_Params)],
         "fwt_run": [vp],
@@ -341,6 +343,19 @@ class Context:
         library().fwt_counters(self._h, _ptr(v, ctypes.c_int64), 7)
         return {"lines": int(v[0]), "sections": int(v[1]), "subsegments": int(v[2]), "pairs": int(v[3]),
                 "launches": int(v[4]), "accepted": int(v[5]), "redone_fp64": int(v[6])}
+
+    def vsf_deviation(self, phi_ptr=None):
+        """cal_deviation (subroutine.f90:1519-1546) of omega against the scalar field at device
+        address phi_ptr (N^3, the context's precision), or against |omega| when None."""
+        out = ctypes.c_double()
+        _check(library().fwt_vsf_deviation(self._h, phi_ptr, ctypes.byref(out)))
+        return out.value
+
+    def helicity(self):
+        """Total helicity sum(omega . u) dv (cal_helicity of omega and u, subroutine.f90:1550-1569)."""
+        out = ctypes.c_double()
+        _check(library().fwt_helicity(self._h, ctypes.byref(out)))
+        return out.value
 
     def field_tensor(self, which):
         """Zero-copy torch view (3, N, N, N), index [c, z, y, x], of the raw (unnormalised)

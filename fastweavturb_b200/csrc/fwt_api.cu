@@ -432,6 +432,22 @@ int fwt_field_wh(fwt_ctx *h, float *host_out)
     return stats_field_wh(c, host_out);
 }
 
+int fwt_vsf_deviation(fwt_ctx *h, const void *d_phi, double *deviation)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !deviation) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    return diag_vsf_deviation(c, d_phi, deviation);
+}
+
+int fwt_helicity(fwt_ctx *h, double *helicity)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !helicity) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    return diag_helicity(c, helicity);
+}
+
 int fwt_field_device(fwt_ctx *h, int which, void **ptr)
 {
     Ctx *c = (Ctx *)h;

@@ -172,6 +172,10 @@ int stats_field_uw(Ctx *c, float *host_out);
 int stats_field_wd(Ctx *c, float *host_out);
 int stats_copy_field(Ctx *c, int which, int comp, double *host);
 
+// diagnostics (k_diag.cu)
+int diag_vsf_deviation(Ctx *c, const void *d_phi, double *deviation);
+int diag_helicity(Ctx *c, double *helicity);
+
 // host I/O (fwt_io.cpp)
 int io_read_centerlines(const char *path, std::vector<int64_t> &npoint, std::vector<double> &xyz);
 int io_read_params(const char *path, int nline, fwt_params &p, std::vector<double> &sigma,

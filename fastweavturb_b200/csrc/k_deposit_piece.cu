@@ -553,11 +553,15 @@ template <bool General, bool Accumulate, bool F64>
 __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel(
     const PieceRec *__restrict__ rec, int N, int ntx, int nty, const int64_t *__restrict__ tile_off,
     const uint32_t *__restrict__ list, double scale, void *__restrict__ wx, void *__restrict__ wy,
-    void *__restrict__ wz, void *__restrict__ mm, int *__restrict__ err, const RedoCtx redo)
+    void *__restrict__ wz, int *__restrict__ err, const RedoCtx redo)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     long long(*acc)[kAccN] = reinterpret_cast<long long(*)[kAccN]>(dsm);
     const int tile = blockIdx.x;
+    const int64_t c0 = tile_off[tile], c1 = tile_off[tile + 1];
+    // a tile that no record of this batch meets keeps its values: earlier batches wrote them,
+    // or the field was cleared before the first
+    if (c0 == c1) return;
     const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
     const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -573,7 +577,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
     else
         tile_acc_init<Accumulate>(acc, N, x0, y0, z0, scale, (const float *)wx, (const float *)wy, (const float *)wz);
     __syncthreads();
-    const int64_t c0 = tile_off[tile], c1 = tile_off[tile + 1];
+
     const int nchunks = (int)((c1 - c0 + kPChunk - 1) / kPChunk);
     const float fscale = (float)scale;
     const float fmaxq = 4.0e18f;
@@ -811,9 +815,9 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
     __syncthreads();
     if constexpr (F64)
         tile_epilogue_f64(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, (double *)wx, (double *)wy,
-                          (double *)wz, (unsigned long long *)mm);
+                          (double *)wz);
     else
-        tile_epilogue(acc, N, x0, y0, z0, scale, (float *)wx, (float *)wy, (float *)wz, (uint32_t *)mm);
+        tile_epilogue(acc, N, x0, y0, z0, scale, (float *)wx, (float *)wy, (float *)wz);
 }
 
 // ------------------------------------------------------------------------------ host
@@ -916,9 +920,6 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     char *w = (char *)c->b_w.p;
     void *wx = w, *wy = w + n3 * rb, *wz = w + 2 * n3 * rb;
     FWT_TRY(buf_reserve(c, C.scratch[19], 128));   // deposit_lines cleared the tallies at 64
-    void *d_mm = (char *)C.scratch[19].p + 16;
-    if (f64) mm_init64_kernel<<<1, 32, 0, c->stream>>>((unsigned long long *)d_mm, 6);
-    else mm_init_kernel<<<1, 32, 0, c->stream>>>((uint32_t *)d_mm, 6);
     const bool general = !(c->p.sigma_ratio == 1.0 && c->p.eta_t == 0.0);
     const bool accumulate = c->w_written;
     const double scale = fixed_point_scale(c);
@@ -930,7 +931,7 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
         FWT_CUDA(cudaFuncSetAttribute(deposit_piece_kernel<G, A, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                       (int)kPieceSmem));                                                   \
         deposit_piece_kernel<G, A, D><<<(unsigned)ntiles, kDepThreads, kPieceSmem, c->stream>>>(          \
-            B.piece, N, ntx, nty, d_toff, d_list, scale, wx, wy, wz, d_mm, d_err, rctx);                    \
+            B.piece, N, ntx, nty, d_toff, d_list, scale, wx, wy, wz, d_err, rctx);                    \
         FWT_CUDA(cudaGetLastError());                                                                      \
     } while (0)
     if (f64) {
@@ -948,7 +949,10 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     c->launches += 2;
     c->w_written = true;
     FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    FWT_TRY(read_dep_range(c, d_mm, f64));   // synchronises the stream
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    // tiles without candidates keep their values, so the field's range is taken when it is
+    // needed (stats_minmax)
+    c->wmm_valid = false;
     if (herr & 2) return fail(FWT_E_TIMEOUT, "deposit: bulk copy wait ran out");
     if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
     return 0;

@@ -123,6 +123,10 @@ int spectral_init(Ctx *c)
     const bool dbl = c->p.precision == 64;
     FWT_CUFFT(cufftCreate(&c->plan_r2c));
     FWT_CUFFT(cufftCreate(&c->plan_c2r));
+    // the two plans run one after the other on the context's stream: one work area serves
+    // both (at 1024^3 in FP64 each would otherwise hold tens of GB of its own)
+    FWT_CUFFT(cufftSetAutoAllocation(c->plan_r2c, 0));
+    FWT_CUFFT(cufftSetAutoAllocation(c->plan_c2r, 0));
     size_t ws1 = 0, ws2 = 0;
     const long long nh = (long long)N * N * (N / 2 + 1), n3 = (long long)N * N * N;
     FWT_CUFFT(cufftMakePlanMany(c->plan_r2c, 3, n, nullptr, 1, (int)0, nullptr, 1, 0,
@@ -134,6 +138,9 @@ int spectral_init(Ctx *c)
     FWT_CUFFT(cufftSetStream(c->plan_r2c, c->stream));
     FWT_CUFFT(cufftSetStream(c->plan_c2r, c->stream));
     c->fft_ws_bytes = std::max(ws1, ws2);
+    FWT_TRY(buf_reserve(c, c->b_fftws, c->fft_ws_bytes));
+    FWT_CUFFT(cufftSetWorkArea(c->plan_r2c, c->b_fftws.p));
+    FWT_CUFFT(cufftSetWorkArea(c->plan_c2r, c->b_fftws.p));
     c->plans = true;
     return 0;
 }

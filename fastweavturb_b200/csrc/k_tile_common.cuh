@@ -183,14 +183,12 @@ __device__ __forceinline__ void tile_acc_init(long long (*acc)[kAccN], int N, in
     }
 }
 
-// Fixed point -> float, coalesced float4 stores of the tile, component min/max folded in.
+// Fixed point -> float, coalesced float4 stores of the tile.
 __device__ __forceinline__ void tile_epilogue(long long (*acc)[kAccN], int N, int x0, int y0, int z0, double scale,
-                                              float *__restrict__ wx, float *__restrict__ wy, float *__restrict__ wz,
-                                              uint32_t *__restrict__ mm)
+                                              float *__restrict__ wx, float *__restrict__ wy, float *__restrict__ wz)
 {
-    const int tid = threadIdx.x, lane = tid & 31;
+    const int tid = threadIdx.x;
     const double inv = 1.0 / scale;
-    float mn[3] = {3.4e38f, 3.4e38f, 3.4e38f}, mx[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
     const bool full = (x0 + TX <= N) && (y0 + TY <= N) && (z0 + TZ <= N);
     if (full) {
         for (int q4 = tid; q4 < TP / 4; q4 += blockDim.x) {
@@ -207,8 +205,6 @@ __device__ __forceinline__ void tile_epilogue(long long (*acc)[kAccN], int N, in
                 v4.w = (float)((double)acc[d][pa + 3] * inv);
                 float *w = d == 0 ? wx : (d == 1 ? wy : wz);
                 *reinterpret_cast<float4 *>(w + g) = v4;
-                mn[d] = fminf(mn[d], fminf(fminf(v4.x, v4.y), fminf(v4.z, v4.w)));
-                mx[d] = fmaxf(mx[d], fmaxf(fmaxf(v4.x, v4.y), fmaxf(v4.z, v4.w)));
             }
         }
     } else {
@@ -222,20 +218,7 @@ __device__ __forceinline__ void tile_epilogue(long long (*acc)[kAccN], int N, in
                 const float v1 = (float)((double)acc[d][lx + kSY * ly + kSZ * lz] * inv);
                 float *w = d == 0 ? wx : (d == 1 ? wy : wz);
                 w[g] = v1;
-                mn[d] = fminf(mn[d], v1);
-                mx[d] = fmaxf(mx[d], v1);
             }
-        }
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        for (int o2 = 16; o2 > 0; o2 >>= 1) {
-            mn[d] = fminf(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o2));
-            mx[d] = fmaxf(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o2));
-        }
-        if (lane == 0) {
-            atomicMin(mm + 2 * d, f2ord(mn[d]));
-            atomicMax(mm + 2 * d + 1, f2ord(mx[d]));
         }
     }
 }
@@ -263,14 +246,12 @@ __device__ __forceinline__ void tile_acc_init_f64(double (*acc)[kAccN], int N, i
     }
 }
 
-// FP64 tile store (coalesced double2 stores) and the exact component min/max (64-bit ordered
-// atomics, mm: 6 words).
+// FP64 tile store (coalesced double2 stores).
 __device__ __forceinline__ void tile_epilogue_f64(double (*acc)[kAccN], int N, int x0, int y0, int z0,
                                                   double *__restrict__ wx, double *__restrict__ wy,
-                                                  double *__restrict__ wz, unsigned long long *__restrict__ mm)
+                                                  double *__restrict__ wz)
 {
-    const int tid = threadIdx.x, lane = tid & 31;
-    double mn[3] = {1.7e308, 1.7e308, 1.7e308}, mx[3] = {-1.7e308, -1.7e308, -1.7e308};
+    const int tid = threadIdx.x;
     const bool full = (x0 + TX <= N) && (y0 + TY <= N) && (z0 + TZ <= N);
     if (full) {
         for (int q2 = tid; q2 < TP / 2; q2 += blockDim.x) {
@@ -285,8 +266,6 @@ __device__ __forceinline__ void tile_epilogue_f64(double (*acc)[kAccN], int N, i
                 v2.y = acc[d][pa + 1];
                 double *w = d == 0 ? wx : (d == 1 ? wy : wz);
                 *reinterpret_cast<double2 *>(w + g) = v2;
-                mn[d] = fmin(mn[d], fmin(v2.x, v2.y));
-                mx[d] = fmax(mx[d], fmax(v2.x, v2.y));
             }
         }
     } else {
@@ -300,20 +279,7 @@ __device__ __forceinline__ void tile_epilogue_f64(double (*acc)[kAccN], int N, i
                 const double v1 = acc[d][lx + kSY * ly + kSZ * lz];
                 double *w = d == 0 ? wx : (d == 1 ? wy : wz);
                 w[g] = v1;
-                mn[d] = fmin(mn[d], v1);
-                mx[d] = fmax(mx[d], v1);
             }
-        }
-    }
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        for (int o2 = 16; o2 > 0; o2 >>= 1) {
-            mn[d] = fmin(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o2));
-            mx[d] = fmax(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o2));
-        }
-        if (lane == 0) {
-            atomicMin(mm + 2 * d, d2ord(mn[d]));
-            atomicMax(mm + 2 * d + 1, d2ord(mx[d]));
         }
     }
 }
@@ -347,8 +313,7 @@ __device__ __forceinline__ int box_index(int i, int lo, int N)
     return lo + o;
 }
 
-__global__ void mm_init64_kernel(unsigned long long *mm, int n);
-int read_dep_range(Ctx *c, const void *d_mm, bool f64);
+
 
 
 // ---------------------------------------------------------------- FP64 redo of ill-conditioned pairs
@@ -410,7 +375,6 @@ __global__ void tile_scatter_kernel(const uint32_t *__restrict__ key, const uint
                                     const int64_t *__restrict__ tile_off, uint32_t *__restrict__ cursor,
                                     uint32_t *__restrict__ list);
 __global__ void u32_to_i64_kernel(const uint32_t *__restrict__ a, int64_t n, int64_t *__restrict__ b);
-__global__ void mm_init_kernel(uint32_t *mm, int n);
 
 // Scale of the int64 fixed-point tile sums for the context's lines.
 double fixed_point_scale(const Ctx *c);

@@ -129,6 +129,18 @@ int fwt_field_wh(fwt_ctx *ctx, float *host_out);
 /* Copy a normalised (after fwt_normalize) or raw field to the host as doubles,
  * column-major.  which = 0: omega, 1: u; component 0..2. */
 int fwt_copy_field(fwt_ctx *ctx, int which, int component, double *host_colmajor);
+/* The vortex-surface-field deviation of cal_deviation (subroutine.f90:1519-1546), whose call
+ * the reference keeps commented out (tube.f90:1050-1053, 1201): the mean over the grid of
+ * |omega . grad phi| / (|omega| |grad phi| + 1e-11), grad phi by sixth-order central
+ * differences on the periodic grid (wall_phiv's ghost layers, subroutine.f90:1575-1601).
+ * d_phi: a device scalar field N^3 of the context's precision (column-major), or NULL for
+ * phi = |omega| (the "VSF deviation of vorticity magnitude" of tube.f90:1201).  0 when omega
+ * is everywhere tangent to the level sets of phi. */
+int fwt_vsf_deviation(fwt_ctx *ctx, const void *d_phi, double *deviation);
+/* Total helicity, cal_helicity of (omega, u) (subroutine.f90:1550-1569, its call commented out
+ * at tube.f90:1027): sum of omega . u times the cell volume (2 pi / N)^3, of the normalised
+ * fields after fwt_normalize, of the raw fields before. */
+int fwt_helicity(fwt_ctx *ctx, double *helicity);
 /* Device address of a field held by the context: three N^3 arrays (components x, y, z, each
  * column-major, x fastest) of the context's precision (float or double), raw (unnormalised:
  * divide by u' of fwt_normalize for the normalised field).  Valid until the next call that

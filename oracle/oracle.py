@@ -488,6 +488,31 @@ def field_wh(vor, vel, n_d):
     return np.stack([wm, h])  # (2, nz, ny, nx) == Fortran (nx, ny, nz, 2)
 
 
+def vsf_deviation(vor, phi):
+    """cal_deviation (subroutine.f90:1519-1546): mean of |omega . grad phi| /
+    (|omega| |grad phi| + 1e-11), grad phi by the reference's sixth-order central differences
+    on the periodic grid (the ghost layers of wall_phiv, subroutine.f90:1575-1601, are the
+    periodic images).  Arrays are [c, z, y, x]."""
+    N = phi.shape[0]
+    dx = 2.0 * np.pi / N
+
+    def d6(axis):
+        f = lambda o: np.roll(phi, -o, axis=axis)
+        return (9.0 * f(-2) - f(-3) - 45.0 * f(-1) + 45.0 * f(1) - 9.0 * f(2) + f(3)) / 60.0 / dx
+
+    gx, gy, gz = d6(2), d6(1), d6(0)
+    graph = np.sqrt(gx ** 2 + gy ** 2 + gz ** 2)
+    vorti = np.sqrt(vor[0] ** 2 + vor[1] ** 2 + vor[2] ** 2)
+    dot = vor[0] * gx + vor[1] * gy + vor[2] * gz
+    return float(np.sum(np.abs(dot) / (vorti * graph + 1.0e-11)) / N ** 3)
+
+
+def helicity(vor, vel):
+    """cal_helicity of omega and u (subroutine.f90:1550-1569): sum omega . u dv."""
+    N = vor.shape[1]
+    return cal_helicity(vor, vel, (2.0 * np.pi / N) ** 3)
+
+
 def dx_dy_dz(phy, d):
     """dx_dy_dz_dp_dm with switch_d = d (1, 2, 3: d/dx, d/dy, d/dz; subroutine.f90:1128-1163):
     forward transform, times i k_d, backward transform, real part."""

@@ -122,3 +122,32 @@ def test_cfg1_first_tubes_of_every_level(fwt, cfg1_bounded, precision, mode, tol
     ctx.deposit()
     assert rel_l2(ctx.field(0), vor) <= tol
     ctx.close()
+
+
+@pytest.mark.parametrize("precision,mode,tol", [(32, 0, 1e-4), (64, 0, 1e-10)])
+def test_cfg0_vsf_deviation_and_helicity(fwt, orc, cfg0_case, precision, mode, tol):
+    """The diagnostics the reference keeps commented out (tube.f90:1027, 1050-1053): the VSF
+    deviation of the vorticity magnitude (cal_deviation, subroutine.f90:1519-1546) and the total
+    helicity (cal_helicity of omega and u), against the oracle's on its FP64 fields.  The
+    helicity of randomly signed tubes nearly cancels, so its error is measured against
+    sum |omega . u| dv."""
+    w, p, cl, ref = cfg0_case
+    ctx = fwt.Context(gpu_params(fwt, w, precision=precision, deposit_mode=mode))
+    ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+    ctx.run()
+    ctx.cal_helicity()
+    vor, vel = ref["vor"], ref["vel"]
+    dev = ctx.vsf_deviation()
+    dev_o = orc.vsf_deviation(vor, np.sqrt(vor[0] ** 2 + vor[1] ** 2 + vor[2] ** 2))
+    assert 0.0 < dev_o < 1.0
+    assert dev == pytest.approx(dev_o, rel=tol)
+    h = ctx.helicity()
+    h_o = orc.helicity(vor, vel)
+    scale = float(np.sum(np.abs(vor[0] * vel[0] + vor[1] * vel[1] + vor[2] * vel[2]))) * (2 * np.pi / w.N) ** 3
+    assert abs(h - h_o) <= tol * scale
+    # a caller-given scalar field: phi = |omega| passed explicitly gives the same number
+    import torch
+    wt = ctx.field_tensor(0)
+    phi = torch.sqrt((wt.double() ** 2).sum(0)).to(wt.dtype).contiguous()
+    assert ctx.vsf_deviation(phi.data_ptr()) == pytest.approx(dev, rel=1e-6)
+    ctx.close()

@@ -431,3 +431,24 @@ def test_dissipation_of_a_shear_and_a_strain(orc):
     vel = np.stack([np.sin(X) * np.cos(Y), -np.cos(X) * np.sin(Y), np.zeros_like(X)])
     assert np.allclose(orc.dissipation_field(vel), 2.0 * np.cos(X) ** 2 * np.cos(Y) ** 2, atol=1e-12)
     assert np.allclose(orc.dx_dy_dz(np.sin(2 * X), 1), 2 * np.cos(2 * X), atol=1e-12)
+
+
+def test_vsf_deviation_and_helicity_known_answers(orc):
+    """cal_deviation (subroutine.f90:1519-1546): omega along x with phi independent of x gives
+    omega . grad phi = 0, deviation ~0; omega along x with phi = sin(x + 0.3) gives |omega . grad
+    phi| = |omega| |grad phi|, deviation 1 (up to the 1e-11 guard).  The sixth-order stencil
+    differentiates sin to O(dx^6).  cal_helicity: omega = u = (1, 0, 0) gives (2 pi)^3."""
+    N = 32
+    x = np.arange(N) * 2 * np.pi / N - np.pi
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    vor = np.stack([1.0 + 0.5 * np.cos(Y) * np.sin(Z), np.zeros_like(X), np.zeros_like(X)])
+    # rounding leaves |d phi/dx| ~ 1e-16; where grad phi vanishes too (the extrema of phi) the
+    # 1e-11 guard bounds such points' ratios by ~1e-5
+    assert orc.vsf_deviation(vor, np.exp(np.cos(Y) + np.sin(2 * Z))) < 1e-6
+    vor = np.stack([np.ones_like(X), np.zeros_like(X), np.zeros_like(X)])
+    assert orc.vsf_deviation(vor, np.sin(X + 0.3)) == pytest.approx(1.0, abs=1e-8)
+    # an oblique case: omega = (1, 1, 0) / sqrt2, phi = sin(x + 0.3): |cos| / sqrt2 / |cos| = 1/sqrt2
+    vor = np.stack([np.ones_like(X), np.ones_like(X), np.zeros_like(X)]) / np.sqrt(2.0)
+    assert orc.vsf_deviation(vor, np.sin(X + 0.3)) == pytest.approx(1.0 / np.sqrt(2.0), abs=1e-8)
+    vel = np.stack([np.ones_like(X), np.zeros_like(X), np.zeros_like(X)])
+    assert orc.helicity(vel, vel) == pytest.approx((2 * np.pi) ** 3, rel=1e-14)
