@@ -57,6 +57,7 @@ EXPORTS = [
     "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
     "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_field_uw", "fwt_field_wd",
     "fwt_set_outputs", "fwt_copy_field", "fwt_field_device", "fwt_vsf_deviation", "fwt_helicity",
+    "fwt_isosurface",
     "fwt_write_outputs", "fwt_run_dir", "fwt_run",
     "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
     "fwt_set_tuning", "fwt_mlp_create", "fwt_mlp_destroy", "fwt_mlp_nparams", "fwt_mlp_get_params", "fwt_mlp_set_params",
@@ -101,6 +102,8 @@ def library(path: str | None = None):
         "fwt_field_device": [vp, ip, ctypes.POINTER(vp)],
         "fwt_vsf_deviation": [vp, vp, dp],
         "fwt_helicity": [vp, dp],
+        "fwt_isosurface": [vp, ctypes.c_float, ctypes.POINTER(ctypes.c_float), ctypes.c_int64, i64p,
+                           ctypes.POINTER(ctypes.c_float)],
         "fwt_write_outputs": [vp, ctypes.c_char_p],
         "fwt_run_dir": [ctypes.c_char_p, ctypes.POINTER(_Params)],
         "fwt_run": [vp],
@@ -357,6 +360,19 @@ class Context:
         _check(library().fwt_helicity(self._h, ctypes.byref(out)))
         return out.value
 
+    def isosurface(self, iso=0.0):
+        """Triangles (T, 3, 4): vertices (x, y, z, helicity) of the |omega| isosurface of the
+        field_wh box (output/field_wh_norm.py:56-89), and the iso value used (iso <= 0: the
+        script's 3 rms(|omega|) / sqrt 2)."""
+        n = ctypes.c_int64()
+        used = ctypes.c_float()
+        _check(library().fwt_isosurface(self._h, float(iso), None, 0, ctypes.byref(n), ctypes.byref(used)))
+        tris = np.zeros((max(n.value, 1), 3, 4), dtype=np.float32)
+        if n.value:
+            _check(library().fwt_isosurface(self._h, float(used.value), _ptr(tris, ctypes.c_float), n.value,
+                                            ctypes.byref(n), ctypes.byref(used)))
+        return tris[:n.value], float(used.value)
+
     def field_tensor(self, which):
         """Zero-copy torch view (3, N, N, N), index [c, z, y, x], of the raw (unnormalised)
         field on the device (which = 0: omega, 1: u), in the context's precision.  Valid until
@@ -409,3 +425,22 @@ def fbb_signs(seed, ntubes):
     out = np.zeros(ntubes, dtype=np.int32)
     _check(library().fwt_fbb_signs(ctypes.c_uint64(seed), ntubes, _ptr(out, ctypes.c_int)))
     return out
+
+
+def write_ply(path, tris):
+    """Write isosurface triangles (T, 3, 4): x, y, z, helicity per vertex (Context.isosurface)
+    as a binary little-endian PLY mesh: 3T vertices with a float `helicity` property and T
+    triangular faces.  The headless stand-in for the rendering script's screenshot
+    (output/field_wh_norm.py:114-118): any mesh viewer colours it by the helicity."""
+    tris = np.ascontiguousarray(tris, dtype="<f4").reshape(-1, 3, 4)
+    T = tris.shape[0]
+    head = ("ply\nformat binary_little_endian 1.0\ncomment |omega| isosurface coloured by the helicity omega.u\n"
+            f"element vertex {3 * T}\nproperty float x\nproperty float y\nproperty float z\n"
+            f"property float helicity\nelement face {T}\nproperty list uchar int vertex_indices\nend_header\n")
+    faces = np.zeros(T, dtype=[("n", "u1"), ("v", "<i4", (3,))])
+    faces["n"] = 3
+    faces["v"] = np.arange(3 * T, dtype="<i4").reshape(T, 3)
+    with open(path, "wb") as f:
+        f.write(head.encode("ascii"))
+        f.write(tris.tobytes())
+        f.write(faces.tobytes())

@@ -448,6 +448,14 @@ int fwt_helicity(fwt_ctx *h, double *helicity)
     return diag_helicity(c, helicity);
 }
 
+int fwt_isosurface(fwt_ctx *h, float iso, float *tris, int64_t max_tris, int64_t *ntris, float *iso_used)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !ntris) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    return iso_extract(c, iso, tris, max_tris, ntris, iso_used);
+}
+
 int fwt_field_device(fwt_ctx *h, int which, void **ptr)
 {
     Ctx *c = (Ctx *)h;

@@ -175,6 +175,7 @@ int stats_copy_field(Ctx *c, int which, int comp, double *host);
 // diagnostics (k_diag.cu)
 int diag_vsf_deviation(Ctx *c, const void *d_phi, double *deviation);
 int diag_helicity(Ctx *c, double *helicity);
+int iso_extract(Ctx *c, float iso, float *host_tris, int64_t max_tris, int64_t *ntris, float *iso_used);
 
 // host I/O (fwt_io.cpp)
 int io_read_centerlines(const char *path, std::vector<int64_t> &npoint, std::vector<double> &xyz);

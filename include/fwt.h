@@ -141,6 +141,15 @@ int fwt_vsf_deviation(fwt_ctx *ctx, const void *d_phi, double *deviation);
  * at tube.f90:1027): sum of omega . u times the cell volume (2 pi / N)^3, of the normalised
  * fields after fwt_normalize, of the raw fields before. */
 int fwt_helicity(fwt_ctx *ctx, double *helicity);
+/* Isosurface of |omega| on the field_wh data box, coloured by the helicity omega . u: the
+ * compute part of the reference's rendering script (output/field_wh_norm.py:56-89), whose
+ * rendering needs a graphics stack and is not reproduced.  The box is n_d^3 points of the
+ * normalised fields (after fwt_normalize) at the script's coordinates x_i = 2 pi i / (n_d - 1).
+ * iso <= 0 takes the script's iso value 3 rms(|omega|) / sqrt 2 (returned in *iso_used).
+ * Marching tetrahedra: tris receives ntris triangles of 3 vertices (x, y, z, helicity), 12
+ * floats per triangle, wound with the normal pointing to decreasing |omega|, in a deterministic
+ * order.  tris = NULL only counts; a count above max_tris is FWT_E_RANGE. */
+int fwt_isosurface(fwt_ctx *ctx, float iso, float *tris, int64_t max_tris, int64_t *ntris, float *iso_used);
 /* Device address of a field held by the context: three N^3 arrays (components x, y, z, each
  * column-major, x fastest) of the context's precision (float or double), raw (unnormalised:
  * divide by u' of fwt_normalize for the normalised field).  Valid until the next call that

@@ -631,3 +631,93 @@ def philox_raw(ctr, key):
     u32p = ctypes.POINTER(ctypes.c_uint32)
     lib().orc_philox_raw(c.ctypes.data_as(u32p), k.ctypes.data_as(u32p), out.ctypes.data_as(u32p))
     return out
+
+
+# ----------------------------------------------------------------------------- isosurface
+
+_TET_AXES = [(1, 2), (1, 4), (2, 1), (2, 4), (4, 1), (4, 2)]
+
+
+def isosurface_iso(box_v):
+    """output/field_wh_norm.py:71-73: iso_w = sqrt(mean(|omega|^2)) * 3 / sqrt(2)."""
+    v = box_v.astype(np.float64)
+    return np.float32(np.sqrt(np.sum(v * v) / v.size) * 3.0 / np.sqrt(2.0))
+
+
+def isosurface(box_v, box_h, iso):
+    """Marching tetrahedra on the field_wh box (arrays [k, j, i], float32), the restatement of
+    the library's extraction: six tetrahedra per cube around the 0-7 diagonal, a vertex inside
+    when its value exceeds iso, crossings interpolated from the edge's lower corner, triangles
+    wound from inside to outside, in cube order (x fastest), then tetrahedron, then triangle.
+    Every float32 operation is rounded on its own, as on the device.  Returns (T, 3, 4)
+    vertices (x, y, z, helicity) at x_i = 2 pi i / (n - 1)."""
+    f32 = np.float32
+    n = box_v.shape[0]
+    m1 = n - 1
+    iso = f32(iso)
+    step = f32(2.0 * np.pi / (n - 1))
+    k, j, i = np.meshgrid(np.arange(m1), np.arange(m1), np.arange(m1), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+    q = i + m1 * (j + m1 * k)
+    corner = lambda c: (k + ((c >> 2) & 1), j + ((c >> 1) & 1), i + (c & 1))
+    val = [box_v[corner(c)].astype(f32) for c in range(8)]
+    hel = [box_h[corner(c)].astype(f32) for c in range(8)]
+    pos = [np.stack([(i + (c & 1)).astype(f32), (j + ((c >> 1) & 1)).astype(f32),
+                     (k + ((c >> 2) & 1)).astype(f32)], axis=1) for c in range(8)]
+    inside = [val[c] > iso for c in range(8)]
+
+    def crossing(sel, a, b):
+        if a > b:
+            a, b = b, a
+        va, vb = val[a][sel], val[b][sel]
+        t = ((iso - va) / (vb - va)).astype(f32)
+        xa, xb = pos[a][sel], pos[b][sel]
+        p = ((xa + t[:, None] * (xb - xa)) * step).astype(f32)
+        ha, hb = hel[a][sel], hel[b][sel]
+        h = (ha + t * (hb - ha)).astype(f32)
+        return np.concatenate([p, h[:, None]], axis=1)
+
+    def wind(p, r, s, d):
+        e1, e2 = r[:, :3] - p[:, :3], s[:, :3] - p[:, :3]
+        nx = e1[:, 1] * e2[:, 2] - e1[:, 2] * e2[:, 1]
+        ny = e1[:, 2] * e2[:, 0] - e1[:, 0] * e2[:, 2]
+        nz = e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0]
+        dot = (nx * d[0] + ny * d[1]) + nz * d[2]
+        flip = (dot < f32(0.0))[:, None]
+        return np.stack([p, np.where(flip, s, r), np.where(flip, r, s)], axis=1)
+
+    tris, keys = [], []
+    for tt, (a, b) in enumerate(_TET_AXES):
+        cs = [0, a, a | b, 7]
+        for mask in range(1, 15):
+            ins = [c for s, c in enumerate(cs) if (mask >> s) & 1]
+            outs = [c for s, c in enumerate(cs) if not (mask >> s) & 1]
+            sel = np.ones(q.size, dtype=bool)
+            for s, c in enumerate(cs):
+                sel &= inside[c] == bool((mask >> s) & 1)
+            if not sel.any():
+                continue
+            d = [f32(f32(sum((c >> ax) & 1 for c in outs)) / f32(len(outs)))
+                 - f32(f32(sum((c >> ax) & 1 for c in ins)) / f32(len(ins))) for ax in range(3)]
+            d = [f32(x) for x in d]
+            if len(ins) == 1 or len(outs) == 1:
+                lone = ins[0] if len(ins) == 1 else outs[0]
+                oth = outs if len(ins) == 1 else ins
+                p = [crossing(sel, lone, o) for o in oth]
+                tris.append(wind(p[0], p[1], p[2], d))
+                keys.append(np.stack([q[sel], np.full(sel.sum(), tt), np.zeros(sel.sum(), dtype=np.int64)], 1))
+            else:
+                p0 = crossing(sel, ins[0], outs[0])
+                p1 = crossing(sel, ins[0], outs[1])
+                p2 = crossing(sel, ins[1], outs[1])
+                p3 = crossing(sel, ins[1], outs[0])
+                tris.append(wind(p0, p1, p2, d))
+                keys.append(np.stack([q[sel], np.full(sel.sum(), tt), np.zeros(sel.sum(), dtype=np.int64)], 1))
+                tris.append(wind(p0, p2, p3, d))
+                keys.append(np.stack([q[sel], np.full(sel.sum(), tt), np.ones(sel.sum(), dtype=np.int64)], 1))
+    if not tris:
+        return np.zeros((0, 3, 4), dtype=f32)
+    tris = np.concatenate(tris)
+    keys = np.concatenate(keys)
+    order = np.lexsort((keys[:, 2], keys[:, 1], keys[:, 0]))
+    return tris[order]

@@ -151,3 +151,23 @@ def test_cfg0_vsf_deviation_and_helicity(fwt, orc, cfg0_case, precision, mode, t
     phi = torch.sqrt((wt.double() ** 2).sum(0)).to(wt.dtype).contiguous()
     assert ctx.vsf_deviation(phi.data_ptr()) == pytest.approx(dev, rel=1e-6)
     ctx.close()
+
+
+def test_isosurface_matches_the_restatement_bit_for_bit(fwt, orc, cfg0_case, tmp_path):
+    """The |omega| isosurface of the field_wh box (output/field_wh_norm.py:56-89) at the script's
+    iso value: the device's triangles equal the oracle's marching tetrahedra on the same box bit
+    for bit (same order, same float32 rounding), and the PLY file holds them."""
+    w, p, cl, ref = cfg0_case
+    ctx = fwt.Context(gpu_params(fwt, w, precision=32, deposit_mode=0))
+    ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+    ctx.run()
+    box = ctx.output_v()                       # (2, n, n, n): |omega| and omega.u, [z, y, x]
+    tris, iso = ctx.isosurface()
+    assert iso == pytest.approx(float(orc.isosurface_iso(box[0])), rel=1e-6)
+    assert len(tris) > 1000
+    tr_o = orc.isosurface(box[0], box[1], np.float32(iso))
+    assert tris.shape == tr_o.shape
+    assert np.array_equal(tris, tr_o)
+    fwt.api.write_ply(tmp_path / "iso.ply", tris)
+    assert (tmp_path / "iso.ply").stat().st_size > 48 * len(tris)
+    ctx.close()

@@ -84,3 +84,21 @@ def test_benchmark_workloads_follow_their_configurations():
             assert L.H == 0.7 and np.isclose(L.Gamma, (L.sigma / s0) ** (4.0 / 3.0))
     assert configs.cfg1().ntubes == 5460 and configs.cfg1().nnodes == 38347776
     assert configs.cfg2().ntubes == 43690
+
+
+def test_write_ply_layout(tmp_path):
+    """The PLY writer of isosurface triangles: header counts, vertex records of 4 floats and
+    faces of (3, i, i+1, i+2)."""
+    from fastweavturb_b200.api import write_ply
+    tris = np.arange(2 * 3 * 4, dtype=np.float32).reshape(2, 3, 4)
+    p = tmp_path / "m.ply"
+    write_ply(p, tris)
+    raw = p.read_bytes()
+    end = raw.index(b"end_header\n") + len(b"end_header\n")
+    head = raw[:end].decode()
+    assert "element vertex 6" in head and "element face 2" in head and "property float helicity" in head
+    body = raw[end:]
+    v = np.frombuffer(body[:6 * 16], dtype="<f4").reshape(6, 4)
+    assert np.array_equal(v, tris.reshape(6, 4))
+    f = np.frombuffer(body[6 * 16:], dtype=[("n", "u1"), ("v", "<i4", (3,))])
+    assert list(f["n"]) == [3, 3] and f["v"].tolist() == [[0, 1, 2], [3, 4, 5]]

@@ -452,3 +452,43 @@ def test_vsf_deviation_and_helicity_known_answers(orc):
     assert orc.vsf_deviation(vor, np.sin(X + 0.3)) == pytest.approx(1.0 / np.sqrt(2.0), abs=1e-8)
     vel = np.stack([np.ones_like(X), np.zeros_like(X), np.zeros_like(X)])
     assert orc.helicity(vel, vel) == pytest.approx((2 * np.pi) ** 3, rel=1e-14)
+
+
+def test_isosurface_of_a_sphere_is_closed_and_outward(orc):
+    """Marching tetrahedra (the contour step of output/field_wh_norm.py:81) on a radial field:
+    every vertex near the iso-radius, every edge shared by exactly two triangles (a closed
+    surface), every normal pointing outward (to decreasing values), area close to 4 pi R^2, and
+    the helicity scalar interpolated linearly (h = x gives the vertex x)."""
+    n = 33
+    x = np.linspace(0.0, 2 * np.pi, n)
+    Z, Y, X = np.meshgrid(x, x, x, indexing="ij")
+    c = np.pi
+    r2 = (X - c) ** 2 + (Y - c) ** 2 + (Z - c) ** 2
+    v = np.exp(-r2).astype(np.float32)
+    R = 1.7
+    iso = np.float32(np.exp(-R * R))
+    tris = orc.isosurface(v, X.astype(np.float32), iso)
+    assert tris.shape[1:] == (3, 4) and len(tris) > 500
+    p = tris[:, :, :3].astype(np.float64)
+    rad = np.linalg.norm(p - c, axis=2)
+    assert np.abs(rad - R).max() < 0.05
+    np.testing.assert_allclose(tris[:, :, 3], tris[:, :, 0], rtol=1e-5, atol=1e-5)
+    e1, e2 = p[:, 1] - p[:, 0], p[:, 2] - p[:, 0]
+    nrm = np.cross(e1, e2)
+    area = 0.5 * np.linalg.norm(nrm, axis=1)
+    cen = p.mean(axis=1) - c
+    keep = area > 1e-9
+    assert np.all(np.einsum("ij,ij->i", nrm[keep], cen[keep]) > 0)
+    assert area.sum() == pytest.approx(4 * np.pi * R * R, rel=0.02)
+    # closed: each undirected edge (by exact vertex coordinates) appears in two triangles
+    from collections import Counter
+    key = lambda a: tuple(np.round(a, 6))
+    edges = Counter()
+    for t in p:
+        for s in range(3):
+            a, b = key(t[s]), key(t[(s + 1) % 3])
+            if a != b:
+                edges[tuple(sorted((a, b)))] += 1
+    assert set(edges.values()) == {2}
+    assert orc.isosurface_iso(v) == pytest.approx(np.sqrt(np.mean(v.astype(np.float64) ** 2)) * 3 / np.sqrt(2),
+                                                  rel=1e-6)
