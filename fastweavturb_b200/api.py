@@ -53,7 +53,7 @@ class _Params(ctypes.Structure):
 
 
 EXPORTS = [
-    "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_set_centerlines",
+    "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_check_inputs", "fwt_set_centerlines",
     "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
     "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_field_uw", "fwt_field_wd",
     "fwt_set_outputs", "fwt_copy_field", "fwt_field_device", "fwt_vsf_deviation", "fwt_helicity",
@@ -82,6 +82,7 @@ def library(path: str | None = None):
         "fwt_create": [ctypes.POINTER(_Params), ctypes.POINTER(vp)],
         "fwt_destroy": [vp],
         "fwt_load_inputs": [vp, ctypes.c_char_p, ctypes.c_char_p],
+        "fwt_check_inputs": [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_Params), ctypes.POINTER(ip), i64p],
         "fwt_set_centerlines": [vp, ip, i64p, dp, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
         "fwt_set_centerlines_device": [vp, ip, i64p, vp, vp, vp, dp, dp, ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int)],
@@ -425,6 +426,19 @@ def fbb_signs(seed, ntubes):
     out = np.zeros(ntubes, dtype=np.int32)
     _check(library().fwt_fbb_signs(ctypes.c_uint64(seed), ntubes, _ptr(out, ctypes.c_int)))
     return out
+
+
+def check_inputs(rundir):
+    """Read and validate rundir/centerline_input.dat and rundir/parameters_input.dat without a
+    GPU (fwt_check_inputs); returns (params dict, nline, nodes) or raises FwtError."""
+    p = _Params()
+    _check(library().fwt_default_params(ctypes.byref(p)))
+    nl = ctypes.c_int()
+    nodes = ctypes.c_int64()
+    _check(library().fwt_check_inputs(os.path.join(str(rundir), "centerline_input.dat").encode(),
+                                      os.path.join(str(rundir), "parameters_input.dat").encode(), ctypes.byref(p),
+                                      ctypes.byref(nl), ctypes.byref(nodes)))
+    return {f: getattr(p, f) for f, _ in _Params._fields_}, nl.value, nodes.value
 
 
 def write_ply(path, tris):

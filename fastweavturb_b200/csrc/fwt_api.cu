@@ -98,7 +98,6 @@ void kt_reset(Ctx *c)
     for (int i = 0; i < 8; ++i) {
         c->ktime[i] = 0;
         c->kcount[i] = 0;
-        c->kbytes[i] = 0;
     }
 }
 
@@ -325,6 +324,29 @@ int fwt_set_centerlines_device(fwt_ctx *h, int nline, const int64_t *npoint, con
     c->d_x = d_x;
     c->d_y = d_y;
     c->d_z = d_z;
+    return 0;
+}
+
+int fwt_check_inputs(const char *cpath, const char *ppath, fwt_params *p, int *nline, int64_t *nodes)
+{
+    if (!cpath || !ppath || !p) return fail(FWT_E_ARG, "null argument");
+    std::vector<int64_t> np;
+    std::vector<double> xyz, sig, gam;
+    std::vector<int> nT, filt;
+    FWT_TRY(io_read_centerlines(cpath, np, xyz));
+    FWT_TRY(io_read_params(ppath, (int)np.size(), *p, sig, gam, nT, filt));
+    FWT_TRY(validate(*p));
+    if (p->line_s < 1 || p->line_e > (int)np.size() || p->line_s > p->line_e)
+        return fail(FWT_E_ARG, "line_s..line_e outside 1..nline");
+    for (size_t i = 0; i < np.size(); ++i)
+        if (!(sig[i] > 0) || !std::isfinite(gam[i]) || nT[i] < 0)
+            return fail(FWT_E_ARG, "line " + std::to_string(i + 1) + ": sigma must be positive, Gamma finite, n_T >= 0");
+    if (nline) *nline = (int)np.size();
+    if (nodes) {
+        int64_t t = 0;
+        for (auto v : np) t += v;
+        *nodes = t;
+    }
     return 0;
 }
 

@@ -138,7 +138,6 @@ struct Ctx {
     size_t ev_used = 0;
     double ktime[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t kcount[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int64_t kbytes[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // algorithmic bytes moved by the category
     double t_setup_acc = 0;
 };
 

@@ -109,8 +109,16 @@ int io_read_centerlines(const char *path, std::vector<int64_t> &npoint, std::vec
         total += npoint[i];
     }
     xyz.resize((size_t)total * 3);
+    std::string tok;
     for (int64_t i = 0; i < total * 3; ++i) {
-        if (!(f >> xyz[i])) return fail(FWT_E_IO, "centerline file: truncated node list");
+        if (!(f >> tok)) return fail(FWT_E_IO, "centerline file: truncated node list");
+        // strtod also reads Fortran's NaN / Infinity spellings, which are then refused as such
+        for (char &ch : tok)
+            if (ch == 'D' || ch == 'd') ch = 'E';
+        char *end = nullptr;
+        xyz[i] = std::strtod(tok.c_str(), &end);
+        if (end == tok.c_str() || *end != 0)
+            return fail(FWT_E_IO, "centerline file: non-numeric coordinate '" + tok + "'");
         if (!std::isfinite(xyz[i])) return fail(FWT_E_IO, "centerline file: non-finite coordinate");
     }
     return 0;

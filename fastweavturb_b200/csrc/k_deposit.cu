@@ -101,7 +101,6 @@ int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc)
     const int64_t want = (B.nsub * 32 + 255) / 256;
     const unsigned blocks = (unsigned)std::min<int64_t>(want, (int64_t)sms * 64);
     const int km = kt_begin(c, KT_DEPOSIT);
-    c->kbytes[KT_DEPOSIT] += B.nsub * (int64_t)sizeof(SubSeg);
     if (c->p.precision == 64) {
         double *w = (double *)c->b_w.p;
         deposit_walk_kernel<double, true><<<blocks, 256, 0, c->stream>>>(

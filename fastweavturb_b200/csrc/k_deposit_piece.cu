@@ -943,9 +943,6 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     }
 #undef FWT_PIECE_LAUNCH
     kt_end(c, km);
-    // algorithmic bytes: omega written once (read too when accumulating), one list entry and
-    // one record per (tile, piece) pair
-    c->kbytes[KT_DEPOSIT] += (int64_t)(3 * n3 * rb * (accumulate ? 2 : 1)) + npairs * (int64_t)(4 + sizeof(PieceRec));
     c->launches += 2;
     c->w_written = true;
     FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));

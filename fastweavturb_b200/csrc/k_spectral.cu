@@ -181,8 +181,6 @@ static int launch_bs(Ctx *c, int mode, double kc2, double *d_shw, double *d_shu,
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((rows + 7) / 8, (int64_t)sms * 8));
     const size_t shb = sizeof(double) * 2 * (N / 2 + 1);
     const int km = kt_begin(c, KT_SPECTRAL);
-    // algorithmic bytes: the three half-spectrum components read and written once
-    c->kbytes[KT_SPECTRAL] += (int64_t)(2 * 3 * nh * 2 * real_bytes(c));
     if (c->p.precision == 64) {
         cufftDoubleComplex *s = (cufftDoubleComplex *)c->b_spec.p;
         biot_savart_kernel<double><<<blocks, 256, shb, c->stream>>>(s, s + nh, s + 2 * nh, N, mode, kc2, d_shw, d_shu,

@@ -70,6 +70,14 @@ int fwt_destroy(fwt_ctx *ctx);
 /* Reads both input files; the scalar block of params_path overrides N..dzeta_sup of the
  * context (tube.f90:168-223, 341-379).  Writes nothing. */
 int fwt_load_inputs(fwt_ctx *ctx, const char *centerline_path, const char *params_path);
+/* Read and validate the two input files without a context or a GPU (the reference's input
+ * reading, tube.f90:168-223, 341-379, and the checks fwt_load_inputs and fwt_create apply):
+ * p receives the file's scalars over the defaults it holds, nline and nodes the line and node
+ * counts.  A truncated or non-numeric file, a non-finite coordinate, a line with fewer than two
+ * nodes, a missing parameter row, N_downsample not dividing N or a bad line range is an
+ * FWT_E_IO / FWT_E_ARG error naming the fault. */
+int fwt_check_inputs(const char *centerline_path, const char *params_path, fwt_params *p, int *nline,
+                     int64_t *nodes);
 
 /* Array form of the same inputs (tube.f90:353-379 after the broadcasts): nline lines,
  * npoint[l] nodes each, xyz row-major (npointall x 3) host doubles in [-pi,pi), and the
