@@ -342,6 +342,11 @@ class Context:
         """Tubes up to this truncation radius (grid spacings) take the chord-piece kernel."""
         _check(library().fwt_set_tuning(self._h, 1, float(cells)))
 
+    def set_raster_radius_limit(self, cells):
+        """Piece tubes up to this truncation radius (grid spacings) are rasterised once per piece
+        (0: never; negative: the default)."""
+        _check(library().fwt_set_tuning(self._h, 2, float(cells)))
+
     def counters(self):
         v = np.zeros(7, dtype=np.int64)
         library().fwt_counters(self._h, _ptr(v, ctypes.c_int64), 7)

@@ -635,6 +635,10 @@ int fwt_set_tuning(fwt_ctx *h, int key, double value)
 {
     Ctx *c = (Ctx *)h;
     if (!c) return fail(FWT_E_ARG, "null context");
+    if (key == FWT_TUNE_RASTER_RT_CELLS) {
+        c->raster_rt_cells = value;
+        return 0;
+    }
     if (key == FWT_TUNE_PIECE_RT_CELLS) {
         c->piece_rt_cells = value;
         return 0;

@@ -75,6 +75,7 @@ struct Ctx {
     fwt_params p{};
     int dev = 0;
     double piece_rt_cells = -1.0;   // tuning: piece kernel radius limit in grid spacings (< 0: default)
+    double raster_rt_cells = -1.0;  // tuning: radius limit of rasterised pieces in grid spacings (< 0: default)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
 
@@ -102,7 +103,7 @@ struct Ctx {
     size_t fft_ws_bytes = 0;
 
     // scratch (centerline set-up, deposition, statistics)
-    DevBuf scratch[25];
+    DevBuf scratch[28];
 
     // state
     bool have_w = false, have_u = false, normalised = false;

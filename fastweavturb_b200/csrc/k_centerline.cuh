@@ -60,6 +60,9 @@ struct CenterlineBatch {
     SegRec *rec = nullptr;       // nsub FP32 records (tile-owned kernel)
     int64_t npieces = 0;         // chord pieces (piece kernel)
     PieceRec *piece = nullptr;   // npieces FP32 piece records
+    bool raster = false;                 // pieces rasterised once (thin tubes), see piece_raster
+    const int64_t *ras_off = nullptr;    // piece -> first rasterised point (npieces + 1)
+    const uint32_t *ras_pts = nullptr;   // chord | x << 3 | y << 12 | z << 21 per accepted point
     const int *rec_map = nullptr;        // record (sub-segment or piece) -> section slot
     const int64_t *rec_first = nullptr;  // section slot -> its first record
     std::vector<int64_t> line_ntf_sum;  // 2 x nl: sum(ntf), max(ntf) per line

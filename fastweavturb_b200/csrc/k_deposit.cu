@@ -161,6 +161,13 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
     auto thin = [&](int l) {
         return tile_path && c->p.Rtube_ratio * c->p.sigma_ratio * c->sigma[l] <= rt_cells * dxg;
     };
+    // radius limit of rasterised pieces: fwt_set_tuning, else FWT_RASTER_RT_CELLS, else the default
+    const char *renv = std::getenv("FWT_RASTER_RT_CELLS");
+    const double ras_cells =
+        c->raster_rt_cells >= 0.0 ? c->raster_rt_cells : (renv ? std::atof(renv) : kRasterMaxRtCells);
+    auto rasterised = [&](int l) {
+        return thin(l) && c->p.Rtube_ratio * c->p.sigma_ratio * c->sigma[l] <= ras_cells * dxg;
+    };
     int la = line_s - 1;
     while (la < line_e) {
         // batch: consecutive lines up to the node cap, ending after a filtered line and where
@@ -172,13 +179,14 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
             ++lb;
             if (c->if_filter[lb - 1]) break;
             if (lb < line_e && nodes + c->npoint[lb] > cap) break;
-            if (lb < line_e && thin(lb) != thin(la)) break;
+            if (lb < line_e && (thin(lb) != thin(la) || rasterised(lb) != rasterised(la))) break;
         }
         const BatchRecords mode =
             !tile_path ? BatchRecords::Walk : (thin(la) ? BatchRecords::Pieces : BatchRecords::SubSeg);
         if (std::getenv("FWT_SYNC_CHECK"))
             std::fprintf(stderr, "libfwt: batch lines %d..%d records %d\n", la + 1, lb, (int)mode);
         CenterlineBatch B;
+        B.raster = mode == BatchRecords::Pieces && rasterised(la);
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);

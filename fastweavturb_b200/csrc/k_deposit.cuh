@@ -664,5 +664,9 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out);
 // through the piece kernel; thicker tubes through the sub-segment kernel, whose analytic
 // row intervals skip most of a large box.
 constexpr double kPieceMaxRtCells = 8.0;
+// Piece lines whose truncation radius is at most this many grid spacings have their pieces
+// rasterised once (piece_raster) instead of searched in every tile: a chord then accepts only a
+// few points, and the per-tile search dominated their cost.
+constexpr double kRasterMaxRtCells = 2.5;
 
 }  // namespace fwt

@@ -442,6 +442,99 @@ __device__ __forceinline__ bool piece_accepts_wide(const PieceRec &R, int j, int
     return fmaf(-t0, t0, e2) < R2 + 1e-5f * (e2 + R2) + e * e;
 }
 
+// ------------------------------------------------------------------------------ raster
+// The thinnest tubes (truncation radius of a few grid spacings) accept only two or three points
+// per chord, and a chord's box meets two to four tiles: searching each (tile, piece) pair's rows
+// repeats the per-chord set-up in every tile for a handful of points.  Their pieces are
+// therefore rasterised once, in a pass over pieces: one thread per piece walks, for each chord,
+// the columns of the chord's box along the axis best aligned with the chord, bounds each column
+// by the chord's two planes (0.05-point margin) and applies the deposition kernel's acceptance
+// test (piece_accepts; the widened test in the FP64 path) to the points in between.  A first
+// pass counts the points of every piece, a scan gives each piece its offset, and a second pass
+// writes them: chord | x << 3 | y << 12 | z << 21, offsets from the piece's box origin.  The
+// deposition kernel then only evaluates the listed points that fall in its tile.  err bit 16:
+// a chord box wider than 511 points (the 9-bit offsets).
+constexpr int kRasterMaxOff = 511;
+
+template <bool Wide, bool Write>
+__global__ void __launch_bounds__(128) piece_raster_kernel(const PieceRec *__restrict__ rec, int64_t npieces,
+                                                           int64_t *__restrict__ off, uint32_t *__restrict__ pts,
+                                                           int *__restrict__ err)
+{
+    const int64_t pc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pc >= npieces) return;
+    const PieceRec &R = rec[pc];
+    const int64_t o = Write ? off[pc] : 0;
+    // the write pass stays inside the slots the counting pass reserved for this piece
+    const int64_t cap = Write ? off[pc + 1] - o : 0;
+    int64_t n = 0;
+    const int nch = R.nch;
+    const float dx = R.dx;
+    for (int j = 0; j < nch; ++j) {
+        const float4 pj = R.pl[j], pk = R.pl[j + 1];
+        const uint32_t blo = __float_as_uint(R.chq[j].z), bhi = __float_as_uint(R.chq[j].w);
+        int lo[3], hi[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = unpack3(blo, d);
+            hi[d] = unpack3(bhi, d);
+        }
+        if (hi[0] > kRasterMaxOff || hi[1] > kRasterMaxOff || hi[2] > kRasterMaxOff) {
+            atomicOr(err, 16);
+            continue;
+        }
+        const float ax = fabsf(pj.x), ay = fabsf(pj.y), az = fabsf(pj.z);
+        const int a = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+        const int b = a == 2 ? 0 : a + 1, c = a == 0 ? 2 : a - 1;
+        const float ja = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
+        const float ka = a == 0 ? pk.x : (a == 1 ? pk.y : pk.z);
+        const float sja = 1.0f / (dx * ja);
+        const float ska = fabsf(ka) > 0.05f ? 1.0f / (dx * ka) : 0.0f;
+        const int alo = a == 0 ? lo[0] : (a == 1 ? lo[1] : lo[2]);
+        const int ahi = a == 0 ? hi[0] : (a == 1 ? hi[1] : hi[2]);
+        const int clo = c == 0 ? lo[0] : (c == 1 ? lo[1] : lo[2]), chi = c == 0 ? hi[0] : (c == 1 ? hi[1] : hi[2]);
+        const int blo_ = b == 0 ? lo[0] : (b == 1 ? lo[1] : lo[2]), bhi_ = b == 0 ? hi[0] : (b == 1 ? hi[1] : hi[2]);
+        for (int ic = clo; ic <= chi; ++ic) {
+            for (int ib = blo_; ib <= bhi_; ++ib) {
+                // the column's point at a-offset 0, in the piece frame
+                const int r0x = a == 0 ? 0 : (b == 0 ? ib : ic);
+                const int r0y = a == 1 ? 0 : (b == 1 ? ib : ic);
+                const int r0z = a == 2 ? 0 : (b == 2 ? ib : ic);
+                const float dxv = fmaf((float)r0x, dx, R.off[0]);
+                const float dyv = fmaf((float)r0y, dx, R.off[1]);
+                const float dzv = fmaf((float)r0z, dx, R.off[2]);
+                const float T0 = fmaf(dzv, pj.z, fmaf(dyv, pj.y, fmaf(dxv, pj.x, -pj.w)));
+                // t_j(ra) = T0 + ra dx n_j[a] >= 0
+                float flo = (float)alo - 0.05f, fhi = (float)ahi + 0.05f;
+                const float r0 = -T0 * sja;
+                if (ja > 0.0f) flo = fmaxf(flo, r0 - 0.05f);
+                else fhi = fminf(fhi, r0 + 0.05f);
+                if (ska != 0.0f) {   // t_{j+1}(ra) = T1 + ra dx n_{j+1}[a] < 0
+                    const float T1 = fmaf(dzv, pk.z, fmaf(dyv, pk.y, fmaf(dxv, pk.x, -pk.w)));
+                    const float r1 = -T1 * ska;
+                    if (ka > 0.0f) fhi = fminf(fhi, r1 + 0.05f);
+                    else flo = fmaxf(flo, r1 - 0.05f);
+                }
+                const int ilo = max(alo, (int)ceilf(flo)), ihi = min(ahi, (int)floorf(fhi));
+                for (int ra = ilo; ra <= ihi; ++ra) {
+                    const int rx = a == 0 ? ra : r0x, ry = a == 1 ? ra : r0y, rz = a == 2 ? ra : r0z;
+                    const bool ok = Wide ? piece_accepts_wide(R, j, rx, ry, rz) : piece_accepts(R, j, rx, ry, rz);
+                    if (!ok) continue;
+                    if (Write) {
+                        if (n >= cap) {
+                            atomicOr(err, 32);
+                            continue;
+                        }
+                        pts[o + n] = (uint32_t)j | ((uint32_t)rx << 3) | ((uint32_t)ry << 12) | ((uint32_t)rz << 21);
+                    }
+                    ++n;
+                }
+            }
+        }
+    }
+    if (!Write) off[pc] = n;
+}
+
 // Evaluate the first `cnt` queued (point, chord) pairs, one per lane, into the tile cells;
 // pairs whose curved-branch amplification exceeds kRedoCond go to the redo queue instead.
 template <bool General, bool F64>
@@ -549,11 +642,12 @@ __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[
 // reference's tests (tube.f90:793-818: t_j >= 0, t_{j+1} < 0, distance to chord line j below
 // Rtube) with the plane tests in the piece frame and, within the rounding band of a plane, in
 // that sample's own frame.  Accepted pairs are queued and evaluated 32 at a time.
-template <bool General, bool Accumulate, bool F64>
+template <bool General, bool Accumulate, bool F64, bool Raster>
 __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel(
     const PieceRec *__restrict__ rec, int N, int ntx, int nty, const int64_t *__restrict__ tile_off,
     const uint32_t *__restrict__ list, double scale, void *__restrict__ wx, void *__restrict__ wy,
-    void *__restrict__ wz, int *__restrict__ err, const RedoCtx redo)
+    void *__restrict__ wz, int *__restrict__ err, const RedoCtx redo, const int64_t *__restrict__ ras_off,
+    const uint32_t *__restrict__ ras_pts)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     long long(*acc)[kAccN] = reinterpret_cast<long long(*)[kAccN]>(dsm);
@@ -605,203 +699,247 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
             S.box[lane] = B;
         }
         __syncwarp();
-        // lane = (piece k, chord j): chord j's box clipped to the tile and its rows
-        int nrows = 0;
-        {
-            const int k = lane >> 3, j = lane & 7;
-            if (k < nc && j < S.rec[k].nch && S.box[k].vol > 0) {
-                const PieceRec &R = S.rec[k];
-                const PBox &B = S.box[k];
-                const uint32_t blo = __float_as_uint(R.chq[j].z), bhi = __float_as_uint(R.chq[j].w);
-                ChordRows &C = S.cr;
-                bool nonempty = true;
-                int co[3], cnn[3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    const int tlo = B.lo[d] + B.dl[d], thi = tlo + B.n[d] - 1;   // the tile part of the piece box
-                    const int lo = max(tlo, unpack3(blo, d)), hi = min(thi, unpack3(bhi, d));
-                    co[d] = lo;
-                    cnn[d] = max(0, hi - lo + 1);
-                    C.o[d][lane] = (uint16_t)lo;
-                    C.n[d][lane] = (uint8_t)cnn[d];
-                    nonempty = nonempty && cnn[d] > 0;
-                }
-                const float4 pj = R.pl[j], pk = R.pl[j + 1];
-                const float ax = fabsf(pj.x), ay = fabsf(pj.y), az = fabsf(pj.z);
-                const int a = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
-                C.axis[lane] = (uint8_t)a;
-                const int nbv = a == 0 ? cnn[1] : (a == 1 ? cnn[2] : cnn[0]);
-                const int ncv = a == 0 ? cnn[2] : (a == 1 ? cnn[0] : cnn[1]);
-                C.nb[lane] = (uint8_t)nbv;
-                C.rnb[lane] = nonempty ? 1.000001f / (float)nbv : 0.0f;
-                const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
-                const float tb = a == 0 ? pk.x : (a == 1 ? pk.y : pk.z);
-                // the bounds below carry margins of 0.05 point and 1 %: approximate reciprocals
-                // (a few ulp) are ample, and the reference's tests decide every candidate
-                C.isa[lane] = __fdividef(1.0f, R.dx * ta);
-                C.isb[lane] = fabsf(tb) > 0.05f ? __fdividef(1.0f, R.dx * tb) : 0.0f;
-                const float q2 = R.dx * R.dx * (1.0f - ta * ta);
-                C.q2[lane] = q2 > 0.01f * R.dx * R.dx ? q2 : 0.0f;
-                C.i2q[lane] = q2 > 0.01f * R.dx * R.dx ? __fdividef(0.5f, q2) : 0.0f;
-                C.ncol[lane] = 0;
-                nrows = nonempty ? nbv * ncv : 0;
-                const float cth = pj.x * pk.x + pj.y * pk.y + pj.z * pk.z;
-                if (nonempty && ncv <= kMaxCol && cth > 0.5f) {
-                    // the chord's sweep and the ellipse of its cross-section, in (b, c)
-                    const float4 oj = R.po[j], ok1 = R.po[j + 1];
-                    const float lx_ = oj.x - ok1.x, ly_ = oj.y - ok1.y, lz_ = oj.z - ok1.z;
-                    const float rt = sqrtf(R.chq[j].y);
-                    const float sweep = sqrtf(lx_ * lx_ + ly_ * ly_ + lz_ * lz_) +
-                                        __fdividef(rt * sqrtf(fmaxf(1.0f - cth * cth, 0.0f)), cth);
-                    const int b = a == 2 ? 0 : a + 1, cc = a == 0 ? 2 : a - 1;
-                    const float nb_ = b == 0 ? pj.x : (b == 1 ? pj.y : pj.z);
-                    const float nc_ = cc == 0 ? pj.x : (cc == 1 ? pj.y : pj.z);
-                    const float nbc = sqrtf(nb_ * nb_ + nc_ * nc_);
-                    const float inbc = nbc > 1e-4f ? __fdividef(1.0f, nbc) : 0.0f;
-                    const float wb = nbc > 1e-4f ? nb_ * inbc : 1.0f, wc = nbc > 1e-4f ? nc_ * inbc : 0.0f;
-                    const float Bm = rt * fabsf(ta);
-                    const float f = 1.0f + __fdividef(sweep * nbc, 2.0f * Bm);
-                    const float Ae = fmaf(f * rt, 1.01f, 0.05f * R.dx), Be = fmaf(f * Bm, 1.01f, 0.05f * R.dx);
-                    const float ia2 = __fdividef(1.0f, Ae * Ae), ib2 = __fdividef(1.0f, Be * Be);
-                    // centre: S_j + (sweep / 2) n, with S_j = -po[j] (mesh-point offsets times dx)
-                    const float sb = -(b == 0 ? oj.x : (b == 1 ? oj.y : oj.z)), sc = -(cc == 0 ? oj.x : (cc == 1 ? oj.y : oj.z));
-                    const float Cb = fmaf(0.5f * sweep, nb_, sb), Cc = fmaf(0.5f * sweep, nc_, sc);
-                    const int ob = b == 0 ? co[0] : (b == 1 ? co[1] : co[2]);
-                    const int oc = cc == 0 ? co[0] : (cc == 1 ? co[1] : co[2]);
-                    const float al = fmaf(wc * wc, ia2, wb * wb * ib2);
-                    const float cross_ = 2.0f * wb * wc * (ib2 - ia2);
-                    const float g2 = fmaf(wb * wb, ia2, wc * wc * ib2);
-                    const float i2a = __fdividef(0.5f, al);
-                    int rows = 0;
-                    const float idx = __fdividef(1.0f, R.dx);
-#pragma unroll 1
-                    for (int jc = 0; jc < ncv; ++jc) {
-                        const float z = fmaf((float)(oc + jc), R.dx, -Cc);
-                        const float be = cross_ * z, ga = fmaf(g2 * z, z, -1.0f);
-                        const float disc = fmaf(be, be, -4.0f * al * ga);
-                        int jb0 = 0, nrow = 0;
-                        if (disc >= 0.0f) {
-                            const float sq = sqrtf(disc);
-                            const float y1 = (-be - sq) * i2a, y2 = (-be + sq) * i2a;
-                            const float u1 = fmaf(Cb + y1, idx, -(float)ob), u2 = fmaf(Cb + y2, idx, -(float)ob);
-                            jb0 = max(0, (int)ceilf(fmaxf(u1, -2.0f) - 0.05f));
-                            const int jb1 = min(nbv - 1, (int)floorf(fminf(u2, (float)nbv + 1.0f) + 0.05f));
-                            nrow = max(0, jb1 - jb0 + 1);
-                        }
-                        C.col[jc][lane] = (uint16_t)(rows | (jb0 << 12));
-                        rows += nrow;
-                    }
-                    C.ncol[lane] = (uint8_t)ncv;
-                    nrows = rows;
-                }
+        if constexpr (Raster) {
+            // the staged pieces' rasterised points (piece_raster_kernel) that lie in this tile,
+            // flattened over the pieces, one per lane
+            int64_t p0 = 0, pn = 0;
+            if (lane < nc) {
+                const uint32_t id = v & ((1u << 26) - 1u);
+                p0 = ras_off[id];
+                pn = S.box[lane].vol > 0 ? ras_off[id + 1] - p0 : 0;
             }
-        }
-        int incl = nrows;
+            int64_t start[kPChunk], pbase[kPChunk], total = 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        const int roff = incl - nrows;
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        __syncwarp();
-        // Rows, one per lane: the index interval where the row can pass chord j's two planes
-        // and its cylinder (with a 0.05-point margin and Rtube^2 widened by 2e-3, far above the
-        // FP32 rounding of the bounds); its points join the candidate queue, which is tested
-        // 32 at a time.
-        int cn = 0;   // queued candidates (warp-uniform)
-        for (int r0 = 0; r0 < total; r0 += 32) {
-            const int r = r0 + lane;
-            int c = 0;   // chord lane of row r: last lane whose first row is <= r
-#pragma unroll
-            for (int step = 16; step > 0; step >>= 1) {
-                const int t = c + step;
-                const int ot = __shfl_sync(0xffffffffu, roff, t);
-                if (ot <= r) c = t;
+            for (int k = 0; k < kPChunk; ++k) {
+                start[k] = total;
+                pbase[k] = __shfl_sync(0xffffffffu, p0, k);
+                total += __shfl_sync(0xffffffffu, pn, k);
             }
-            const int rc = __shfl_sync(0xffffffffu, roff, c);
-            int i = 1, ihi = 0, a = 0, lx = 0, ly = 0, lz = 0;
-            if (r < total) {
-                const int k = c >> 3, j = c & 7;
-                const ChordRows &C = S.cr;
-                const PieceRec &R = S.rec[k];
-                const PBox &B = S.box[k];
-                a = C.axis[c];
-                const int rr = r - rc;
-                int jc, jb;
-                if (C.ncol[c] > 0) {
-                    // column of row rr: last column whose first row is <= rr (ncol <= 16)
-                    jc = 0;
-#pragma unroll
-                    for (int step = 8; step > 0; step >>= 1) {
-                        const int t = jc + step;
-                        if (t < C.ncol[c] && (int)(C.col[t][c] & 0xfffu) <= rr) jc = t;
-                    }
-                    jb = (int)(C.col[jc][c] >> 12) + (rr - (int)(C.col[jc][c] & 0xfffu));
-                } else {
-                    jc = (int)((float)rr * C.rnb[c]);
-                    if (jc * C.nb[c] > rr) --jc;
-                    jb = rr - jc * C.nb[c];
-                }
-                const int bx = C.o[0][c] + (a == 0 ? 0 : (a == 1 ? jc : jb));
-                const int by = C.o[1][c] + (a == 0 ? jb : (a == 1 ? 0 : jc));
-                const int bz = C.o[2][c] + (a == 0 ? jc : (a == 1 ? jb : 0));
-                lx = bx - B.dl[0];
-                ly = by - B.dl[1];
-                lz = bz - B.dl[2];
-                const float4 pj = R.pl[j], pk = R.pl[j + 1], oj = R.po[j], ok1 = R.po[j + 1];
-                // row base relative to sample j and to sample j + 1
-                const float ex = fmaf((float)bx, R.dx, oj.x), ey = fmaf((float)by, R.dx, oj.y),
-                            ez = fmaf((float)bz, R.dx, oj.z);
-                const float T0 = fmaf(ez, pj.z, fmaf(ey, pj.y, ex * pj.x));
-                const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
-                const int na = a == 0 ? C.n[0][c] : (a == 1 ? C.n[1][c] : C.n[2][c]);
-                float lo = -2.0f, hi = (float)na + 1.0f;
-                const float r0f = -T0 * C.isa[c];          // t_j >= 0
-                if (ta > 0.0f) lo = fmaxf(lo, r0f);
-                else hi = fminf(hi, r0f);
-                if (C.isb[c] != 0.0f) {                     // t_{j+1} < 0
-                    const float fx = fmaf((float)bx, R.dx, ok1.x), fy = fmaf((float)by, R.dx, ok1.y),
-                                fz = fmaf((float)bz, R.dx, ok1.z);
-                    const float T1 = fmaf(fz, pk.z, fmaf(fy, pk.y, fx * pk.x));
-                    const float r1f = -T1 * C.isb[c];
-                    if (C.isb[c] > 0.0f) hi = fminf(hi, r1f);
-                    else lo = fmaxf(lo, r1f);
-                }
-                if (C.q2[c] > 0.0f) {                       // rho^2 < Rtube^2 about chord line j
-                    const float ea = a == 0 ? ex : (a == 1 ? ey : ez);
-                    const float e2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-                    const float Q1 = 2.0f * R.dx * (ea - T0 * ta);
-                    const float Q0 = e2 - T0 * T0;
-                    const float R2w = fmaf(R.chq[j].y, 1.002f, 1e-6f * e2);
-                    const float disc = Q1 * Q1 - 4.0f * C.q2[c] * (Q0 - R2w);
-                    if (disc < 0.0f) {
-                        hi = -3.0f;
-                    } else {
-                        const float sq = sqrtf(disc);
-                        lo = fmaxf(lo, (-Q1 - sq) * C.i2q[c]);
-                        hi = fminf(hi, (-Q1 + sq) * C.i2q[c]);
-                    }
-                }
-                i = max(0, (int)ceilf(lo - 0.05f));
-                ihi = min(na - 1, (int)floorf(hi + 0.05f));
-            }
-            while (__any_sync(0xffffffffu, i <= ihi)) {
-                const bool has = i <= ihi;
+            for (int64_t t0 = 0; t0 < total; t0 += 32) {
+                const int64_t t = t0 + lane;
+                bool ok = false;
                 uint32_t code = 0u;
-                if (has) {
-                    code = (uint32_t)c | ((uint32_t)(lx + (a == 0 ? i : 0)) << 5) |
-                           ((uint32_t)(ly + (a == 1 ? i : 0)) << 9) | ((uint32_t)(lz + (a == 2 ? i : 0)) << 12);
-                    ++i;
+                if (t < total) {
+                    int k = 0;
+#pragma unroll
+                    for (int kk = 1; kk < kPChunk; ++kk)
+                        if (kk < nc && t >= start[kk]) k = kk;
+                    const uint32_t e = __ldg(ras_pts + pbase[k] + (t - start[k]));
+                    const int j = (int)(e & 7u);
+                    const PBox &B = S.box[k];
+                    const int lx = (int)((e >> 3) & 511u) - B.dl[0], ly = (int)((e >> 12) & 511u) - B.dl[1],
+                              lz = (int)((e >> 21) & 511u) - B.dl[2];
+                    ok = lx >= B.lo[0] && lx < B.lo[0] + B.n[0] && ly >= B.lo[1] && ly < B.lo[1] + B.n[1] &&
+                         lz >= B.lo[2] && lz < B.lo[2] + B.n[2];
+                    code = (uint32_t)k | ((uint32_t)j << 3) | ((uint32_t)lx << 6) | ((uint32_t)ly << 10) |
+                           ((uint32_t)lz << 13);
                 }
-                const unsigned bal = __ballot_sync(0xffffffffu, has);
-                if (has) S.cq[cn + __popc(bal & ((1u << lane) - 1u))] = code;
-                cn += __popc(bal);
+                const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                if (ok) S.q[qn + __popc(bal & ((1u << lane) - 1u))] = code;
+                qn += __popc(bal);
                 __syncwarp();
-                if (cn >= 32) test_candidates<General, F64>(S, acc, lane, 32, cn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+                if (qn >= 32)
+                    drain_pieces<General, F64>(S, acc, lane, 32, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
             }
+        } else {
+            // lane = (piece k, chord j): chord j's box clipped to the tile and its rows
+            int nrows = 0;
+            {
+                const int k = lane >> 3, j = lane & 7;
+                if (k < nc && j < S.rec[k].nch && S.box[k].vol > 0) {
+                    const PieceRec &R = S.rec[k];
+                    const PBox &B = S.box[k];
+                    const uint32_t blo = __float_as_uint(R.chq[j].z), bhi = __float_as_uint(R.chq[j].w);
+                    ChordRows &C = S.cr;
+                    bool nonempty = true;
+                    int co[3], cnn[3];
+    #pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const int tlo = B.lo[d] + B.dl[d], thi = tlo + B.n[d] - 1;   // the tile part of the piece box
+                        const int lo = max(tlo, unpack3(blo, d)), hi = min(thi, unpack3(bhi, d));
+                        co[d] = lo;
+                        cnn[d] = max(0, hi - lo + 1);
+                        C.o[d][lane] = (uint16_t)lo;
+                        C.n[d][lane] = (uint8_t)cnn[d];
+                        nonempty = nonempty && cnn[d] > 0;
+                    }
+                    const float4 pj = R.pl[j], pk = R.pl[j + 1];
+                    const float ax = fabsf(pj.x), ay = fabsf(pj.y), az = fabsf(pj.z);
+                    const int a = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+                    C.axis[lane] = (uint8_t)a;
+                    const int nbv = a == 0 ? cnn[1] : (a == 1 ? cnn[2] : cnn[0]);
+                    const int ncv = a == 0 ? cnn[2] : (a == 1 ? cnn[0] : cnn[1]);
+                    C.nb[lane] = (uint8_t)nbv;
+                    C.rnb[lane] = nonempty ? 1.000001f / (float)nbv : 0.0f;
+                    const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
+                    const float tb = a == 0 ? pk.x : (a == 1 ? pk.y : pk.z);
+                    // the bounds below carry margins of 0.05 point and 1 %: approximate reciprocals
+                    // (a few ulp) are ample, and the reference's tests decide every candidate
+                    C.isa[lane] = __fdividef(1.0f, R.dx * ta);
+                    C.isb[lane] = fabsf(tb) > 0.05f ? __fdividef(1.0f, R.dx * tb) : 0.0f;
+                    const float q2 = R.dx * R.dx * (1.0f - ta * ta);
+                    C.q2[lane] = q2 > 0.01f * R.dx * R.dx ? q2 : 0.0f;
+                    C.i2q[lane] = q2 > 0.01f * R.dx * R.dx ? __fdividef(0.5f, q2) : 0.0f;
+                    C.ncol[lane] = 0;
+                    nrows = nonempty ? nbv * ncv : 0;
+                    const float cth = pj.x * pk.x + pj.y * pk.y + pj.z * pk.z;
+                    if (nonempty && ncv <= kMaxCol && cth > 0.5f) {
+                        // the chord's sweep and the ellipse of its cross-section, in (b, c)
+                        const float4 oj = R.po[j], ok1 = R.po[j + 1];
+                        const float lx_ = oj.x - ok1.x, ly_ = oj.y - ok1.y, lz_ = oj.z - ok1.z;
+                        const float rt = sqrtf(R.chq[j].y);
+                        const float sweep = sqrtf(lx_ * lx_ + ly_ * ly_ + lz_ * lz_) +
+                                            __fdividef(rt * sqrtf(fmaxf(1.0f - cth * cth, 0.0f)), cth);
+                        const int b = a == 2 ? 0 : a + 1, cc = a == 0 ? 2 : a - 1;
+                        const float nb_ = b == 0 ? pj.x : (b == 1 ? pj.y : pj.z);
+                        const float nc_ = cc == 0 ? pj.x : (cc == 1 ? pj.y : pj.z);
+                        const float nbc = sqrtf(nb_ * nb_ + nc_ * nc_);
+                        const float inbc = nbc > 1e-4f ? __fdividef(1.0f, nbc) : 0.0f;
+                        const float wb = nbc > 1e-4f ? nb_ * inbc : 1.0f, wc = nbc > 1e-4f ? nc_ * inbc : 0.0f;
+                        const float Bm = rt * fabsf(ta);
+                        const float f = 1.0f + __fdividef(sweep * nbc, 2.0f * Bm);
+                        const float Ae = fmaf(f * rt, 1.01f, 0.05f * R.dx), Be = fmaf(f * Bm, 1.01f, 0.05f * R.dx);
+                        const float ia2 = __fdividef(1.0f, Ae * Ae), ib2 = __fdividef(1.0f, Be * Be);
+                        // centre: S_j + (sweep / 2) n, with S_j = -po[j] (mesh-point offsets times dx)
+                        const float sb = -(b == 0 ? oj.x : (b == 1 ? oj.y : oj.z)), sc = -(cc == 0 ? oj.x : (cc == 1 ? oj.y : oj.z));
+                        const float Cb = fmaf(0.5f * sweep, nb_, sb), Cc = fmaf(0.5f * sweep, nc_, sc);
+                        const int ob = b == 0 ? co[0] : (b == 1 ? co[1] : co[2]);
+                        const int oc = cc == 0 ? co[0] : (cc == 1 ? co[1] : co[2]);
+                        const float al = fmaf(wc * wc, ia2, wb * wb * ib2);
+                        const float cross_ = 2.0f * wb * wc * (ib2 - ia2);
+                        const float g2 = fmaf(wb * wb, ia2, wc * wc * ib2);
+                        const float i2a = __fdividef(0.5f, al);
+                        int rows = 0;
+                        const float idx = __fdividef(1.0f, R.dx);
+    #pragma unroll 1
+                        for (int jc = 0; jc < ncv; ++jc) {
+                            const float z = fmaf((float)(oc + jc), R.dx, -Cc);
+                            const float be = cross_ * z, ga = fmaf(g2 * z, z, -1.0f);
+                            const float disc = fmaf(be, be, -4.0f * al * ga);
+                            int jb0 = 0, nrow = 0;
+                            if (disc >= 0.0f) {
+                                const float sq = sqrtf(disc);
+                                const float y1 = (-be - sq) * i2a, y2 = (-be + sq) * i2a;
+                                const float u1 = fmaf(Cb + y1, idx, -(float)ob), u2 = fmaf(Cb + y2, idx, -(float)ob);
+                                jb0 = max(0, (int)ceilf(fmaxf(u1, -2.0f) - 0.05f));
+                                const int jb1 = min(nbv - 1, (int)floorf(fminf(u2, (float)nbv + 1.0f) + 0.05f));
+                                nrow = max(0, jb1 - jb0 + 1);
+                            }
+                            C.col[jc][lane] = (uint16_t)(rows | (jb0 << 12));
+                            rows += nrow;
+                        }
+                        C.ncol[lane] = (uint8_t)ncv;
+                        nrows = rows;
+                    }
+                }
+            }
+            int incl = nrows;
+    #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int roff = incl - nrows;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            __syncwarp();
+            // Rows, one per lane: the index interval where the row can pass chord j's two planes
+            // and its cylinder (with a 0.05-point margin and Rtube^2 widened by 2e-3, far above the
+            // FP32 rounding of the bounds); its points join the candidate queue, which is tested
+            // 32 at a time.
+            int cn = 0;   // queued candidates (warp-uniform)
+            for (int r0 = 0; r0 < total; r0 += 32) {
+                const int r = r0 + lane;
+                int c = 0;   // chord lane of row r: last lane whose first row is <= r
+    #pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int t = c + step;
+                    const int ot = __shfl_sync(0xffffffffu, roff, t);
+                    if (ot <= r) c = t;
+                }
+                const int rc = __shfl_sync(0xffffffffu, roff, c);
+                int i = 1, ihi = 0, a = 0, lx = 0, ly = 0, lz = 0;
+                if (r < total) {
+                    const int k = c >> 3, j = c & 7;
+                    const ChordRows &C = S.cr;
+                    const PieceRec &R = S.rec[k];
+                    const PBox &B = S.box[k];
+                    a = C.axis[c];
+                    const int rr = r - rc;
+                    int jc, jb;
+                    if (C.ncol[c] > 0) {
+                        // column of row rr: last column whose first row is <= rr (ncol <= 16)
+                        jc = 0;
+    #pragma unroll
+                        for (int step = 8; step > 0; step >>= 1) {
+                            const int t = jc + step;
+                            if (t < C.ncol[c] && (int)(C.col[t][c] & 0xfffu) <= rr) jc = t;
+                        }
+                        jb = (int)(C.col[jc][c] >> 12) + (rr - (int)(C.col[jc][c] & 0xfffu));
+                    } else {
+                        jc = (int)((float)rr * C.rnb[c]);
+                        if (jc * C.nb[c] > rr) --jc;
+                        jb = rr - jc * C.nb[c];
+                    }
+                    const int bx = C.o[0][c] + (a == 0 ? 0 : (a == 1 ? jc : jb));
+                    const int by = C.o[1][c] + (a == 0 ? jb : (a == 1 ? 0 : jc));
+                    const int bz = C.o[2][c] + (a == 0 ? jc : (a == 1 ? jb : 0));
+                    lx = bx - B.dl[0];
+                    ly = by - B.dl[1];
+                    lz = bz - B.dl[2];
+                    const float4 pj = R.pl[j], pk = R.pl[j + 1], oj = R.po[j], ok1 = R.po[j + 1];
+                    // row base relative to sample j and to sample j + 1
+                    const float ex = fmaf((float)bx, R.dx, oj.x), ey = fmaf((float)by, R.dx, oj.y),
+                                ez = fmaf((float)bz, R.dx, oj.z);
+                    const float T0 = fmaf(ez, pj.z, fmaf(ey, pj.y, ex * pj.x));
+                    const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
+                    const int na = a == 0 ? C.n[0][c] : (a == 1 ? C.n[1][c] : C.n[2][c]);
+                    float lo = -2.0f, hi = (float)na + 1.0f;
+                    const float r0f = -T0 * C.isa[c];          // t_j >= 0
+                    if (ta > 0.0f) lo = fmaxf(lo, r0f);
+                    else hi = fminf(hi, r0f);
+                    if (C.isb[c] != 0.0f) {                     // t_{j+1} < 0
+                        const float fx = fmaf((float)bx, R.dx, ok1.x), fy = fmaf((float)by, R.dx, ok1.y),
+                                    fz = fmaf((float)bz, R.dx, ok1.z);
+                        const float T1 = fmaf(fz, pk.z, fmaf(fy, pk.y, fx * pk.x));
+                        const float r1f = -T1 * C.isb[c];
+                        if (C.isb[c] > 0.0f) hi = fminf(hi, r1f);
+                        else lo = fmaxf(lo, r1f);
+                    }
+                    if (C.q2[c] > 0.0f) {                       // rho^2 < Rtube^2 about chord line j
+                        const float ea = a == 0 ? ex : (a == 1 ? ey : ez);
+                        const float e2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+                        const float Q1 = 2.0f * R.dx * (ea - T0 * ta);
+                        const float Q0 = e2 - T0 * T0;
+                        const float R2w = fmaf(R.chq[j].y, 1.002f, 1e-6f * e2);
+                        const float disc = Q1 * Q1 - 4.0f * C.q2[c] * (Q0 - R2w);
+                        if (disc < 0.0f) {
+                            hi = -3.0f;
+                        } else {
+                            const float sq = sqrtf(disc);
+                            lo = fmaxf(lo, (-Q1 - sq) * C.i2q[c]);
+                            hi = fminf(hi, (-Q1 + sq) * C.i2q[c]);
+                        }
+                    }
+                    i = max(0, (int)ceilf(lo - 0.05f));
+                    ihi = min(na - 1, (int)floorf(hi + 0.05f));
+                }
+                while (__any_sync(0xffffffffu, i <= ihi)) {
+                    const bool has = i <= ihi;
+                    uint32_t code = 0u;
+                    if (has) {
+                        code = (uint32_t)c | ((uint32_t)(lx + (a == 0 ? i : 0)) << 5) |
+                               ((uint32_t)(ly + (a == 1 ? i : 0)) << 9) | ((uint32_t)(lz + (a == 2 ? i : 0)) << 12);
+                        ++i;
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, has);
+                    if (has) S.cq[cn + __popc(bal & ((1u << lane) - 1u))] = code;
+                    cn += __popc(bal);
+                    __syncwarp();
+                    if (cn >= 32) test_candidates<General, F64>(S, acc, lane, 32, cn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+                }
+            }
+            if (cn > 0) test_candidates<General, F64>(S, acc, lane, cn, cn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
         }
-        if (cn > 0) test_candidates<General, F64>(S, acc, lane, cn, cn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
         if (qn > 0) drain_pieces<General, F64>(S, acc, lane, qn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
         __syncwarp();   // the warp's stage is reused by its next chunk
         int nxt = 0;
@@ -821,6 +959,8 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
 }
 
 // ------------------------------------------------------------------------------ host
+int piece_raster(Ctx *c, CenterlineBatch &B, int *d_err);
+
 // Set-up of the batch's pieces (after the section pass of centerline_setup).
 int piece_setup(Ctx *c, CenterlineBatch &B)
 {
@@ -859,6 +999,50 @@ int piece_setup(Ctx *c, CenterlineBatch &B)
     FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     FWT_CUDA(cudaStreamSynchronize(c->stream));
     if (herr & 8) return fail(FWT_E_RANGE, "piece box wider than 1023 grid points");
+    if (B.raster && np_ > 0) FWT_TRY(piece_raster(c, B, d_err));
+    return 0;
+}
+
+// Rasterise the batch's pieces (piece_raster_kernel): count, scan, write.  A batch whose chord
+// boxes exceed the 9-bit offsets, or whose point list would exceed the memory budget, is
+// deposited by the row search instead (B.raster = false).
+int piece_raster(Ctx *c, CenterlineBatch &B, int *d_err)
+{
+    Ctx &C = *c;
+    const int64_t np_ = B.npieces;
+    const bool wide = c->p.precision == 64;
+    FWT_TRY(buf_reserve(c, C.scratch[25], sizeof(int64_t) * (size_t)(np_ + 1)));
+    int64_t *d_off = (int64_t *)C.scratch[25].p;
+    FWT_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
+    const unsigned g = (unsigned)((np_ + 127) / 128);
+    int km = kt_begin(c, KT_CENTERLINE);
+    if (wide) piece_raster_kernel<true, false><<<g, 128, 0, c->stream>>>(B.piece, np_, d_off, nullptr, d_err);
+    else piece_raster_kernel<false, false><<<g, 128, 0, c->stream>>>(B.piece, np_, d_off, nullptr, d_err);
+    FWT_TRY(scan_exclusive_i64(c, d_off, np_, d_off + np_, C.scratch[12]));
+    kt_end(c, km);
+    int64_t total = 0;
+    int herr = 0;
+    FWT_CUDA(cudaMemcpyAsync(&total, d_off + np_, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    const int64_t budget = (int64_t)1 << 32;   // points (16 GB of codes)
+    if ((herr & 16) || total > budget) {
+        B.raster = false;
+        return 0;
+    }
+    FWT_TRY(buf_reserve(c, C.scratch[26], sizeof(uint32_t) * (size_t)std::max<int64_t>(total, 1)));
+    uint32_t *d_pts = (uint32_t *)C.scratch[26].p;
+    km = kt_begin(c, KT_CENTERLINE);
+    if (wide) piece_raster_kernel<true, true><<<g, 128, 0, c->stream>>>(B.piece, np_, d_off, d_pts, d_err);
+    else piece_raster_kernel<false, true><<<g, 128, 0, c->stream>>>(B.piece, np_, d_off, d_pts, d_err);
+    kt_end(c, km);
+    c->launches += 5;
+    FWT_CUDA(cudaGetLastError());
+    FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    if (herr & 32) return fail(FWT_E_STATE, "piece raster: the two passes disagreed on a piece's points");
+    B.ras_off = d_off;
+    B.ras_pts = d_pts;
     return 0;
 }
 
@@ -926,21 +1110,26 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     RedoCtx rctx = redo_ctx(c, B, scale, true);
     rctx.tally = (unsigned long long *)((char *)C.scratch[19].p + 64);
     km = kt_begin(c, KT_DEPOSIT);
-#define FWT_PIECE_LAUNCH(G, A, D)                                                                          \
+#define FWT_PIECE_LAUNCH(G, A, D, R)                                                                       \
     do {                                                                                                   \
-        FWT_CUDA(cudaFuncSetAttribute(deposit_piece_kernel<G, A, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                      (int)kPieceSmem));                                                   \
-        deposit_piece_kernel<G, A, D><<<(unsigned)ntiles, kDepThreads, kPieceSmem, c->stream>>>(          \
-            B.piece, N, ntx, nty, d_toff, d_list, scale, wx, wy, wz, d_err, rctx);                    \
+        FWT_CUDA(cudaFuncSetAttribute(deposit_piece_kernel<G, A, D, R>,                                    \
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPieceSmem));      \
+        deposit_piece_kernel<G, A, D, R><<<(unsigned)ntiles, kDepThreads, kPieceSmem, c->stream>>>(       \
+            B.piece, N, ntx, nty, d_toff, d_list, scale, wx, wy, wz, d_err, rctx, B.ras_off, B.ras_pts);    \
         FWT_CUDA(cudaGetLastError());                                                                      \
     } while (0)
+#define FWT_PIECE_LAUNCH_R(G, A, D)                                                                        \
+    do {                                                                                                   \
+        if (B.raster) FWT_PIECE_LAUNCH(G, A, D, true); else FWT_PIECE_LAUNCH(G, A, D, false);              \
+    } while (0)
     if (f64) {
-        if (accumulate) FWT_PIECE_LAUNCH(true, true, true); else FWT_PIECE_LAUNCH(true, false, true);
+        if (accumulate) FWT_PIECE_LAUNCH_R(true, true, true); else FWT_PIECE_LAUNCH_R(true, false, true);
     } else if (general) {
-        if (accumulate) FWT_PIECE_LAUNCH(true, true, false); else FWT_PIECE_LAUNCH(true, false, false);
+        if (accumulate) FWT_PIECE_LAUNCH_R(true, true, false); else FWT_PIECE_LAUNCH_R(true, false, false);
     } else {
-        if (accumulate) FWT_PIECE_LAUNCH(false, true, false); else FWT_PIECE_LAUNCH(false, false, false);
+        if (accumulate) FWT_PIECE_LAUNCH_R(false, true, false); else FWT_PIECE_LAUNCH_R(false, false, false);
     }
+#undef FWT_PIECE_LAUNCH_R
 #undef FWT_PIECE_LAUNCH
     kt_end(c, km);
     c->launches += 2;

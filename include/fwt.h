@@ -210,6 +210,11 @@ int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
  * restores the default, 8).  Results agree within FP32 rounding either way; the choice is
  * speed only, and the ensemble autotuner sets it per grid size. */
 #define FWT_TUNE_PIECE_RT_CELLS 1
+/* FWT_TUNE_RASTER_RT_CELLS: piece lines whose truncation radius is at most `value` grid
+ * spacings are rasterised once per piece (their accepted points listed before the deposition)
+ * instead of searched within every tile; 0 switches it off, value < 0 restores the default, 2.5.
+ * The accepted points and their values are the same either way. */
+#define FWT_TUNE_RASTER_RT_CELLS 2
 int fwt_set_tuning(fwt_ctx *ctx, int key, double value);
 
 /* Message of the last error on this thread. */

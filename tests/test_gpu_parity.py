@@ -103,6 +103,32 @@ def test_ntf_bit_exact_across_curvatures(fwt, orc, H, dB_over_sigma):
     ctx.close()
 
 
+@pytest.mark.parametrize("precision", [32, 64])
+def test_rasterised_pieces_equal_searched_pieces(fwt, orc, precision):
+    """Thin tubes (truncation radius 0.6-1.2 grid spacings on 64^3): the pieces rasterised once
+    (the default below 2.5 grid spacings) and the pieces searched in every tile accept the same
+    points with the same test, so the FP32 fields are identical (int64 fixed-point sums) and the
+    FP64 fields agree to the order of their FP64 additions; both match the oracle."""
+    from fastweavturb_b200.configs import small
+    w = small(N=64, seed=7, nlev=2, tubes0=3, nodes0=128, sigma0=0.04)
+    p, cl = oracle_inputs(orc, w)
+    fields = {}
+    for cells in (-1.0, 0.0):
+        ctx = fwt.Context(gpu_params(fwt, w, precision=precision, deposit_mode=0))
+        ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+        ctx.set_raster_radius_limit(cells)
+        ctx.deposit(1, w.ntubes)
+        fields[cells] = ctx.field(0).copy()
+        ctx.close()
+    assert np.abs(fields[-1.0]).max() > 0
+    if precision == 32:
+        assert np.array_equal(fields[-1.0], fields[0.0])
+    else:
+        assert rel_l2(fields[-1.0], fields[0.0]) <= 1e-15
+    vor, _ = orc.deposit(p, cl)
+    assert rel_l2(fields[-1.0], vor) <= (TOL32 if precision == 32 else TOL64)
+
+
 def test_piece_and_subsegment_kernels_agree(fwt, orc):
     """Thin tubes (Rtube 1.2-1.9 grid spacings on 64^3) deposited by the chord-piece kernel and
     by the sub-segment kernel: the same accepted points, evaluated by two forms of the same
