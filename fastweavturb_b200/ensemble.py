@@ -10,10 +10,17 @@ synchronisations, overlap on the device.  Each realisation's centerlines are gen
 device, the field is built and its statistics stay on the device until read.
 
 Autotuner: before the first realisation of a grid size, the deposition of a probe
-realisation is timed with the chord-piece kernel limit at each candidate value (the tube
-radius in grid spacings up to which the piece kernel is used instead of the sub-segment
-kernel) and the fastest is kept for the rest of that size.  Both kernels give the same
-field within FP32 rounding; only the speed differs.
+realisation is timed over the deposition kernels' selection limits, one after the other: the
+tube radius (grid spacings) up to which lines take the chord-piece kernel instead of the
+sub-segment kernel, then the radius up to which pieces are rasterised once instead of searched
+per tile.  The fastest setting of each is kept for the rest of that size.  Every choice gives
+the same field within FP32 rounding; only the speed differs.  (The tile shape itself,
+16 x 8 x 8 points, is fixed at compile time.)
+
+    python -m fastweavturb_b200.ensemble [--members 64] [--workers 4]
+
+runs the benchmark ensemble (configs.ensemble_member with seeds 1..members) and prints its
+Mpts/s next to the same members built one at a time.
 """
 from __future__ import annotations
 
@@ -27,7 +34,8 @@ import numpy as np
 from .api import Context, Params, sp_exponents
 from .configs import build_workload
 
-TUNE_CANDIDATES = (0.0, 2.5, 5.0, 8.0)
+TUNE_CANDIDATES = (0.0, 2.5, 5.0, 8.0)          # chord-piece kernel radius limit
+RASTER_CANDIDATES = (0.0, 1.5, 2.5, 4.0)        # rasterised pieces radius limit
 
 
 class Ensemble:
@@ -50,35 +58,48 @@ class Ensemble:
                                                device=self.device, pdf_bins=201, Sp_order=self.Sp_order,
                                                vorticity_output=0))
                 if N in self.tuned:
-                    self.ctx[key].set_piece_radius_limit(self.tuned[N])
+                    self.ctx[key].set_piece_radius_limit(self.tuned[N][0])
+                    self.ctx[key].set_raster_radius_limit(self.tuned[N][1])
             return self.ctx[key]
 
     def _load(self, ctx, w):
         return build_workload(ctx, w)
 
     def autotune(self, w):
-        """Time the deposition of workload w for every candidate limit; keep the fastest."""
+        """Time the deposition of workload w over the piece limit, then over the raster limit
+        (at the best piece limit); keep the fastest of each."""
         import torch
         ctx = self.context(w.N)
         keep = self._load(ctx, w)
-        times = {}
-        for cells in TUNE_CANDIDATES:
-            ctx.set_piece_radius_limit(cells)
+
+        def timed():
             ctx.deposit(1, w.ntubes)        # warm (allocations for this kernel choice)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             ctx.deposit(1, w.ntubes)
             torch.cuda.synchronize()
-            times[cells] = time.perf_counter() - t0
-        best = min(times, key=times.get)
+            return time.perf_counter() - t0
+
+        times = {}
+        ctx.set_raster_radius_limit(-1.0)
+        for cells in TUNE_CANDIDATES:
+            ctx.set_piece_radius_limit(cells)
+            times[("piece", cells)] = timed()
+        best_piece = min(TUNE_CANDIDATES, key=lambda v: times[("piece", v)])
+        ctx.set_piece_radius_limit(best_piece)
+        for cells in RASTER_CANDIDATES:
+            ctx.set_raster_radius_limit(cells)
+            times[("raster", cells)] = timed()
+        best_raster = min(RASTER_CANDIDATES, key=lambda v: times[("raster", v)])
         with self._lock:
             for (n, _), c in self.ctx.items():
                 if n == w.N:
-                    c.set_piece_radius_limit(best)
-        self.tuned[w.N] = best
+                    c.set_piece_radius_limit(best_piece)
+                    c.set_raster_radius_limit(best_raster)
+        self.tuned[w.N] = (best_piece, best_raster)
         self.tune_log[w.N] = times
         del keep
-        return best
+        return self.tuned[w.N]
 
     def slots_for(self, N):
         """Contexts kept for grid size N: every worker for small fields, fewer for large ones,
@@ -142,3 +163,39 @@ def member_statistics(ctx, N, Sp_order=6):
     rdr = r * (2 * np.pi / N)
     zeta, flat = sp_exponents(rdr, Sp) if len(r) >= 10 else (np.full(Sp.shape[0], np.nan), Sp[3] / Sp[1] ** 2)
     return {"Ek": Ek, "r": r, "Sp": Sp, "zeta": zeta, "flat": flat, "up": s["up"], "Etot": s["Etot"]}
+
+
+def cfg3_members(n=64, seed0=1):
+    """The benchmark ensemble: n realisations, seeds seed0.., grid sizes, levels, H, density and
+    circulation exponent drawn per realisation (configs.ensemble_member)."""
+    from .configs import ensemble_member
+    return [ensemble_member(seed0 + k) for k in range(n)]
+
+
+def main(argv=None):
+    import argparse
+    import json
+
+    import torch
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--members", type=int, default=64)
+    ap.add_argument("--workers", type=int, default=4)
+    args = ap.parse_args(argv)
+    members = cfg3_members(args.members)
+    ens = Ensemble(workers=args.workers, tune=True)
+    ens.run(members[:min(4, len(members))], stats=False)     # warm: plans, buffers, autotuning
+    _, t_conc, rate = ens.run(members, stats=False)
+    # the same members one at a time (the sum of the single-field times)
+    ens.workers = 1
+    _, t_seq, rate_seq = ens.run(members, stats=False)
+    ens.close()
+    torch.cuda.synchronize()
+    print(json.dumps({"members": len(members), "points": sum(w.N ** 3 for w in members),
+                      "sizes": {str(N): sum(1 for w in members if w.N == N) for N in sorted({w.N for w in members})},
+                      "concurrent_s": t_conc, "concurrent_mpts_s": rate, "sequential_s": t_seq,
+                      "sequential_mpts_s": rate_seq, "tuned": {str(k): v for k, v in ens.tuned.items()}}))
+
+
+if __name__ == "__main__":
+    main()

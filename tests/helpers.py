@@ -5,15 +5,24 @@ import numpy as np
 
 
 def oracle_inputs(O, w, line_e=None):
-    """(Params, Centerlines) of workload `w` drawn with the oracle's own generator."""
-    xyz = []
+    """(Params, Centerlines) of workload `w` drawn with the oracle's own generator: one stream
+    numbered across the levels, or (w.level_streams) one stream per level."""
+    from fastweavturb_b200.configs import level_seed
+
+    xyz, signs = [], []
     t = 0
-    for L in w.levels:
-        for _ in range(L.tubes):
-            xyz.append(O.fbb_tube(w.seed, t, L.nodes, L.H, L.dB))
+    for lv, L in enumerate(w.levels):
+        for k in range(L.tubes):
+            if w.level_streams:
+                s = level_seed(w.seed, lv)
+                xyz.append(O.fbb_tube(s, k, L.nodes, L.H, L.dB))
+                signs.append(O.fbb_sign(s, k))
+            else:
+                xyz.append(O.fbb_tube(w.seed, t, L.nodes, L.H, L.dB))
+                signs.append(O.fbb_sign(w.seed, t))
             t += 1
     xyz = np.concatenate(xyz)
-    signs = np.array([O.fbb_sign(w.seed, i) for i in range(w.ntubes)])
+    signs = np.array(signs)
     npoint, sig, gam, nT = w.line_arrays(signs)
     p = O.Params(N=w.N, N_downsample=w.N, line_s=1, line_e=line_e or w.ntubes, sigma_ratio=w.sigma_ratio,
                  eta_t=w.eta_t, ntf_times=w.ntf_times, ntf_pre=w.ntf_pre, Rtube_ratio=w.Rtube_ratio,

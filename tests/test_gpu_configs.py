@@ -171,3 +171,25 @@ def test_isosurface_matches_the_restatement_bit_for_bit(fwt, orc, cfg0_case, tmp
     fwt.api.write_ply(tmp_path / "iso.ply", tris)
     assert (tmp_path / "iso.ply").stat().st_size > 48 * len(tris)
     ctx.close()
+
+
+def test_ensemble_member_matches_oracle(fwt, orc):
+    """A member of the benchmark ensemble (configs.ensemble_member: H, levels, density and
+    circulation exponent drawn from its seed, one generator stream per level), built through
+    the autotuned Ensemble, against the oracle run of the same centerlines: E(k), u' and
+    S_2..S_6 within the FP32 tolerance."""
+    from fastweavturb_b200.configs import ensemble_member
+    from fastweavturb_b200.ensemble import Ensemble
+
+    w = ensemble_member(18, N=64)            # 3 levels, 125 tubes, 111,104 nodes
+    assert w.level_streams and len(w.levels) == 3
+    p, cl = oracle_inputs(orc, w)
+    ref = orc.run(p, cl, sp_pmax=6)
+    ens = Ensemble(workers=1, tune=True)
+    (st,), secs, rate = ens.run([w])
+    assert 64 in ens.tuned
+    ens.close()
+    assert st["up"] == pytest.approx(ref["up"], rel=TOL32)
+    assert rel_l2(st["Ek"], ref["spectrum"]) <= TOL32
+    for q in range(1, 6):
+        np.testing.assert_allclose(st["Sp"][q], ref["Sp"][q], rtol=10 * TOL32)
