@@ -57,7 +57,7 @@ EXPORTS = [
     "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
     "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_field_uw", "fwt_field_wd",
     "fwt_set_outputs", "fwt_copy_field", "fwt_field_device", "fwt_vsf_deviation", "fwt_helicity",
-    "fwt_isosurface",
+    "fwt_isosurface", "fwt_set_slab", "fwt_biot_savart_block", "fwt_sp_block",
     "fwt_write_outputs", "fwt_run_dir", "fwt_run",
     "fwt_timings", "fwt_kernel_times", "fwt_counters", "fwt_last_error", "fwt_fbb_generate", "fwt_fbb_signs",
     "fwt_set_tuning", "fwt_mlp_create", "fwt_mlp_destroy", "fwt_mlp_nparams", "fwt_mlp_get_params", "fwt_mlp_set_params",
@@ -105,6 +105,9 @@ def library(path: str | None = None):
         "fwt_helicity": [vp, dp],
         "fwt_isosurface": [vp, ctypes.c_float, ctypes.POINTER(ctypes.c_float), ctypes.c_int64, i64p,
                            ctypes.POINTER(ctypes.c_float)],
+        "fwt_set_slab": [vp, ip, ip],
+        "fwt_biot_savart_block": [vp, vp, ip, ip, dp],
+        "fwt_sp_block": [vp, vp, ip, ip, ip, ip, ctypes.c_double, ctypes.POINTER(ctypes.c_int), ip, dp],
         "fwt_write_outputs": [vp, ctypes.c_char_p],
         "fwt_run_dir": [ctypes.c_char_p, ctypes.POINTER(_Params)],
         "fwt_run": [vp],
@@ -310,9 +313,10 @@ class Context:
 
     def copy_field(self, which, component):
         """which 0: omega, 1: u; normalised once cal_helicity ran.  Array [k, j, i]."""
-        out = np.zeros(self.N ** 3)
+        nz = self._slab[1] if getattr(self, "_slab", None) else self.N
+        out = np.zeros(self.N * self.N * nz)
         _check(library().fwt_copy_field(self._h, which, component, _ptr(out, ctypes.c_double)))
-        return out.reshape(self.N, self.N, self.N)
+        return out.reshape(nz, self.N, self.N)
 
     def field(self, which):
         return np.stack([self.copy_field(which, c) for c in range(3)])
@@ -379,6 +383,28 @@ class Context:
                                             ctypes.byref(n), ctypes.byref(used)))
         return tris[:n.value], float(used.value)
 
+    def set_slab(self, z0, nz):
+        """Hold and deposit only planes z0 .. z0 + nz - 1 (fwt_set_slab); (0, 0): the whole grid."""
+        _check(library().fwt_set_slab(self._h, int(z0), int(nz)))
+        self._slab = (int(z0), int(nz)) if nz else None
+
+    def biot_savart_block(self, spec_ptr, y0, ny):
+        """fwt_biot_savart_block on a device y-pencil; returns (shells_w, shells_u, energy, enstrophy)
+        of the pencil."""
+        nek = self.N // 2
+        out = np.zeros(2 * (nek + 1) + 2)
+        _check(library().fwt_biot_savart_block(self._h, ctypes.c_void_p(spec_ptr), int(y0), int(ny),
+                                               _ptr(out, ctypes.c_double)))
+        return out[1:nek + 1], out[nek + 2:2 * nek + 2], out[2 * nek + 2], out[2 * nek + 3]
+
+    def sp_block(self, u_ptr, n0, n1, n2, axis, scale, r):
+        """fwt_sp_block: S_p sums (10, len(r)) of one component on a device box along `axis`."""
+        r = np.ascontiguousarray(r, dtype=np.int32)
+        out = np.zeros(10 * len(r))
+        _check(library().fwt_sp_block(self._h, ctypes.c_void_p(u_ptr), n0, n1, n2, axis, float(scale),
+                                      _ptr(r, ctypes.c_int), len(r), _ptr(out, ctypes.c_double)))
+        return out.reshape(10, len(r))
+
     def field_tensor(self, which):
         """Zero-copy torch view (3, N, N, N), index [c, z, y, x], of the raw (unnormalised)
         field on the device (which = 0: omega, 1: u), in the context's precision.  Valid until
@@ -388,10 +414,11 @@ class Context:
         p = ctypes.c_void_p()
         _check(library().fwt_field_device(self._h, which, ctypes.byref(p)))
         N = self.N
+        nz = getattr(self, "_slab", None)[1] if getattr(self, "_slab", None) else N
         dt = "<f4" if self.params.precision == 32 else "<f8"
 
         class _View:
-            __cuda_array_interface__ = {"shape": (3, N, N, N), "typestr": dt, "data": (p.value, False),
+            __cuda_array_interface__ = {"shape": (3, nz, N, N), "typestr": dt, "data": (p.value, False),
                                         "version": 3, "strides": None}
 
         return torch.as_tensor(_View(), device=torch.device("cuda", self.params.device))

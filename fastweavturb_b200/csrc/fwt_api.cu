@@ -454,6 +454,44 @@ int fwt_field_wh(fwt_ctx *h, float *host_out)
     return stats_field_wh(c, host_out);
 }
 
+int fwt_set_slab(fwt_ctx *h, int z0, int nz)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c) return fail(FWT_E_ARG, "null context");
+    const int N = c->p.N;
+    if (nz == 0 && z0 == 0) {
+        c->slab_z0 = c->slab_nz = 0;
+    } else {
+        if (z0 < 0 || nz <= 0 || z0 + nz > N || z0 % 8 || nz % 8)
+            return fail(FWT_E_ARG, "slab: planes z0 .. z0 + nz - 1 within the grid, z0 and nz multiples of 8");
+        if (c->p.deposit_mode != 0) return fail(FWT_E_ARG, "slab: the tile-owned deposition only (deposit_mode 0)");
+        c->slab_z0 = z0;
+        c->slab_nz = nz;
+    }
+    // the field buffers change size: the next deposition starts from zero
+    buf_free(c, c->b_w);
+    buf_free(c, c->b_u);
+    reset_state(c);
+    return 0;
+}
+
+int fwt_biot_savart_block(fwt_ctx *h, void *spec, int y0, int ny, double *sums)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !spec || !sums) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    return spectral_block(c, spec, y0, ny, sums);
+}
+
+int fwt_sp_block(fwt_ctx *h, const void *u, int n0, int n1, int n2, int axis, double scale, const int *r, int nr,
+                 double *sums)
+{
+    Ctx *c = (Ctx *)h;
+    if (!c || !u || !r || !sums) return fail(FWT_E_ARG, "null argument");
+    cudaSetDevice(c->dev);
+    return stats_sp_block(c, u, n0, n1, n2, axis, scale, r, nr, sums);
+}
+
 int fwt_vsf_deviation(fwt_ctx *h, const void *d_phi, double *deviation)
 {
     Ctx *c = (Ctx *)h;

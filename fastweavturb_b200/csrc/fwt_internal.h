@@ -74,6 +74,7 @@ struct Timers {
 struct Ctx {
     fwt_params p{};
     int dev = 0;
+    int slab_z0 = 0, slab_nz = 0;   // z-slab context (fwt_set_slab): planes slab_z0 .. + slab_nz - 1; 0: whole grid
     double piece_rt_cells = -1.0;   // tuning: piece kernel radius limit in grid spacings (< 0: default)
     double raster_rt_cells = -1.0;  // tuning: radius limit of rasterised pieces in grid spacings (< 0: default)
     cudaStream_t stream = nullptr;
@@ -161,12 +162,15 @@ int deposit_lines(Ctx *c, int line_s, int line_e);
 int spectral_init(Ctx *c);
 int spectral_filter(Ctx *c, double k_c);
 int spectral_biot_savart(Ctx *c);
+int spectral_block(Ctx *c, void *spec, int y0, int ny, double *host_sums);
 
 // statistics (k_stats.cu)
 int stats_minmax(Ctx *c, int which);
 int stats_normalise(Ctx *c);
 int stats_pdf(Ctx *c, int which, int comp, int nbins, float *val, float *pdf, uint64_t *counts);
 int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp);
+int stats_sp_block(Ctx *c, const void *u, int n0, int n1, int n2, int axis, double s, const int *r, int nr,
+                   double *sums);
 int stats_field_wh(Ctx *c, float *host_out);
 int stats_field_uw(Ctx *c, float *host_out);
 int stats_field_wd(Ctx *c, float *host_out);
@@ -188,7 +192,10 @@ int fbb_generate(Ctx *c, uint64_t seed, int nlev, const int *tubes, const int *n
                  const double *dB, double *d_x, double *d_y, double *d_z);
 
 int scaling_exponents(const double *rdr, const double *Sp, int nr, int pmax, double *zeta, double *flat);
-inline size_t field_elems(const Ctx *c) { return (size_t)c->p.N * c->p.N * c->p.N; }
+inline size_t field_elems(const Ctx *c)
+{
+    return (size_t)c->p.N * c->p.N * (size_t)(c->slab_nz ? c->slab_nz : c->p.N);
+}
 inline size_t real_bytes(const Ctx *c) { return c->p.precision == 64 ? 8 : 4; }
 
 }  // namespace fwt

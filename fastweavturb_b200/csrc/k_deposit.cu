@@ -130,6 +130,7 @@ static int64_t batch_node_cap(const Ctx *c)
 int deposit_lines(Ctx *c, int line_s, int line_e)
 {
     if (!c->have_lines) return fail(FWT_E_STATE, "no centerlines set");
+    if (c->slab_nz && c->p.deposit_mode != 0) return fail(FWT_E_STATE, "a z-slab context deposits with deposit_mode 0");
     if (line_s < 1 || line_e > c->nline || line_s > line_e)
         return fail(FWT_E_ARG, "line range outside 1..nline");
     const size_t n3 = field_elems(c);

@@ -125,6 +125,7 @@ struct RedoCtx {
     const double *X, *Y, *Z, *cze, *coe, *dtf;
     int64_t node_base;
     int N, pieces;
+    int zs, nz;                // planes of the context's field: zs .. zs + nz - 1
     double Rtube_ratio, dzeta_sup, eta, scale;
 };
 

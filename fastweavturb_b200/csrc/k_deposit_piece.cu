@@ -644,7 +644,7 @@ __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[
 // that sample's own frame.  Accepted pairs are queued and evaluated 32 at a time.
 template <bool General, bool Accumulate, bool F64, bool Raster>
 __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel(
-    const PieceRec *__restrict__ rec, int N, int ntx, int nty, const int64_t *__restrict__ tile_off,
+    const PieceRec *__restrict__ rec, int N, int ntx, int nty, int tz0, const int64_t *__restrict__ tile_off,
     const uint32_t *__restrict__ list, double scale, void *__restrict__ wx, void *__restrict__ wy,
     void *__restrict__ wz, int *__restrict__ err, const RedoCtx redo, const int64_t *__restrict__ ras_off,
     const uint32_t *__restrict__ ras_pts)
@@ -656,8 +656,10 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
     // a tile that no record of this batch meets keeps its values: earlier batches wrote them,
     // or the field was cleared before the first
     if (c0 == c1) return;
-    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
+    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tz0 + tile / (ntx * nty);
     const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
+    // the context's planes: the whole grid, or its z-slab
+    const int zs = redo.zs, zlim = redo.zs + redo.nz;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     PieceStage &S = reinterpret_cast<PieceStage *>(dsm + kAccBytes)[warp];
     if (lane == 0) mbar_init(&S.bar);
@@ -666,10 +668,11 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
     __shared__ int next_chunk;
     if (threadIdx.x == 0) next_chunk = kDepWarps;
     if constexpr (F64)
-        tile_acc_init_f64<Accumulate>(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, (const double *)wx,
+        tile_acc_init_f64<Accumulate>(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, zs, zlim, (const double *)wx,
                                       (const double *)wy, (const double *)wz);
     else
-        tile_acc_init<Accumulate>(acc, N, x0, y0, z0, scale, (const float *)wx, (const float *)wy, (const float *)wz);
+        tile_acc_init<Accumulate>(acc, N, x0, y0, z0, zs, zlim, scale, (const float *)wx, (const float *)wy,
+                                  (const float *)wz);
     __syncthreads();
 
     const int nchunks = (int)((c1 - c0 + kPChunk - 1) / kPChunk);
@@ -952,10 +955,10 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
     if (lane == 0 && redo.tally) atomicAdd(redo.tally, (unsigned long long)nacc);
     __syncthreads();
     if constexpr (F64)
-        tile_epilogue_f64(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, (double *)wx, (double *)wy,
+        tile_epilogue_f64(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, zs, zlim, (double *)wx, (double *)wy,
                           (double *)wz);
     else
-        tile_epilogue(acc, N, x0, y0, z0, scale, (float *)wx, (float *)wy, (float *)wz);
+        tile_epilogue(acc, N, x0, y0, z0, zs, zlim, scale, (float *)wx, (float *)wy, (float *)wz);
 }
 
 // ------------------------------------------------------------------------------ host
@@ -1049,7 +1052,10 @@ int piece_raster(Ctx *c, CenterlineBatch &B, int *d_err)
 int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
 {
     const int N = c->p.N;
-    const int ntx = (N + TX - 1) / TX, nty = (N + TY - 1) / TY, ntz = (N + TZ - 1) / TZ;
+    const int ntx = (N + TX - 1) / TX, nty = (N + TY - 1) / TY;
+    // tiles of the context's planes: the whole grid, or its z-slab (whole tiles)
+    const int tz0 = c->slab_nz ? c->slab_z0 / TZ : 0;
+    const int ntz = c->slab_nz ? c->slab_nz / TZ : (N + TZ - 1) / TZ;
     const int64_t ntiles = (int64_t)ntx * nty * ntz;
     const int64_t nrec = B.npieces;
     if (nrec >= ((int64_t)1 << 26)) return fail(FWT_E_RANGE, "piece batch exceeds 2^26");
@@ -1060,7 +1066,7 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     FWT_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
     const unsigned bq = (unsigned)((nrec + 255) / 256);
     int km = kt_begin(c, KT_BINNING);
-    if (nrec > 0) pair_count_kernel<PieceRec><<<bq, 256, 0, c->stream>>>(B.piece, nrec, N, d_cnt, d_err);
+    if (nrec > 0) pair_count_kernel<PieceRec><<<bq, 256, 0, c->stream>>>(B.piece, nrec, N, tz0, ntz, d_cnt, d_err);
     FWT_TRY(scan_exclusive_i64(c, d_cnt, nrec, d_cnt + nrec, C.scratch[12]));
     kt_end(c, km);
     int64_t npairs = 0;
@@ -1079,7 +1085,8 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     FWT_CUDA(cudaMemsetAsync(d_tcnt, 0, tb * 2, c->stream));
     km = kt_begin(c, KT_BINNING);
     if (nrec > 0)
-        pair_emit_kernel<PieceRec><<<bq, 256, 0, c->stream>>>(B.piece, nrec, N, ntx, nty, d_cnt, d_key, d_val, d_tcnt);
+        pair_emit_kernel<PieceRec><<<bq, 256, 0, c->stream>>>(B.piece, nrec, N, ntx, nty, tz0, ntz, d_cnt, d_key, d_val,
+                                                                d_tcnt);
     u32_to_i64_kernel<<<(unsigned)((ntiles + 255) / 256), 256, 0, c->stream>>>(d_tcnt, ntiles, d_toff);
     FWT_TRY(scan_exclusive_i64(c, d_toff, ntiles, d_toff + ntiles, C.scratch[13]));
     FWT_TRY(buf_reserve(c, C.scratch[23], sizeof(uint32_t) * (size_t)(npairs + 8)));
@@ -1115,7 +1122,7 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
         FWT_CUDA(cudaFuncSetAttribute(deposit_piece_kernel<G, A, D, R>,                                    \
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPieceSmem));      \
         deposit_piece_kernel<G, A, D, R><<<(unsigned)ntiles, kDepThreads, kPieceSmem, c->stream>>>(       \
-            B.piece, N, ntx, nty, d_toff, d_list, scale, wx, wy, wz, d_err, rctx, B.ras_off, B.ras_pts);    \
+            B.piece, N, ntx, nty, tz0, d_toff, d_list, scale, wx, wy, wz, d_err, rctx, B.ras_off, B.ras_pts);    \
         FWT_CUDA(cudaGetLastError());                                                                      \
     } while (0)
 #define FWT_PIECE_LAUNCH_R(G, A, D)                                                                        \

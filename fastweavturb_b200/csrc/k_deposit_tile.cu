@@ -282,7 +282,7 @@ __device__ __forceinline__ bool rec_tests_wide(const SegRec &R, float d0x, float
 
 template <bool General, bool Accumulate, bool F64>
 __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
-    const SegRec *__restrict__ rec, int N, int ntx, int nty, const int64_t *__restrict__ tile_off,
+    const SegRec *__restrict__ rec, int N, int ntx, int nty, int tz0, const int64_t *__restrict__ tile_off,
     const uint32_t *__restrict__ list, double scale, void *__restrict__ wx, void *__restrict__ wy,
     void *__restrict__ wz, int *__restrict__ err, const RedoCtx redo)
 {
@@ -293,8 +293,10 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
     // a tile that no record of this batch meets keeps its values: earlier batches wrote them,
     // or the field was cleared before the first
     if (c0 == c1) return;
-    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tile / (ntx * nty);
+    const int tx = tile % ntx, ty = (tile / ntx) % nty, tz = tz0 + tile / (ntx * nty);
     const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
+    // the context's planes: the whole grid, or its z-slab
+    const int zs = redo.zs, zlim = redo.zs + redo.nz;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     WarpStage &S = reinterpret_cast<WarpStage *>(dsm + kAccBytes)[warp];
     if (lane == 0) mbar_init(&S.bar);
@@ -303,10 +305,11 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
     __shared__ int next_chunk;
     if (threadIdx.x == 0) next_chunk = kDepWarps;
     if constexpr (F64)
-        tile_acc_init_f64<Accumulate>(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, (const double *)wx,
+        tile_acc_init_f64<Accumulate>(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, zs, zlim, (const double *)wx,
                                       (const double *)wy, (const double *)wz);
     else
-        tile_acc_init<Accumulate>(acc, N, x0, y0, z0, scale, (const float *)wx, (const float *)wy, (const float *)wz);
+        tile_acc_init<Accumulate>(acc, N, x0, y0, z0, zs, zlim, scale, (const float *)wx, (const float *)wy,
+                                  (const float *)wz);
     __syncthreads();
 
     const int nchunks = (int)((c1 - c0 + kWarpChunk - 1) / kWarpChunk);
@@ -424,10 +427,10 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
     if (lane == 0 && redo.tally) atomicAdd(redo.tally, (unsigned long long)nacc);
     __syncthreads();
     if constexpr (F64)
-        tile_epilogue_f64(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, (double *)wx, (double *)wy,
+        tile_epilogue_f64(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, zs, zlim, (double *)wx, (double *)wy,
                           (double *)wz);
     else
-        tile_epilogue(acc, N, x0, y0, z0, scale, (float *)wx, (float *)wy, (float *)wz);
+        tile_epilogue(acc, N, x0, y0, z0, zs, zlim, scale, (float *)wx, (float *)wy, (float *)wz);
 }
 
 
@@ -451,6 +454,8 @@ RedoCtx redo_ctx(const Ctx *c, const CenterlineBatch &B, double scale, bool piec
     r.node_base = B.node_base;
     r.N = c->p.N;
     r.pieces = pieces ? 1 : 0;
+    r.zs = c->slab_nz ? c->slab_z0 : 0;
+    r.nz = c->slab_nz ? c->slab_nz : c->p.N;
     r.Rtube_ratio = c->p.Rtube_ratio;
     r.dzeta_sup = c->p.dzeta_sup;
     r.eta = c->p.eta_t;
@@ -475,7 +480,10 @@ double fixed_point_scale(const Ctx *c)
 int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
 {
     const int N = c->p.N;
-    const int ntx = (N + TX - 1) / TX, nty = (N + TY - 1) / TY, ntz = (N + TZ - 1) / TZ;
+    const int ntx = (N + TX - 1) / TX, nty = (N + TY - 1) / TY;
+    // tiles of the context's planes: the whole grid, or its z-slab (whole tiles)
+    const int tz0 = c->slab_nz ? c->slab_z0 / TZ : 0;
+    const int ntz = c->slab_nz ? c->slab_nz / TZ : (N + TZ - 1) / TZ;
     const int64_t ntiles = (int64_t)ntx * nty * ntz;
     if (B.nsub >= ((int64_t)1 << 26)) return fail(FWT_E_RANGE, "sub-segment batch exceeds 2^26");
     if (!B.rec) return fail(FWT_E_STATE, "tile deposition needs the FP32 sub-segment records");
@@ -488,7 +496,7 @@ int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     FWT_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
     const unsigned bq = (unsigned)((B.nsub + 255) / 256);
     int km = kt_begin(c, KT_BINNING);
-    if (B.nsub > 0) pair_count_kernel<SegRec><<<bq, 256, 0, c->stream>>>(B.rec, B.nsub, N, d_cnt, d_err);
+    if (B.nsub > 0) pair_count_kernel<SegRec><<<bq, 256, 0, c->stream>>>(B.rec, B.nsub, N, tz0, ntz, d_cnt, d_err);
     FWT_TRY(scan_exclusive_i64(c, d_cnt, B.nsub, d_cnt + B.nsub, C.scratch[12]));
     kt_end(c, km);
     int64_t npairs = 0;
@@ -507,7 +515,8 @@ int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     FWT_CUDA(cudaMemsetAsync(d_tcnt, 0, tb * 2, c->stream));
     km = kt_begin(c, KT_BINNING);
     if (B.nsub > 0)
-        pair_emit_kernel<SegRec><<<bq, 256, 0, c->stream>>>(B.rec, B.nsub, N, ntx, nty, d_cnt, d_key, d_val, d_tcnt);
+        pair_emit_kernel<SegRec><<<bq, 256, 0, c->stream>>>(B.rec, B.nsub, N, ntx, nty, tz0, ntz, d_cnt, d_key, d_val,
+                                                              d_tcnt);
     u32_to_i64_kernel<<<(unsigned)((ntiles + 255) / 256), 256, 0, c->stream>>>(d_tcnt, ntiles, d_toff);
     FWT_TRY(scan_exclusive_i64(c, d_toff, ntiles, d_toff + ntiles, C.scratch[13]));
     FWT_TRY(buf_reserve(c, C.scratch[23], sizeof(uint32_t) * (size_t)(npairs + 8)));
@@ -543,7 +552,7 @@ int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
         FWT_CUDA(cudaFuncSetAttribute(deposit_tile_kernel<G, A, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                       (int)kDepSmem));                                                    \
         deposit_tile_kernel<G, A, D><<<(unsigned)ntiles, kDepThreads, kDepSmem, c->stream>>>(             \
-            B.rec, N, ntx, nty, d_toff, d_list, scale, wx, wy, wz, d_err, rctx);                     \
+            B.rec, N, ntx, nty, tz0, d_toff, d_list, scale, wx, wy, wz, d_err, rctx);                     \
         FWT_CUDA(cudaGetLastError());                                                                     \
     } while (0)
     if (f64) {

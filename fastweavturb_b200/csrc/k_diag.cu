@@ -83,6 +83,7 @@ unsigned diag_grid(const Ctx *c, size_t n)
 
 int diag_vsf_deviation(Ctx *c, const void *d_phi, double *deviation)
 {
+    if (c->slab_nz) return fail(FWT_E_STATE, "VSF deviation: not available on a z-slab context");
     if (!c->have_w) return fail(FWT_E_STATE, "vsf_deviation: omega not built");
     const int N = c->p.N;
     const size_t n3 = field_elems(c);
@@ -119,6 +120,7 @@ int diag_vsf_deviation(Ctx *c, const void *d_phi, double *deviation)
 
 int diag_helicity(Ctx *c, double *helicity)
 {
+    if (c->slab_nz) return fail(FWT_E_STATE, "helicity: not available on a z-slab context");
     if (!c->have_u) return fail(FWT_E_STATE, "helicity: u not built");
     const int N = c->p.N;
     const size_t n3 = field_elems(c);

@@ -35,11 +35,14 @@ __device__ __forceinline__ void shell_add(double *sh, int nek, int s, double v, 
 }
 
 // mode = 0: Biot-Savart; mode = 1: low-pass filter (zero |k|^2 > kc2) and scale
+// The spectrum is a block of the half spectrum: all kz, the ky indices y0 .. y0 + ny - 1, all
+// kx, stored [kz][ky - y0][kx] (the whole half spectrum: y0 = 0, ny = N; one y-pencil of a grid
+// split over GPUs: its ky range).
 template <typename Real>
 __global__ void __launch_bounds__(256) biot_savart_kernel(typename Cplx<Real>::T *__restrict__ sx,
                                                           typename Cplx<Real>::T *__restrict__ sy,
-                                                          typename Cplx<Real>::T *__restrict__ sz, int N, int mode,
-                                                          double kc2, double *__restrict__ g_shw,
+                                                          typename Cplx<Real>::T *__restrict__ sz, int N, int y0,
+                                                          int ny, int mode, double kc2, double *__restrict__ g_shw,
                                                           double *__restrict__ g_shu, double *__restrict__ g_tot)
 {
     extern __shared__ double sh[];   // 2 * (nek + 1)
@@ -53,8 +56,8 @@ __global__ void __launch_bounds__(256) biot_savart_kernel(typename Cplx<Real>::T
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const Real inv = (Real)(1.0 / ((double)N * N * N));
     double tot_u = 0.0, tot_w = 0.0;
-    for (int64_t row = warp0; row < (int64_t)N * N; row += nwarps) {
-        const int jy = (int)(row % N), jz = (int)(row / N);
+    for (int64_t row = warp0; row < (int64_t)N * ny; row += nwarps) {
+        const int jy = y0 + (int)(row % ny), jz = (int)(row / ny);
         const int ky = (jy + N / 2) % N - N / 2, kz = (jz + N / 2) % N - N / 2;
         const Real kye = (jy == N / 2) ? (Real)0 : (Real)ky;
         const Real kze = (jz == N / 2) ? (Real)0 : (Real)kz;
@@ -183,12 +186,12 @@ static int launch_bs(Ctx *c, int mode, double kc2, double *d_shw, double *d_shu,
     const int km = kt_begin(c, KT_SPECTRAL);
     if (c->p.precision == 64) {
         cufftDoubleComplex *s = (cufftDoubleComplex *)c->b_spec.p;
-        biot_savart_kernel<double><<<blocks, 256, shb, c->stream>>>(s, s + nh, s + 2 * nh, N, mode, kc2, d_shw, d_shu,
-                                                                    d_tot);
+        biot_savart_kernel<double><<<blocks, 256, shb, c->stream>>>(s, s + nh, s + 2 * nh, N, 0, N, mode, kc2, d_shw,
+                                                                    d_shu, d_tot);
     } else {
         cufftComplex *s = (cufftComplex *)c->b_spec.p;
-        biot_savart_kernel<float><<<blocks, 256, shb, c->stream>>>(s, s + nh, s + 2 * nh, N, mode, kc2, d_shw, d_shu,
-                                                                   d_tot);
+        biot_savart_kernel<float><<<blocks, 256, shb, c->stream>>>(s, s + nh, s + 2 * nh, N, 0, N, mode, kc2, d_shw,
+                                                                   d_shu, d_tot);
     }
     kt_end(c, km);
     c->launches += 1;
@@ -198,6 +201,7 @@ static int launch_bs(Ctx *c, int mode, double kc2, double *d_shw, double *d_shu,
 
 int spectral_filter(Ctx *c, double k_c)
 {
+    if (c->slab_nz) return fail(FWT_E_STATE, "spectral filter: not available on a z-slab context");
     if (!c->have_w) return fail(FWT_E_STATE, "filter before deposition");
     FWT_TRY(spectral_init(c));
     FWT_TRY(spec_buffers(c));
@@ -210,6 +214,7 @@ int spectral_filter(Ctx *c, double k_c)
 
 int spectral_biot_savart(Ctx *c)
 {
+    if (c->slab_nz) return fail(FWT_E_STATE, "Biot-Savart: not available on a z-slab context");
     if (!c->have_w) return fail(FWT_E_STATE, "Biot-Savart before deposition");
     const int N = c->p.N;
     const int nek = N / 2;
@@ -233,6 +238,44 @@ int spectral_biot_savart(Ctx *c)
     c->have_u = true;
     c->normalised = false;
     c->umm_valid = false;
+    return 0;
+}
+
+// Biot-Savart on one y-pencil of the half spectrum (a grid split over GPUs): spec holds the
+// three components, each [N kz][ny ky][N/2 + 1 kx] from ky = y0, unscaled forward transforms
+// of omega; in place it becomes u^ as in spectral_biot_savart.  host_sums receives the pencil's
+// shell sums of 1/2 |w^|^2 and 1/2 |u^|^2 (shells 1..N/2) and its total energy and enstrophy
+// (2 (N/2 + 1) + 2 values: [0] and [N/2 + 1] unused), to be summed over the pencils.
+int spectral_block(Ctx *c, void *spec, int y0, int ny, double *host_sums)
+{
+    const int N = c->p.N;
+    const int nek = N / 2;
+    if (y0 < 0 || ny < 1 || y0 + ny > N) return fail(FWT_E_ARG, "biot_savart_block: ky range outside 0..N-1");
+    FWT_TRY(buf_reserve(c, c->scratch[11], sizeof(double) * (2 * (nek + 1) + 4)));
+    double *d_shw = (double *)c->scratch[11].p, *d_shu = d_shw + (nek + 1), *d_tot = d_shu + (nek + 1);
+    FWT_CUDA(cudaMemsetAsync(d_shw, 0, sizeof(double) * (2 * (nek + 1) + 4), c->stream));
+    const size_t nb = (size_t)N * ny * (N / 2 + 1);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+    const int64_t rows = (int64_t)N * ny;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((rows + 7) / 8, (int64_t)sms * 8));
+    const size_t shb = sizeof(double) * 2 * (N / 2 + 1);
+    const int km = kt_begin(c, KT_SPECTRAL);
+    if (c->p.precision == 64) {
+        cufftDoubleComplex *s = (cufftDoubleComplex *)spec;
+        biot_savart_kernel<double><<<blocks, 256, shb, c->stream>>>(s, s + nb, s + 2 * nb, N, y0, ny, 0, 0.0, d_shw,
+                                                                    d_shu, d_tot);
+    } else {
+        cufftComplex *s = (cufftComplex *)spec;
+        biot_savart_kernel<float><<<blocks, 256, shb, c->stream>>>(s, s + nb, s + 2 * nb, N, y0, ny, 0, 0.0, d_shw,
+                                                                   d_shu, d_tot);
+    }
+    kt_end(c, km);
+    c->launches += 1;
+    FWT_CUDA(cudaGetLastError());
+    FWT_CUDA(cudaMemcpyAsync(host_sums, d_shw, sizeof(double) * (2 * (nek + 1) + 2), cudaMemcpyDeviceToHost,
+                             c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
 }
 

@@ -88,9 +88,12 @@ __host__ __device__ constexpr int sp_lines(int N)
     return N < (sizeof(Real) == 8 ? 16 : 32) ? N : (sizeof(Real) == 8 ? 16 : 32);
 }
 
+// The field is a box n0 x n1 x n2 (x fastest) whose extent along `axis` is the line length N:
+// the whole grid, or a z-slab (axes 0, 1) or y-pencil (axis 2) of a grid split over GPUs.
 template <typename Real, int PMAX, int MPW>
-__global__ void __launch_bounds__(256) sp_kernel(const Real *__restrict__ u, int N, int axis, double s,
-                                                 const int *__restrict__ rs, int nr, double *__restrict__ Sp)
+__global__ void __launch_bounds__(256) sp_kernel(const Real *__restrict__ u, int N, int n0, int n1, int n2, int axis,
+                                                 double s, const int *__restrict__ rs, int nr,
+                                                 double *__restrict__ Sp)
 {
     extern __shared__ __align__(16) unsigned char sp_smem[];
     Real *tile = reinterpret_cast<Real *>(sp_smem);   // N x (W + 1)
@@ -108,30 +111,31 @@ __global__ void __launch_bounds__(256) sp_kernel(const Real *__restrict__ u, int
         const int m = warp + a * nwarps;
         rr[a] = m < nr ? rs[m] % N : -1;
     }
-    // axis 0: groups of W consecutive x-rows (row = y + N z); axes 1, 2: groups of W
+    // axis 0: groups of W consecutive x-rows (row = y + n1 z); axes 1, 2: groups of W
     // consecutive x at fixed z (axis 1) or fixed y (axis 2)
-    const int xgroups = (N + W - 1) / W;
-    const int64_t ngroups = axis == 0 ? ((int64_t)N * N + W - 1) / W : (int64_t)xgroups * N;
+    const int xgroups = (n0 + W - 1) / W;
+    const int64_t nrows = (int64_t)n1 * n2;
+    const int64_t ngroups = axis == 0 ? (nrows + W - 1) / W : (int64_t)xgroups * (axis == 1 ? n2 : n1);
     for (int64_t g = blockIdx.x; g < ngroups; g += gridDim.x) {
         __syncthreads();
         int nl;   // lines of this group
         if (axis == 0) {
             const int64_t row0 = g * W;
-            nl = (int)min((int64_t)W, (int64_t)N * N - row0);
+            nl = (int)min((int64_t)W, nrows - row0);
             for (int e = threadIdx.x; e < N * nl; e += blockDim.x) {
                 const int x = e % N, l = e / N;
-                tile[x * ld + l] = u[(size_t)(row0 + l) * N + x];
+                tile[x * ld + l] = u[(size_t)(row0 + l) * n0 + x];
             }
         } else {
             const int xg = (int)(g % xgroups), o = (int)(g / xgroups);
             const int x0 = xg * W;
-            nl = min(W, N - x0);
+            nl = min(W, n0 - x0);
             for (int e = threadIdx.x; e < N * W; e += blockDim.x) {
                 const int l = e % W, pos = e / W;
                 if (l >= nl) continue;
                 size_t gi;
-                if (axis == 1) gi = (size_t)(x0 + l) + (size_t)N * ((size_t)pos + (size_t)N * o);
-                else gi = (size_t)(x0 + l) + (size_t)N * ((size_t)o + (size_t)N * pos);
+                if (axis == 1) gi = (size_t)(x0 + l) + (size_t)n0 * ((size_t)pos + (size_t)n1 * o);
+                else gi = (size_t)(x0 + l) + (size_t)n0 * ((size_t)o + (size_t)n1 * pos);
                 tile[pos * ld + l] = u[gi];
             }
         }
@@ -237,6 +241,7 @@ int stats_minmax(Ctx *c, int which)
 
 int stats_normalise(Ctx *c)
 {
+    if (c->slab_nz) return fail(FWT_E_STATE, "normalise: not available on a z-slab context");
     if (!c->have_u) return fail(FWT_E_STATE, "normalise before Biot-Savart");
     // Etot = sum u.u dv / 2 / (2pi)^3 = 1/2 <u^2>; up = sqrt(2 Etot / 3) (tube.f90:1028-1030)
     c->Etot = c->Etot_raw;
@@ -265,6 +270,7 @@ static void pdf_layout(float vmin, float vmax, int nbins, std::vector<float> &va
 
 int stats_pdf(Ctx *c, int which, int comp, int nbins, float *val, float *pdf, uint64_t *counts)
 {
+    if (c->slab_nz) return fail(FWT_E_STATE, "pdf: not available on a z-slab context");
     if (which != 0 && which != 1) return fail(FWT_E_ARG, "pdf: which must be 0 (u) or 1 (omega)");
     if (comp < -1 || comp > 2) return fail(FWT_E_ARG, "pdf: component must be -1..2");
     if (nbins < 1 || nbins > 8192) return fail(FWT_E_ARG, "pdf: nbins must be 1..8192");
@@ -338,6 +344,7 @@ int stats_pdf(Ctx *c, int which, int comp, int nbins, float *val, float *pdf, ui
 
 int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp)
 {
+    if (c->slab_nz) return fail(FWT_E_STATE, "S_p: not available on a z-slab context");
     if (!c->normalised) return fail(FWT_E_STATE, "structure functions before normalisation");
     if (pmax < 1 || pmax > 10) return fail(FWT_E_ARG, "Sp: pmax must be 1..10");
     if (nr < 1 || nr > 64) return fail(FWT_E_ARG, "Sp: nr must be 1..64");
@@ -371,7 +378,7 @@ int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp)
         auto k = sp_kernel<REAL, 10, MPW>;                                                                       \
         FWT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));                  \
         for (int ax = 0; ax < 3; ++ax)                                                                           \
-            k<<<blocks, 256, shb, c->stream>>>((const REAL *)c->b_u.p + ax * n3, N, ax, s, d_r, nr, d_sp);        \
+            k<<<blocks, 256, shb, c->stream>>>((const REAL *)c->b_u.p + ax * n3, N, N, N, N, ax, s, d_r, nr, d_sp); \
     } while (0)
     if (c->p.precision == 64) {
         if (mpw <= 1) FWT_SP(double, 1); else if (mpw <= 2) FWT_SP(double, 2); else if (mpw <= 4) FWT_SP(double, 4);
@@ -395,6 +402,7 @@ int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp)
 
 int stats_field_wh(Ctx *c, float *host_out)
 {
+    if (c->slab_nz) return fail(FWT_E_STATE, "field output: not available on a z-slab context");
     if (!c->normalised) return fail(FWT_E_STATE, "field output before normalisation");
     const int N = c->p.N, nd = c->p.N_downsample;
     if (nd < 1 || N % nd) return fail(FWT_E_ARG, "N_downsample must divide N");
@@ -442,6 +450,59 @@ int stats_copy_field(Ctx *c, int which, int comp, double *host)
         FWT_CUDA(cudaStreamSynchronize(c->stream));
         for (size_t i = 0; i < n3; ++i) host[i] = (double)tmp[i] * s;
     }
+    return 0;
+}
+
+// S_p sums of one velocity component on a box (a z-slab or y-pencil of a grid split over GPUs):
+// sums[p * nr + m] = sum over the box's lines along `axis` of (du s)^(p+1), du the increment at
+// separation r[m]; the line axis must span the grid (extent N).  Not normalised: the caller adds
+// the three components' sums over all boxes and divides by 3 N^3, as stats_sp does.
+int stats_sp_block(Ctx *c, const void *u, int n0, int n1, int n2, int axis, double s, const int *r, int nr,
+                   double *sums)
+{
+    const int N = c->p.N;
+    if (axis < 0 || axis > 2) return fail(FWT_E_ARG, "sp_block: axis must be 0..2");
+    const int ext[3] = {n0, n1, n2};
+    if (ext[axis] != N || n0 < 1 || n1 < 1 || n2 < 1) return fail(FWT_E_ARG, "sp_block: the line axis must span N");
+    if (nr < 1 || nr > 64) return fail(FWT_E_ARG, "sp_block: nr must be 1..64");
+    for (int m = 0; m < nr; ++m)
+        if (r[m] < 0) return fail(FWT_E_ARG, "sp_block: negative separation");
+    const bool f64 = c->p.precision == 64;
+    const int W = f64 ? sp_lines<double>(N) : sp_lines<float>(N);
+    FWT_TRY(buf_reserve(c, c->scratch[9], sizeof(int) * 64 + sizeof(double) * 10 * 64 + 64));
+    int *d_r = (int *)c->scratch[9].p;
+    double *d_sp = (double *)((char *)c->scratch[9].p + 256);
+    FWT_CUDA(cudaMemcpyAsync(d_r, r, sizeof(int) * nr, cudaMemcpyHostToDevice, c->stream));
+    FWT_CUDA(cudaMemsetAsync(d_sp, 0, sizeof(double) * 10 * nr, c->stream));
+    const size_t shb = (f64 ? sizeof(double) : sizeof(float)) * (size_t)N * (W + 1);
+    int optin = 0;
+    FWT_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
+    if (shb > (size_t)optin) return fail(FWT_E_RANGE, "sp_block: N too large for one block's shared memory");
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)n0 * n1 * n2 / N / W + 1,
+                                                                             (int64_t)sms * 4));
+    const int mpw = (nr + 7) / 8;
+    const int km = kt_begin(c, KT_STATS);
+#define FWT_SPB(REAL, MPW)                                                                                       \
+    do {                                                                                                         \
+        auto k = sp_kernel<REAL, 10, MPW>;                                                                       \
+        FWT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));                  \
+        k<<<blocks, 256, shb, c->stream>>>((const REAL *)u, N, n0, n1, n2, axis, s, d_r, nr, d_sp);              \
+    } while (0)
+    if (f64) {
+        if (mpw <= 1) FWT_SPB(double, 1); else if (mpw <= 2) FWT_SPB(double, 2); else if (mpw <= 4) FWT_SPB(double, 4);
+        else FWT_SPB(double, 8);
+    } else {
+        if (mpw <= 1) FWT_SPB(float, 1); else if (mpw <= 2) FWT_SPB(float, 2); else if (mpw <= 4) FWT_SPB(float, 4);
+        else FWT_SPB(float, 8);
+    }
+#undef FWT_SPB
+    kt_end(c, km);
+    c->launches += 1;
+    FWT_CUDA(cudaGetLastError());
+    FWT_CUDA(cudaMemcpyAsync(sums, d_sp, sizeof(double) * 10 * nr, cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
 }
 

@@ -67,8 +67,8 @@ __device__ __forceinline__ void agg_inc(uint32_t *cnt, uint32_t key, bool active
 // Binning, step 1: number of (tile, image) pairs of every record (for_each_tile is overloaded
 // per record type).  Boxes wider than one period beyond the domain set err bit 1.
 template <typename Rec>
-__global__ void pair_count_kernel(const Rec *__restrict__ seg, int64_t nsub, int N, int64_t *__restrict__ cnt,
-                                  int *__restrict__ err)
+__global__ void pair_count_kernel(const Rec *__restrict__ seg, int64_t nsub, int N, int tz0, int ntz,
+                                  int64_t *__restrict__ cnt, int *__restrict__ err)
 {
     const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nsub) return;
@@ -79,7 +79,10 @@ __global__ void pair_count_kernel(const Rec *__restrict__ seg, int64_t nsub, int
         const int glo = S.box_lo[d] - 1, ghi = S.box_hi[d] - 1;
         if (floordiv(glo, N) < -1 || floordiv(ghi, N) > 1 || ghi < glo) atomicOr(err, 1);
     }
-    for_each_tile(S, N, [&](int, int, int, uint32_t) { ++c; });
+    // tiles of the context's z-slab only (tz0 .. tz0 + ntz - 1; the whole grid by default)
+    for_each_tile(S, N, [&](int, int, int tz, uint32_t) {
+        if (tz >= tz0 && tz < tz0 + ntz) ++c;
+    });
     cnt[q] = c;
 }
 
@@ -90,7 +93,7 @@ constexpr uint32_t kNoTile = 0xffffffffu;   // key of a pair slot that the emitt
 // inside the record's slots [off[q], off[q+1]) reserved by step 1 and marks any slot it leaves
 // empty, so the sort stays in bounds even if the two passes ever decided a tile differently.
 template <typename Rec>
-__global__ void pair_emit_kernel(const Rec *__restrict__ seg, int64_t nsub, int N, int ntx, int nty,
+__global__ void pair_emit_kernel(const Rec *__restrict__ seg, int64_t nsub, int N, int ntx, int nty, int tz0, int ntz,
                                  const int64_t *__restrict__ off, uint32_t *__restrict__ key,
                                  uint32_t *__restrict__ val, uint32_t *__restrict__ tile_cnt)
 {
@@ -104,8 +107,8 @@ __global__ void pair_emit_kernel(const Rec *__restrict__ seg, int64_t nsub, int 
     uint32_t k0 = 0;
     if (live)
         for_each_tile(S, N, [&](int tx, int ty, int tz, uint32_t img) {
-            if (o >= end) return;
-            const uint32_t tile = (uint32_t)(tx + ntx * (ty + nty * tz));
+            if (o >= end || tz < tz0 || tz >= tz0 + ntz) return;
+            const uint32_t tile = (uint32_t)(tx + ntx * (ty + nty * (tz - tz0)));
             key[o] = tile;
             val[o] = (uint32_t)q | (img << 26);
             ++o;
@@ -161,17 +164,19 @@ __device__ __forceinline__ void bulk_g2s(void *smem, const void *gmem, uint32_t 
 }
 
 // Load the tile's current values into the fixed-point cells (Accumulate) or zero them.
+// The field holds planes zs .. zlim - 1 (the whole grid: zs = 0, zlim = N; a z-slab context:
+// its slab), plane gz stored at gz - zs.
 template <bool Accumulate>
-__device__ __forceinline__ void tile_acc_init(long long (*acc)[kAccN], int N, int x0, int y0, int z0, double scale,
-                                              const float *__restrict__ wx, const float *__restrict__ wy,
-                                              const float *__restrict__ wz)
+__device__ __forceinline__ void tile_acc_init(long long (*acc)[kAccN], int N, int x0, int y0, int z0, int zs,
+                                              int zlim, double scale, const float *__restrict__ wx,
+                                              const float *__restrict__ wy, const float *__restrict__ wz)
 {
     for (int p = threadIdx.x; p < TP; p += blockDim.x) {
         const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
         const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
         long long a0 = 0, a1 = 0, a2 = 0;
-        if (Accumulate && gx < N && gy < N && gz < N) {
-            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
+        if (Accumulate && gx < N && gy < N && gz < zlim) {
+            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * (gz - zs));
             a0 = __double2ll_rn((double)wx[g] * scale);
             a1 = __double2ll_rn((double)wy[g] * scale);
             a2 = __double2ll_rn((double)wz[g] * scale);
@@ -184,17 +189,18 @@ __device__ __forceinline__ void tile_acc_init(long long (*acc)[kAccN], int N, in
 }
 
 // Fixed point -> float, coalesced float4 stores of the tile.
-__device__ __forceinline__ void tile_epilogue(long long (*acc)[kAccN], int N, int x0, int y0, int z0, double scale,
-                                              float *__restrict__ wx, float *__restrict__ wy, float *__restrict__ wz)
+__device__ __forceinline__ void tile_epilogue(long long (*acc)[kAccN], int N, int x0, int y0, int z0, int zs, int zlim,
+                                              double scale, float *__restrict__ wx, float *__restrict__ wy,
+                                              float *__restrict__ wz)
 {
     const int tid = threadIdx.x;
     const double inv = 1.0 / scale;
-    const bool full = (x0 + TX <= N) && (y0 + TY <= N) && (z0 + TZ <= N);
+    const bool full = (x0 + TX <= N) && (y0 + TY <= N) && (z0 + TZ <= zlim);
     if (full) {
         for (int q4 = tid; q4 < TP / 4; q4 += blockDim.x) {
             const int p = 4 * q4;
             const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
-            const size_t g = (size_t)(x0 + lx) + (size_t)N * ((size_t)(y0 + ly) + (size_t)N * (z0 + lz));
+            const size_t g = (size_t)(x0 + lx) + (size_t)N * ((size_t)(y0 + ly) + (size_t)N * (z0 + lz - zs));
             const int pa = lx + kSY * ly + kSZ * lz;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
@@ -211,8 +217,8 @@ __device__ __forceinline__ void tile_epilogue(long long (*acc)[kAccN], int N, in
         for (int p = tid; p < TP; p += blockDim.x) {
             const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
             const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
-            if (gx >= N || gy >= N || gz >= N) continue;
-            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
+            if (gx >= N || gy >= N || gz >= zlim) continue;
+            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * (gz - zs));
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 const float v1 = (float)((double)acc[d][lx + kSY * ly + kSZ * lz] * inv);
@@ -225,7 +231,7 @@ __device__ __forceinline__ void tile_epilogue(long long (*acc)[kAccN], int N, in
 
 // FP64 tile cells (the FP64 tile path): load the tile's current values or zero them.
 template <bool Accumulate>
-__device__ __forceinline__ void tile_acc_init_f64(double (*acc)[kAccN], int N, int x0, int y0, int z0,
+__device__ __forceinline__ void tile_acc_init_f64(double (*acc)[kAccN], int N, int x0, int y0, int z0, int zs, int zlim,
                                                   const double *__restrict__ wx, const double *__restrict__ wy,
                                                   const double *__restrict__ wz)
 {
@@ -233,8 +239,8 @@ __device__ __forceinline__ void tile_acc_init_f64(double (*acc)[kAccN], int N, i
         const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
         const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        if (Accumulate && gx < N && gy < N && gz < N) {
-            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
+        if (Accumulate && gx < N && gy < N && gz < zlim) {
+            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * (gz - zs));
             a0 = wx[g];
             a1 = wy[g];
             a2 = wz[g];
@@ -247,17 +253,17 @@ __device__ __forceinline__ void tile_acc_init_f64(double (*acc)[kAccN], int N, i
 }
 
 // FP64 tile store (coalesced double2 stores).
-__device__ __forceinline__ void tile_epilogue_f64(double (*acc)[kAccN], int N, int x0, int y0, int z0,
+__device__ __forceinline__ void tile_epilogue_f64(double (*acc)[kAccN], int N, int x0, int y0, int z0, int zs, int zlim,
                                                   double *__restrict__ wx, double *__restrict__ wy,
                                                   double *__restrict__ wz)
 {
     const int tid = threadIdx.x;
-    const bool full = (x0 + TX <= N) && (y0 + TY <= N) && (z0 + TZ <= N);
+    const bool full = (x0 + TX <= N) && (y0 + TY <= N) && (z0 + TZ <= zlim);
     if (full) {
         for (int q2 = tid; q2 < TP / 2; q2 += blockDim.x) {
             const int p = 2 * q2;
             const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
-            const size_t g = (size_t)(x0 + lx) + (size_t)N * ((size_t)(y0 + ly) + (size_t)N * (z0 + lz));
+            const size_t g = (size_t)(x0 + lx) + (size_t)N * ((size_t)(y0 + ly) + (size_t)N * (z0 + lz - zs));
             const int pa = lx + kSY * ly + kSZ * lz;
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
@@ -272,8 +278,8 @@ __device__ __forceinline__ void tile_epilogue_f64(double (*acc)[kAccN], int N, i
         for (int p = tid; p < TP; p += blockDim.x) {
             const int lx = p % TX, ly = (p / TX) % TY, lz = p / (TX * TY);
             const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
-            if (gx >= N || gy >= N || gz >= N) continue;
-            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * gz);
+            if (gx >= N || gy >= N || gz >= zlim) continue;
+            const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * (gz - zs));
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 const double v1 = acc[d][lx + kSY * ly + kSZ * lz];

@@ -149,6 +149,30 @@ int fwt_vsf_deviation(fwt_ctx *ctx, const void *d_phi, double *deviation);
  * at tube.f90:1027): sum of omega . u times the cell volume (2 pi / N)^3, of the normalised
  * fields after fwt_normalize, of the raw fields before. */
 int fwt_helicity(fwt_ctx *ctx, double *helicity);
+/* Restrict the context to the z-slab of planes z0 .. z0 + nz - 1 (0-based; z0 and nz multiples
+ * of 8; z0 = nz = 0 restores the whole grid): the fields become N x N x nz (column-major, plane
+ * z0 first) and fwt_deposit deposits every line's contribution to those planes only -- the
+ * reference's z-slab ownership (tube.f90:261-265, 800-804), for a grid split over GPUs.  Needs
+ * deposit_mode 0.  The spectral and statistics entry points refuse a slab context
+ * (FWT_E_STATE): the distributed driver does them across the slabs (fwt_biot_savart_block,
+ * fwt_sp_block).  Clears the context's fields. */
+int fwt_set_slab(fwt_ctx *ctx, int z0, int nz);
+/* The Biot-Savart pass of fwt_biot_savart on one y-pencil of the half spectrum, for a grid split
+ * over GPUs (the pencil transposes of the reference's fourier_forward/backward,
+ * subroutine.f90:938-968, are the caller's): spec (device, the context's precision) holds three
+ * components, each [N kz][ny ky][N/2 + 1 kx] for ky = y0 .. y0 + ny - 1, the unscaled forward
+ * transforms of omega; in place they become u^ = i k x w^ / |k|^2 scaled by 1/N^3.  sums
+ * (host, 2 (N/2 + 1) + 2 doubles) receives this pencil's shell sums of 1/2 |w^|^2 at
+ * [1 .. N/2], of 1/2 |u^|^2 at [N/2 + 2 .. N + 1], and its energy and enstrophy at [N + 2],
+ * [N + 3]; the caller adds them over the pencils. */
+int fwt_biot_savart_block(fwt_ctx *ctx, void *spec, int y0, int ny, double *sums);
+/* Structure-function sums of one velocity component on a device box n0 x n1 x n2 (x fastest,
+ * the context's precision) along `axis`, whose extent must be N (a z-slab for axes 0 and 1, a
+ * y-pencil for axis 2): sums[p * nr + m] = sum over the box's lines of (du scale)^(p + 1),
+ * p = 0..9, du the increment at separation r[m] (Sp_calculate's sums, subroutine.f90:64-129,
+ * before the division by 3 N^3). */
+int fwt_sp_block(fwt_ctx *ctx, const void *u, int n0, int n1, int n2, int axis, double scale, const int *r, int nr,
+                 double *sums);
 /* Isosurface of |omega| on the field_wh data box, coloured by the helicity omega . u: the
  * compute part of the reference's rendering script (output/field_wh_norm.py:56-89), whose
  * rendering needs a graphics stack and is not reproduced.  The box is n_d^3 points of the
