@@ -72,3 +72,24 @@ def test_reference_arm_other_ranks_exit_without_work():
                         "--steps", "1", "--warmup", "0"], env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0
     assert r.stdout.strip() == ""
+
+
+def test_reference_arm_estimate_tracks_a_whole_oracle_run(orc):
+    """The reference arm times a bounded sample (the first tube of every level on a reduced grid,
+    the spectral path and statistics on at most 256^3) and scales it to a whole field.  On cfg0,
+    small enough to run whole, the estimate lands within a factor 2 of the measured whole run."""
+    import time
+
+    sys.path.insert(0, ROOT)
+    import bench
+    from fastweavturb_b200.configs import cfg0
+    from helpers import oracle_inputs
+
+    w = cfg0(seed=0)
+    est, parts = bench.cpu_sample_estimate(w)
+    p, cl = oracle_inputs(orc, w)
+    t = time.perf_counter()
+    orc.run(p, cl)
+    whole = time.perf_counter() - t
+    assert 0.5 * whole <= est <= 2.0 * whole, (est, whole)
+    assert "grids [64, 64, 64]" in parts["sample"]
