@@ -431,8 +431,12 @@ def main():
         err = {"omega_rel_l2": rel_l2_device(w32, ctx64.field_tensor(0), torch),
                "u_rel_l2": rel_l2_device(u32, ctx64.field_tensor(1), torch),
                "Ek_omega_rel_l2": rel_l2(ew32, ew64), "Ek_u_rel_l2": rel_l2(eu32, eu64)}
+        # S_p per entry, relative to the larger of the entry and the natural size (max S_2)^(p/2):
+        # odd orders pass through zero
+        s2max = float(np.max(np.abs(sp64[1])))
         for q in range(1, 6):
-            err[f"S{q + 1}_rel"] = float(np.max(np.abs(sp32[q] - sp64[q]) / np.abs(sp64[q])))
+            den = np.maximum(np.abs(sp64[q]), s2max ** ((q + 1) / 2.0))
+            err[f"S{q + 1}_rel"] = float(np.max(np.abs(sp32[q] - sp64[q]) / den))
         v64 = whole_job_rate(1, args.fp64_steps, w.N, ms64)
         fp64 = {"value": v64, "unit": "Mpts/s", "steps": args.fp64_steps, "ms_per_step": ms64 / args.fp64_steps,
                 "path": "FP64 tile path (FP32 candidate tests, the reference's FP64 tests and arithmetic)",

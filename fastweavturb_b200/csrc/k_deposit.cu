@@ -64,10 +64,12 @@ __global__ void __launch_bounds__(256) deposit_walk_kernel(const SubSeg *__restr
                 const int64_t r = idx / nx;
                 const int jj = (int)(r % ny), kk = (int)(r / ny);
                 float o[3], cond;
-                if (!point_f32<General>(G, ii, jj, kk, o, cond)) continue;
+                const int pass = point_f32<General>(G, ii, jj, kk, o, cond);
+                if (pass == 0) continue;
                 const int ip = S.box_lo[0] + ii, jp = S.box_lo[1] + jj, kp = S.box_lo[2] + kk;
-                if (General && !(cond <= kRedoCond)) {
-                    // ill-conditioned curved-branch point: the reference's FP64 arithmetic
+                if (pass == 2 || (General && !(cond <= kRedoCond))) {
+                    // a plane test within its rounding bound, or an ill-conditioned
+                    // curved-branch point: the reference's FP64 tests and arithmetic
                     double o64[3];
                     if (!point_ref_f64(S, P, coe + 18 * (size_t)S.slot, dt, dzeta_sup, eta, dev_pi2() / N, ip, jp, kp,
                                        o64))

@@ -216,11 +216,15 @@ __device__ __forceinline__ void redo_locate(const RedoCtx &R, uint32_t rec, int 
 }
 
 // The reference's FP64 vorticity of the pair (grid point g = wrapped 0-based indices,
-// record rec, chord ch), as a fixed-point contribution.  The tile kernel already accepted the
-// pair; the grid point's image inside the sub-segment's box is the one the reference visits.
-static __device__ __noinline__ bool redo_pair_f64(const RedoCtx &R, uint32_t rec, int ch, int gx, int gy, int gz,
-                                                  long long q[3])
+// record rec, chord ch), as a fixed-point contribution; the grid point's image inside the
+// sub-segment's box (narrower than one period) is the one the reference visits.  decide =
+// false: the FP32 tests accepted the pair.  decide = true: an FP32 plane test fell within its
+// rounding bound of zero, and the reference's FP64 tests (tube.f90:806-818) decide; a rejected
+// pair contributes nothing.  Returns 1 (accepted), 0 (rejected) or -1 (fixed-point overflow).
+static __device__ __noinline__ int redo_pair_f64(const RedoCtx &R, uint32_t rec, int ch, bool decide, int gx, int gy,
+                                                 int gz, long long q[3])
 {
+    q[0] = q[1] = q[2] = 0;
     int slot, j;
     redo_locate(R, rec, ch, slot, j);
     SubSeg S;
@@ -236,7 +240,8 @@ static __device__ __noinline__ bool redo_pair_f64(const RedoCtx &R, uint32_t rec
     }
     double m[3], t0, t1, v[3];
     ref_mesh_f64(dev_pi2() / R.N, ix[0], ix[1], ix[2], m);
-    ref_tests_f64(S, m, t0, t1);
+    const bool pass = ref_tests_f64(S, m, t0, t1);
+    if (decide && !pass) return 0;
     ref_value_f64(S, P, R.coe + 18 * (size_t)slot, R.dtf[slot], R.dzeta_sup, R.eta, m, t0, t1, v);
     bool ok = true;
 #pragma unroll
@@ -246,7 +251,21 @@ static __device__ __noinline__ bool redo_pair_f64(const RedoCtx &R, uint32_t rec
         q[k] = in ? __double2ll_rn(sv) : 0;
         ok = ok && in;
     }
-    return ok;
+    return ok ? 1 : -1;
+}
+
+// Bound of the FP32 rounding of a plane test (x - p) . n evaluated from a record's local
+// offsets d = off + i dx (i along the box, box extents ext grid points) with the offset dci
+// between the record's two plane points: every rounding (off, dx, d, n, the three products and
+// sums) is at most 2^-24 of a term bounded by E = sum_k max|d_k| + |dci_k|, about ten of them;
+// 2e-6 E keeps a factor of three.  Beyond it the FP32 sign is the FP64 sign.
+__device__ __forceinline__ float plane_eps(const float off[3], const int ext[3], float dx, const float dci[3])
+{
+    float E = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        E += fmaxf(fabsf(off[k]), fabsf(fmaf((float)ext[k], dx, off[k]))) + fabsf(dci[k]);
+    return 2.0e-6f * E + 1.0e-30f;
 }
 
 // Curved-branch amplification |1/(1 - kappa rho cos theta)| (tube.f90:876-879) above which an
@@ -261,6 +280,7 @@ struct SegF {
     float g;          // W = t0 * g is the spline argument measured from the start, times Len
     float b[3][5];    // c(z0 + W) - c(z0) = sum_k b[k-1] W^k
     float R2, Rt;
+    float pe;         // rounding bound of the plane tests (plane_eps)
     float smin, A, ph0, om, q;   // sigma = smin + A (sin(ph0 + om W) + 1); dsigma/dzeta = q cos(.)
     float Gamma, Linv, eta;
     // periodic bookkeeping of the reference's two single wraps (coo_curve_spline_5th wraps
@@ -311,6 +331,8 @@ __device__ __forceinline__ void seg_setup_f32(const SubSeg &S, const LineParam &
     }
     G.R2 = (float)(S.Rt * S.Rt);
     G.Rt = (float)S.Rt;
+    const int ext[3] = {S.box_hi[0] - i0, S.box_hi[1] - j0, S.box_hi[2] - k0};
+    G.pe = plane_eps(G.off, ext, G.dx, G.dci);
     // core size sigma(zeta) = smin + A (sin(omega zeta) + 1), zeta = s0 + W/Len
     const double omega = floor(P.length / dev_pi() + 0.5) * (double)P.n_T;
     const double A = (P.sigma_max - P.sigma_min) / 2.0;
@@ -337,21 +359,23 @@ __device__ __forceinline__ void seg_setup_f32(const SubSeg &S, const LineParam &
 // Contribution of sub-segment G at grid offset (ii, jj, kk) from G's origin index
 // (tube.f90:806-892 in the local frame).  General=false is the exact specialisation for a
 // constant core (sigma_ratio = 1) and no twist (eta = 0), where the reference's vorticity
-// reduces to tp * Gamma * T.
+// reduces to tp * Gamma * T.  Returns 0 (rejected), 1 (accepted, out holds the contribution)
+// or 2: a plane test within its rounding bound G.pe of zero, left to the FP64 tests.
 template <bool General>
-__device__ __forceinline__ bool point_f32(const SegF &G, int ii, int jj, int kk, float out[3], float &cond)
+__device__ __forceinline__ int point_f32(const SegF &G, int ii, int jj, int kk, float out[3], float &cond)
 {
     cond = 1.0f;
     const float d0x = fmaf((float)ii, G.dx, G.off[0]);
     const float d0y = fmaf((float)jj, G.dx, G.off[1]);
     const float d0z = fmaf((float)kk, G.dx, G.off[2]);
     const float t0 = d0x * G.tc0[0] + d0y * G.tc0[1] + d0z * G.tc0[2];
-    if (!(t0 >= 0.0f)) return false;
+    if (!(t0 >= -G.pe)) return 0;
     const float ex = d0x - G.dci[0], ey = d0y - G.dci[1], ez = d0z - G.dci[2];
     const float t1 = ex * G.tc1[0] + ey * G.tc1[1] + ez * G.tc1[2];
-    if (!(t1 < 0.0f)) return false;
+    if (!(t1 < G.pe)) return 0;
     const float r2 = d0x * d0x + d0y * d0y + d0z * d0z - t0 * t0;
-    if (!(r2 < G.R2)) return false;
+    if (!(r2 < G.R2)) return 0;
+    if (!(t0 >= G.pe) || !(t1 < -G.pe)) return 2;
     const float W = t0 * G.g;
     float P[3], c1[3];
 #pragma unroll
@@ -381,7 +405,7 @@ __device__ __forceinline__ bool point_f32(const SegF &G, int ii, int jj, int kk,
         out[0] = tp * T[0];
         out[1] = tp * T[1];
         out[2] = tp * T[2];
-        return true;
+        return 1;
     } else {
         float c2[3];
 #pragma unroll
@@ -422,7 +446,7 @@ __device__ __forceinline__ bool point_f32(const SegF &G, int ii, int jj, int kk,
             for (int d = 0; d < 3; ++d)
                 out[d] = tp * (T[d] + G.eta * (t5 * Nv[d] + t6 * B[d]) + (t7 * Nv[d] + t8 * B[d]));
         }
-        return true;
+        return 1;
     }
 }
 
@@ -500,36 +524,6 @@ __device__ __forceinline__ void segrec_from(const SegF &G, const SubSeg &S, SegR
     if (nowrap) R.kq[0] = kNoWrap;
 }
 
-// SegF of record R with its origin moved by (di, dj, dk) grid points from box_lo
-__device__ __forceinline__ void segf_from(const SegRec &R, int di, int dj, int dk, SegF &G)
-{
-    const int dd[3] = {di, dj, dk};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        G.off[d] = fmaf((float)dd[d], R.dx, R.off[d]);
-        G.tc0[d] = R.tc0[d];
-        G.tc1[d] = R.tc1[d];
-        G.dci[d] = R.dci[d];
-        G.thi[d] = R.thi[d];
-        G.tlo[d] = R.tlo[d];
-        G.kq[d] = R.kq[d];
-#pragma unroll
-        for (int k = 0; k < 5; ++k) G.b[d][k] = R.b[5 * d + k];
-    }
-    G.dx = R.dx;
-    G.g = R.g;
-    G.R2 = R.R2;
-    G.Rt = sqrtf(R.R2);
-    G.smin = R.smin;
-    G.A = R.A;
-    G.ph0 = R.ph0;
-    G.om = R.om;
-    G.q = R.q;
-    G.Gamma = R.Gamma;
-    G.Linv = R.Linv;
-    G.eta = R.eta;
-}
-
 // The three acceptance tests of tube.f90:806-818 for the grid point at offset d = x - ci0 in
 // the record's local frame: t0 >= 0, t1 < 0 and rho^2 < Rtube^2.  The arithmetic is spelled
 // out with explicit fmaf so that every caller (the row filter and the evaluation of the tile
@@ -544,6 +538,23 @@ __device__ __forceinline__ bool rec_tests(const RecT &R, float d0x, float d0y, f
     if (!(t1 < 0.0f)) return false;
     const float r2 = fmaf(-t0, t0, fmaf(d0z, d0z, fmaf(d0y, d0y, d0x * d0x)));
     return r2 < R.R2;
+}
+
+// rec_tests with the planes' rounding bound pe (plane_eps): 0 rejected, 1 accepted, 2 a plane
+// test within pe of zero.  The reference's field jumps across the plane shared by two
+// consecutive chords (zeta is interpolated along each chord separately), so such a pair is
+// decided by the reference's FP64 tests; beyond pe the FP32 signs are the FP64 signs.
+template <typename RecT>
+__device__ __forceinline__ int rec_classify(const RecT &R, float d0x, float d0y, float d0z, float pe)
+{
+    const float t0 = fmaf(d0z, R.tc0[2], fmaf(d0y, R.tc0[1], d0x * R.tc0[0]));
+    if (!(t0 >= -pe)) return 0;
+    const float ex = d0x - R.dci[0], ey = d0y - R.dci[1], ez = d0z - R.dci[2];
+    const float t1 = fmaf(ez, R.tc1[2], fmaf(ey, R.tc1[1], ex * R.tc1[0]));
+    if (!(t1 < pe)) return 0;
+    const float r2 = fmaf(-t0, t0, fmaf(d0z, d0z, fmaf(d0y, d0y, d0x * d0x)));
+    if (!(r2 < R.R2)) return 0;
+    return (t0 >= pe && t1 < -pe) ? 1 : 2;
 }
 
 // The vorticity of tube.f90:819-892 for the spline argument W = zb + w, measured from the

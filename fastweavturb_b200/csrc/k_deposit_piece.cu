@@ -38,8 +38,7 @@ struct __align__(16) PieceRec {
     int kq[3];
     float ph0;
     float inv2s2, ftd, amp, Gamma;   // constant-core profile (tube.f90:845-847)
-    float Linv, eta, q, guard;       // guard: half-width of the band around a plane where the
-                                     // piece-frame plane test is redone in the sample's frame
+    float Linv, eta, q, guard;       // guard: rounding bound of the piece-frame plane tests
     int box_lo[3];
     int nch;                // chords of the piece, 1..kPieceMax
     int box_hi[3];
@@ -237,13 +236,16 @@ __global__ void __launch_bounds__(128, 3) piece_build_kernel(
                                 __uint_as_float(pack3(hi3[0] - blo[0], hi3[1] - blo[1], hi3[2] - blo[2])));
         Wm = fmaxf(Wm, (zoff + (float)(nd + Rt) * fabsf(g)) * 1.01f);
     });
-    // FP32 rounding of the piece-frame plane test d . tci_k - c_k stays well below
-    // 1e-6 (|d|_1 + |c_k|); |d|_1 is bounded by the box corners' offsets
+    // FP32 rounding of the piece-frame plane test d . tci_k - c_k: the offsets d (off, dx and
+    // the fma, at most 4 u max|d_k| per axis), the normal (u |d|_1), c_k (u |c_k|) and the three
+    // fused sums (u (|d|_1 + |c_k|) each) add up to 8 u (|d|_1 + |c_k|) with u = 2^-24, below
+    // 5e-7 (|d|_1 + |c_k|); |d|_1 is bounded by the box corners' offsets.  The guard keeps a
+    // factor of four.
     float dmax = 0.0f;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
         dmax += fmaxf(fabsf(R.off[k]), fabsf(R.off[k] + (float)(bhi[k] - blo[k]) * R.dx));
-    R.guard = 1.0e-6f * (dmax + cmax) + 1.0e-30f;
+    R.guard = 2.0e-6f * (dmax + cmax) + 1.0e-30f;
     // the section's quintic Taylor-shifted to the piece start z0 (synthetic division)
     const double z0 = (zj0 - zl) * L;
     bool nowrap = true;
@@ -358,13 +360,14 @@ struct PieceStage {
     PBox box[kPChunk];
     ChordRows cr;
     uint32_t cq[kPQueue];  // candidates: chord lane (piece << 3 | chord) | x << 5 | y << 9 | z << 12 (tile-local)
-    uint32_t q[kPQueue];   // piece | chord << 3 | x << 6 | y << 10 | z << 13 (tile-local)
+    uint32_t q[kPQueue];   // piece | chord << 3 | x << 6 | y << 10 | z << 13 (tile-local) | kPQDecide
     RedoQueue redo;        // ill-conditioned pairs awaiting their FP64 evaluation
     uint32_t id[kPChunk];  // global record ids of the staged pieces
     uint64_t bar;
     uint64_t pad;
 };
 constexpr size_t kPieceSmem = kAccBytes + sizeof(PieceStage) * kDepWarps;
+constexpr uint32_t kPQDecide = 1u << 16;   // queued pair left to the reference's FP64 tests
 // three blocks per SM (the register budget allows three as well): the kernel hides the
 // latency of its record copies with the other blocks' warps
 static_assert(3 * (kPieceSmem + 1024) <= 228 * 1024, "deposit_piece_kernel: three blocks per SM");
@@ -387,41 +390,33 @@ __device__ __forceinline__ void pclip(const PieceRec &R, uint32_t img, int N, in
 }
 
 // The reference's acceptance of mesh point (rx, ry, rz) (offsets from the piece's box origin)
-// by chord j (tube.f90:806-818): t_j >= 0 and t_{j+1} < 0, tested in the piece frame and,
-// within the rounding band of a plane, again in that sample's own frame; then the distance to
-// chord line j below Rtube, in the chord's frame.  The caller keeps the point in chord j's box.
-__device__ __forceinline__ bool piece_accepts(const PieceRec &R, int j, int rx, int ry, int rz)
+// by chord j (tube.f90:806-818): t_j >= 0 and t_{j+1} < 0, tested in the piece frame, then the
+// distance to chord line j below Rtube, in the chord's frame.  Returns 0 (rejected), 1
+// (accepted) or 2: a plane test within its rounding bound (guard) of zero, which the
+// reference's FP64 tests decide (the field jumps across the plane two consecutive chords
+// share).  The caller keeps the point in chord j's box.
+__device__ __forceinline__ int piece_classify(const PieceRec &R, int j, int rx, int ry, int rz)
 {
     const float dxv = fmaf((float)rx, R.dx, R.off[0]);
     const float dyv = fmaf((float)ry, R.dx, R.off[1]);
     const float dzv = fmaf((float)rz, R.dx, R.off[2]);
-    bool pass = true;
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const float4 pl = R.pl[j + h];
-        float tk = fmaf(dzv, pl.z, fmaf(dyv, pl.y, fmaf(dxv, pl.x, -pl.w)));
-        if (fabsf(tk) < R.guard) {
-            const float4 po = R.po[j + h];
-            const float ex = fmaf((float)rx, R.dx, po.x);
-            const float ey = fmaf((float)ry, R.dx, po.y);
-            const float ez = fmaf((float)rz, R.dx, po.z);
-            tk = fmaf(ez, pl.z, fmaf(ey, pl.y, ex * pl.x));
-        }
-        pass = pass && (h == 0 ? tk >= 0.0f : !(tk >= 0.0f));
-    }
-    if (!pass) return false;
-    const float4 cp = R.po[j], pn = R.pl[j];
+    const float4 p0 = R.pl[j], p1 = R.pl[j + 1];
+    const float tj = fmaf(dzv, p0.z, fmaf(dyv, p0.y, fmaf(dxv, p0.x, -p0.w)));
+    const float tk = fmaf(dzv, p1.z, fmaf(dyv, p1.y, fmaf(dxv, p1.x, -p1.w)));
+    if (!(tj >= -R.guard) || !(tk < R.guard)) return 0;
+    const float4 cp = R.po[j];
     const float ex = fmaf((float)rx, R.dx, cp.x);
     const float ey = fmaf((float)ry, R.dx, cp.y);
     const float ez = fmaf((float)rz, R.dx, cp.z);
-    const float t0 = fmaf(ez, pn.z, fmaf(ey, pn.y, ex * pn.x));
+    const float t0 = fmaf(ez, p0.z, fmaf(ey, p0.y, ex * p0.x));
     const float r2 = fmaf(-t0, t0, fmaf(ez, ez, fmaf(ey, ey, ex * ex)));
-    return r2 < R.chq[j].y;
+    if (!(r2 < R.chq[j].y)) return 0;
+    return (tj >= R.guard && tk < -R.guard) ? 1 : 2;
 }
 
-// The candidate test of the FP64 path: piece_accepts with every test widened by far more than
-// its FP32 rounding (the guard band is that rounding), so that every point the reference's FP64
-// tests accept is queued; the FP64 tests then decide.
+// The candidate test of the FP64 path: piece_classify with every test widened by far more than
+// its FP32 rounding (the guard), so that every point the reference's FP64 tests accept is
+// queued; the FP64 tests then decide.
 __device__ __forceinline__ bool piece_accepts_wide(const PieceRec &R, int j, int rx, int ry, int rz)
 {
     const float dxv = fmaf((float)rx, R.dx, R.off[0]);
@@ -449,12 +444,14 @@ __device__ __forceinline__ bool piece_accepts_wide(const PieceRec &R, int j, int
 // therefore rasterised once, in a pass over pieces: one thread per piece walks, for each chord,
 // the columns of the chord's box along the axis best aligned with the chord, bounds each column
 // by the chord's two planes (0.05-point margin) and applies the deposition kernel's acceptance
-// test (piece_accepts; the widened test in the FP64 path) to the points in between.  A first
+// test (piece_classify; the widened test in the FP64 path) to the points in between.  A first
 // pass counts the points of every piece, a scan gives each piece its offset, and a second pass
-// writes them: chord | x << 3 | y << 12 | z << 21, offsets from the piece's box origin.  The
+// writes them: chord | x << 3 | y << 12 | z << 21 | kRasDecide (left to the FP64 tests),
+// offsets from the piece's box origin.  The
 // deposition kernel then only evaluates the listed points that fall in its tile.  err bit 16:
 // a chord box wider than 511 points (the 9-bit offsets).
 constexpr int kRasterMaxOff = 511;
+constexpr uint32_t kRasDecide = 1u << 30;
 
 template <bool Wide, bool Write>
 __global__ void __launch_bounds__(128) piece_raster_kernel(const PieceRec *__restrict__ rec, int64_t npieces,
@@ -518,14 +515,15 @@ __global__ void __launch_bounds__(128) piece_raster_kernel(const PieceRec *__res
                 const int ilo = max(alo, (int)ceilf(flo)), ihi = min(ahi, (int)floorf(fhi));
                 for (int ra = ilo; ra <= ihi; ++ra) {
                     const int rx = a == 0 ? ra : r0x, ry = a == 1 ? ra : r0y, rz = a == 2 ? ra : r0z;
-                    const bool ok = Wide ? piece_accepts_wide(R, j, rx, ry, rz) : piece_accepts(R, j, rx, ry, rz);
-                    if (!ok) continue;
+                    const int cls = Wide ? (piece_accepts_wide(R, j, rx, ry, rz) ? 1 : 0) : piece_classify(R, j, rx, ry, rz);
+                    if (cls == 0) continue;
                     if (Write) {
                         if (n >= cap) {
                             atomicOr(err, 32);
                             continue;
                         }
-                        pts[o + n] = (uint32_t)j | ((uint32_t)rx << 3) | ((uint32_t)ry << 12) | ((uint32_t)rz << 21);
+                        pts[o + n] = (uint32_t)j | ((uint32_t)rx << 3) | ((uint32_t)ry << 12) | ((uint32_t)rz << 21) |
+                                     (cls == 2 ? kRasDecide : 0u);
                     }
                     ++n;
                 }
@@ -536,13 +534,14 @@ __global__ void __launch_bounds__(128) piece_raster_kernel(const PieceRec *__res
 }
 
 // Evaluate the first `cnt` queued (point, chord) pairs, one per lane, into the tile cells;
-// pairs whose curved-branch amplification exceeds kRedoCond go to the redo queue instead.
+// pairs whose curved-branch amplification exceeds kRedoCond, and pairs left to the FP64 tests
+// (kPQDecide), go to the redo queue instead.
 template <bool General, bool F64>
 __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAccN], int lane, int cnt, int &qn,
                                              int &rn, unsigned &nacc, float fscale, float fmaxq, int *__restrict__ err,
     const RedoCtx &redo, int x0, int y0, int z0)
 {
-    bool flag = false, ok64 = false;
+    bool flag = false, ok64 = false, counted = false;
     uint32_t rrec = 0, rcode = 0;
     if (F64 && lane < cnt) {
         // FP64 path: the candidate passed the widened FP32 tests; the reference's FP64 tests
@@ -550,7 +549,7 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
         // whole periods)
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 7u), j = (int)((e >> 3) & 7u);
-        const int lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)(e >> 13);
+        const int lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)((e >> 13) & 7u);
         const PBox &B = S.box[k];
         const PieceRec &R = S.rec[k];
         int slot, jj;
@@ -564,36 +563,43 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
     } else if (lane < cnt) {
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 7u), j = (int)((e >> 3) & 7u);
-        const int lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)(e >> 13);
-        const PBox &B = S.box[k];
-        const PieceRec &R = S.rec[k];
-        const float4 cp = R.po[j], cq = R.chq[j], pn = R.pl[j];
-        const float ex = fmaf((float)(lx + B.dl[0]), R.dx, cp.x);
-        const float ey = fmaf((float)(ly + B.dl[1]), R.dx, cp.y);
-        const float ez = fmaf((float)(lz + B.dl[2]), R.dx, cp.z);
-        const float t0 = fmaf(ez, pn.z, fmaf(ey, pn.y, ex * pn.x));
-        float vv[3], cond;
-        vort_w<General, true>(R, ex, ey, ez, cp.w, t0 * cq.x, cq.y, vv, cond);
-        const int p = lx + kSY * ly + kSZ * lz;
-        flag = General && !(cond <= kRedoCond);
-        if (flag) {
-            rrec = (S.id[k] & ((1u << 26) - 1u)) | ((uint32_t)j << 26);
+        const int lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)((e >> 13) & 7u);
+        if (e & kPQDecide) {
+            flag = true;
+            rrec = (S.id[k] & ((1u << 26) - 1u)) | ((uint32_t)j << 26) | kRedoDecide;
             rcode = redo_code(lx, ly, lz);
         } else {
+            counted = true;
+            const PBox &B = S.box[k];
+            const PieceRec &R = S.rec[k];
+            const float4 cp = R.po[j], cq = R.chq[j], pn = R.pl[j];
+            const float ex = fmaf((float)(lx + B.dl[0]), R.dx, cp.x);
+            const float ey = fmaf((float)(ly + B.dl[1]), R.dx, cp.y);
+            const float ez = fmaf((float)(lz + B.dl[2]), R.dx, cp.z);
+            const float t0 = fmaf(ez, pn.z, fmaf(ey, pn.y, ex * pn.x));
+            float vv[3], cond;
+            vort_w<General, true>(R, ex, ey, ez, cp.w, t0 * cq.x, cq.y, vv, cond);
+            const int p = lx + kSY * ly + kSZ * lz;
+            flag = General && !(cond <= kRedoCond);
+            if (flag) {
+                rrec = (S.id[k] & ((1u << 26) - 1u)) | ((uint32_t)j << 26);
+                rcode = redo_code(lx, ly, lz);
+            } else {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                float sv = vv[d] * fscale;
-                if (!(fabsf(sv) < fmaxq)) {
-                    atomicOr(err, 4);
-                    sv = sv != sv ? 0.0f : copysignf(fmaxq, sv);
+                for (int d = 0; d < 3; ++d) {
+                    float sv = vv[d] * fscale;
+                    if (!(fabsf(sv) < fmaxq)) {
+                        atomicOr(err, 4);
+                        sv = sv != sv ? 0.0f : copysignf(fmaxq, sv);
+                    }
+                    atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(sv));
                 }
-                atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(sv));
             }
         }
     }
     if constexpr (F64) nacc += __popc(__ballot_sync(0xffffffffu, ok64));
-    else nacc += cnt;
-    if constexpr (General && !F64) {
+    else nacc += __popc(__ballot_sync(0xffffffffu, counted));
+    if constexpr (!F64) {
         redo_push(S.redo, lane, flag, rrec, rcode, rn);
         if (rn >= 32) redo_drain(S.redo, redo, acc, lane, 32, rn, x0, y0, z0, err);
     }
@@ -606,8 +612,9 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
     qn = rem;
 }
 
-// Test the first `cnt` candidate points, one per lane (piece_accepts), queue the accepted
-// (point, chord) pairs, drop the candidates and evaluate the queue when it holds 32 pairs.
+// Test the first `cnt` candidate points, one per lane (piece_classify), queue the accepted
+// (point, chord) pairs and those left to the FP64 tests, drop the candidates and evaluate the
+// queue when it holds 32 pairs.
 template <bool General, bool F64>
 __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[kAccN], int lane, int cnt, int &cn,
                                                 int &qn, int &rn, unsigned &nacc, float fscale, float fmaxq,
@@ -620,9 +627,11 @@ __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[
         const int c = (int)(e & 31u), k = c >> 3, j = c & 7;
         const int lx = (int)((e >> 5) & 15u), ly = (int)((e >> 9) & 7u), lz = (int)(e >> 12);
         const PBox &B = S.box[k];
-        ok = F64 ? piece_accepts_wide(S.rec[k], j, lx + B.dl[0], ly + B.dl[1], lz + B.dl[2])
-                 : piece_accepts(S.rec[k], j, lx + B.dl[0], ly + B.dl[1], lz + B.dl[2]);
-        code = (uint32_t)k | ((uint32_t)j << 3) | ((uint32_t)lx << 6) | ((uint32_t)ly << 10) | ((uint32_t)lz << 13);
+        const int cls = F64 ? (piece_accepts_wide(S.rec[k], j, lx + B.dl[0], ly + B.dl[1], lz + B.dl[2]) ? 1 : 0)
+                            : piece_classify(S.rec[k], j, lx + B.dl[0], ly + B.dl[1], lz + B.dl[2]);
+        ok = cls != 0;
+        code = (uint32_t)k | ((uint32_t)j << 3) | ((uint32_t)lx << 6) | ((uint32_t)ly << 10) | ((uint32_t)lz << 13) |
+               (cls == 2 ? kPQDecide : 0u);
     }
     const unsigned bal = __ballot_sync(0xffffffffu, ok);
     if (ok) S.q[qn + __popc(bal & ((1u << lane) - 1u))] = code;
@@ -640,8 +649,8 @@ __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[
 // records with one bulk asynchronous copy each, then walks the rows of the chords' boxes within
 // the tile, one row per lane: the row's candidate interval, then per candidate point the
 // reference's tests (tube.f90:793-818: t_j >= 0, t_{j+1} < 0, distance to chord line j below
-// Rtube) with the plane tests in the piece frame and, within the rounding band of a plane, in
-// that sample's own frame.  Accepted pairs are queued and evaluated 32 at a time.
+// Rtube) with the plane tests in the piece frame; within the rounding bound of a plane the
+// reference's FP64 tests decide.  Accepted pairs are queued and evaluated 32 at a time.
 template <bool General, bool Accumulate, bool F64, bool Raster>
 __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel(
     const PieceRec *__restrict__ rec, int N, int ntx, int nty, int tz0, const int64_t *__restrict__ tile_off,
@@ -735,7 +744,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
                     ok = lx >= B.lo[0] && lx < B.lo[0] + B.n[0] && ly >= B.lo[1] && ly < B.lo[1] + B.n[1] &&
                          lz >= B.lo[2] && lz < B.lo[2] + B.n[2];
                     code = (uint32_t)k | ((uint32_t)j << 3) | ((uint32_t)lx << 6) | ((uint32_t)ly << 10) |
-                           ((uint32_t)lz << 13);
+                           ((uint32_t)lz << 13) | ((e & kRasDecide) ? kPQDecide : 0u);
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, ok);
                 if (ok) S.q[qn + __popc(bal & ((1u << lane) - 1u))] = code;
@@ -949,7 +958,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
         if (lane == 0) nxt = atomicAdd(&next_chunk, 1);
         ch = __shfl_sync(0xffffffffu, nxt, 0);
     }
-    if constexpr (General && !F64)
+    if constexpr (!F64)
         if (rn > 0) redo_drain(S.redo, redo, acc, lane, rn, rn, x0, y0, z0, err);
     if (failed && lane == 0) atomicOr(err, 2);
     if (lane == 0 && redo.tally) atomicAdd(redo.tally, (unsigned long long)nacc);

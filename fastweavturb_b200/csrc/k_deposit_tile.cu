@@ -8,15 +8,16 @@
 //    the tile.
 // 3. deposit_tile_kernel: one CTA per tile, accumulating the tile in shared int64 fixed-point
 //    cells.  Integer addition is associative, so the tile sum is bit-exact whatever the order
-//    of candidates.  Candidates are processed in double-buffered chunks: the ids of chunk i+2
-//    arrive by a bulk asynchronous copy (cp.async.bulk, the TMA engine's 1-D form) and the
-//    FP32 records of chunk i+1 by cp.async while chunk i is evaluated.  A chunk's work is
-//    flattened into grid rows along each candidate's best-aligned axis; each row solves the
-//    two half-space tests and the cylinder test of tube.f90:806-818 for its index interval
-//    (one-point margin) and evaluates the reference predicate and vorticity only there, where
-//    the reference walks the whole box (about 11 points per accepted one at these
-//    sub-segment lengths).  The tile is written once with coalesced float4 stores; its
-//    component min/max are folded into the epilogue.
+//    of candidates.  Each warp claims chunks of candidates and stages their FP32 records with
+//    one bulk asynchronous copy each (cp.async.bulk, the TMA engine's 1-D form, completing on
+//    the warp's mbarrier).  A chunk's work is flattened into grid rows along each candidate's
+//    best-aligned axis; each row solves the two half-space tests and the cylinder test of
+//    tube.f90:806-818 for its index interval (one-point margin) and evaluates the reference
+//    predicate and vorticity only there, where the reference walks the whole box (about 11
+//    points per accepted one at these sub-segment lengths).  A point whose plane test lies
+//    within its FP32 rounding bound of zero is decided by the reference's FP64 tests, and
+//    evaluated in FP64 if accepted: the field jumps across the plane two consecutive chords
+//    share.  The tile is written once with coalesced float4 stores.
 #include <cstdio>
 #include <cstdlib>
 
@@ -105,7 +106,7 @@ struct CandBox {
     float i2q;      // 1 / (2 q2)
     float rnb;      // (1 + 1e-6) / n[(axis+1)%3]: row -> (jb, jc) without an integer divide
     int dl[3];      // dorg - lo: tile-local coordinate -> grid offset from the record's box_lo
-    int pad;
+    float pe;       // rounding bound of the record's plane tests (plane_eps)
 };
 
 // Index interval [ilo, ihi] (clamped to [0, n-1]) of the grid row d0 + i dx e_a that can pass
@@ -179,6 +180,8 @@ __device__ __forceinline__ void clip_box(const SegRec &R, uint32_t img, int N, i
     B.q2 = q2 > 0.01f * dx * dx ? q2 : 0.0f;
     B.i2q = B.q2 > 0.0f ? 0.5f / B.q2 : 0.0f;
     B.rnb = nonempty ? 1.000001f / (float)nbv : 0.0f;
+    const int ext[3] = {R.box_hi[0] - R.box_lo[0], R.box_hi[1] - R.box_lo[1], R.box_hi[2] - R.box_lo[2]};
+    B.pe = plane_eps(R.off, ext, dx, R.dci);
 }
 
 // Warp-autonomous tile deposition.  Each warp claims chunks of kWarpChunk candidates of the
@@ -192,30 +195,33 @@ struct WarpStage {
     SegRec rec[kWarpChunk];
     CandBox box[kWarpChunk];
     uint32_t q[kQueue];         // accepted points: candidate | x << 4 | y << 8 | z << 11 (tile-local)
+                                // | kQDecide (a plane test within its rounding bound)
     RedoQueue redo;             // ill-conditioned pairs awaiting their FP64 evaluation
     uint32_t id[kWarpChunk];    // global record ids of the staged candidates
     uint64_t bar;
     uint64_t pad;
 };
 constexpr size_t kDepSmem = kAccBytes + sizeof(WarpStage) * kDepWarps;
+constexpr uint32_t kQDecide = 1u << 15;
 
 // Evaluate the first `cnt` queued points of the warp, one per lane (rec_tests again for t0,
 // then the vorticity), add them into the tile's fixed-point cells and drop them from the queue.
-// Pairs whose curved-branch amplification exceeds kRedoCond go to the warp's redo queue
-// instead, for an FP64 evaluation.
+// Pairs whose curved-branch amplification exceeds kRedoCond, and pairs with a plane test
+// within its rounding bound (kQDecide), go to the warp's redo queue instead, for the
+// reference's FP64 tests and evaluation.
 template <bool General, bool F64>
 __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN], int lane, int cnt, int &qn,
                                             int &rn, unsigned &nacc, float fscale, float fmaxq, int *__restrict__ err,
                                             const RedoCtx &redo, int x0, int y0, int z0)
 {
-    bool flag = false, ok64 = false;
+    bool flag = false, ok64 = false, counted = false;
     uint32_t rcode = 0, rrec = 0;
     if (F64 && lane < cnt) {
         // FP64 tile path: the candidate passed the widened FP32 tests; the reference's FP64
         // tests decide, at its index in the sub-segment's own box
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 15u);
-        const int lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)(e >> 11);
+        const int lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)((e >> 11) & 7u);
         const CandBox &B = S.box[k];
         const SegRec &R = S.rec[k];
         ok64 = eval_pair_f64(redo, (int64_t)(S.id[k] & ((1u << 26) - 1u)), R.box_lo[0] + lx + B.dl[0],
@@ -224,35 +230,42 @@ __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN
     } else if (lane < cnt) {
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 15u);
-        const int lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)(e >> 11);
-        const CandBox &B = S.box[k];
-        const SegRec &R = S.rec[k];
-        const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
-        const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
-        const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
-        float t0, vv[3], cond;
-        rec_tests(R, d0x, d0y, d0z, t0);
-        rec_vorticity<General>(R, d0x, d0y, d0z, t0, vv, cond);
-        const int p = lx + kSY * ly + kSZ * lz;
-        flag = General && !(cond <= kRedoCond);
-        if (flag) {
-            rrec = S.id[k] & ((1u << 26) - 1u);
+        const int lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)((e >> 11) & 7u);
+        if (e & kQDecide) {
+            flag = true;
+            rrec = (S.id[k] & ((1u << 26) - 1u)) | kRedoDecide;
             rcode = redo_code(lx, ly, lz);
         } else {
+            counted = true;
+            const CandBox &B = S.box[k];
+            const SegRec &R = S.rec[k];
+            const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
+            const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
+            const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
+            float t0, vv[3], cond;
+            rec_tests(R, d0x, d0y, d0z, t0);
+            rec_vorticity<General>(R, d0x, d0y, d0z, t0, vv, cond);
+            const int p = lx + kSY * ly + kSZ * lz;
+            flag = General && !(cond <= kRedoCond);
+            if (flag) {
+                rrec = S.id[k] & ((1u << 26) - 1u);
+                rcode = redo_code(lx, ly, lz);
+            } else {
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                float sv = vv[d] * fscale;
-                if (!(fabsf(sv) < fmaxq)) {
-                    atomicOr(err, 4);
-                    sv = sv != sv ? 0.0f : copysignf(fmaxq, sv);
+                for (int d = 0; d < 3; ++d) {
+                    float sv = vv[d] * fscale;
+                    if (!(fabsf(sv) < fmaxq)) {
+                        atomicOr(err, 4);
+                        sv = sv != sv ? 0.0f : copysignf(fmaxq, sv);
+                    }
+                    atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(sv));
                 }
-                atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)__float2ll_rn(sv));
             }
         }
     }
     if constexpr (F64) nacc += __popc(__ballot_sync(0xffffffffu, ok64));
-    else nacc += cnt;
-    if constexpr (General && !F64) {
+    else nacc += __popc(__ballot_sync(0xffffffffu, counted));
+    if constexpr (!F64) {
         redo_push(S.redo, lane, flag, rrec, rcode, rn);
         if (rn >= 32) redo_drain(S.redo, redo, acc, lane, 32, rn, x0, y0, z0, err);
     }
@@ -351,9 +364,9 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
         const int rowoff = incl - nrows;
         const int total = __shfl_sync(0xffffffffu, incl, kWarpChunk - 1);
         __syncwarp();
-        // Rows, one per lane: solve the row's index interval, test its points (rec_tests) in
-        // lock step and queue the accepted ones; every 32 queued points are evaluated with
-        // all lanes busy.
+        // Rows, one per lane: solve the row's index interval, test its points (rec_classify) in
+        // lock step and queue the accepted ones and those left to the FP64 tests; every 32
+        // queued points are evaluated with all lanes busy.
         for (int r0 = 0; r0 < total; r0 += 32) {
             const int r = r0 + lane;
             // candidate of row r: last k with rowoff_k <= r (binary search over the lanes)
@@ -399,13 +412,12 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
                     const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
                     const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
                     const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
-                    if constexpr (F64) {
-                        ok = rec_tests_wide(R, d0x, d0y, d0z);
-                    } else {
-                        float t0;
-                        ok = rec_tests(R, d0x, d0y, d0z, t0);
-                    }
-                    code = (uint32_t)k | ((uint32_t)lx << 4) | ((uint32_t)ly << 8) | ((uint32_t)lz << 11);
+                    int cls;
+                    if constexpr (F64) cls = rec_tests_wide(R, d0x, d0y, d0z) ? 1 : 0;
+                    else cls = rec_classify(R, d0x, d0y, d0z, B.pe);
+                    ok = cls != 0;
+                    code = (uint32_t)k | ((uint32_t)lx << 4) | ((uint32_t)ly << 8) | ((uint32_t)lz << 11) |
+                           (cls == 2 ? kQDecide : 0u);
                     ++i;
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, ok);
@@ -421,7 +433,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
         if (lane == 0) nxt = atomicAdd(&next_chunk, 1);
         ch = __shfl_sync(0xffffffffu, nxt, 0);
     }
-    if constexpr (General && !F64)
+    if constexpr (!F64)
         if (rn > 0) redo_drain(S.redo, redo, acc, lane, rn, rn, x0, y0, z0, err);
     if (failed && lane == 0) atomicOr(err, 2);
     if (lane == 0 && redo.tally) atomicAdd(redo.tally, (unsigned long long)nacc);

@@ -322,17 +322,19 @@ __device__ __forceinline__ int box_index(int i, int lo, int N)
 
 
 
-// ---------------------------------------------------------------- FP64 redo of ill-conditioned pairs
-// A warp queues the accepted (point, chord) pairs whose curved-branch amplification
-// |1/(1 - kappa rho cos theta)| exceeds kRedoCond (tube.f90:876-879: the FP32 value carries the
-// amplified rounding of kappa, rho and cos theta) and evaluates them 32 at a time, one per
-// lane, in the reference's FP64 arithmetic from the batch's FP64 spline data (redo_pair_f64),
-// adding the fixed-point result into the same tile cells.  Only tubes with a varying core or
-// a twist reach this path: with a constant core and no twist the vorticity has no curvature
-// term.
+// ---------------------------------------------------------------- FP64 redo of pairs
+// A warp queues two kinds of (point, chord) pairs and evaluates them 32 at a time, one per lane,
+// in the reference's FP64 arithmetic from the batch's FP64 spline data (redo_pair_f64), adding
+// the fixed-point result into the same tile cells:
+// * accepted pairs whose curved-branch amplification |1/(1 - kappa rho cos theta)| exceeds
+//   kRedoCond (tube.f90:876-879: the FP32 value carries the amplified rounding of kappa, rho and
+//   cos theta); only tubes with a varying core or a twist have that term;
+// * pairs with a plane test within its FP32 rounding bound of zero, which the reference's FP64
+//   tests decide (the decide bit).
 struct RedoQueue {
-    uint2 e[64];   // x: record id | chord << 26; y: tile-local point x | y << 4 | z << 7
+    uint2 e[64];   // x: record id | chord << 26 | decide << 31; y: tile-local point x | y << 4 | z << 7
 };
+constexpr uint32_t kRedoDecide = 1u << 31;
 
 __device__ __forceinline__ uint32_t redo_code(int lx, int ly, int lz)
 {
@@ -349,21 +351,32 @@ __device__ __forceinline__ void redo_push(RedoQueue &Q, int lane, bool flag, uin
     __syncwarp();
 }
 
-// Evaluate the first cnt queued pairs in FP64 and drop them from the queue.
+// Evaluate the first cnt queued pairs in FP64 and drop them from the queue.  Decided pairs
+// that the FP64 tests accept are added to the tally of accepted pairs.
 __device__ __forceinline__ void redo_drain(RedoQueue &Q, const RedoCtx &R, long long (*acc)[kAccN], int lane, int cnt,
                                            int &rn, int x0, int y0, int z0, int *__restrict__ err)
 {
+    bool taken = false;
     if (lane < cnt) {
         const uint2 e = Q.e[lane];
-        const int lx = (int)(e.y & 15u), ly = (int)((e.y >> 4) & 7u), lz = (int)(e.y >> 7);
+        const int lx = (int)(e.y & 15u), ly = (int)((e.y >> 4) & 7u), lz = (int)((e.y >> 7) & 7u);
+        const bool decide = (e.x & kRedoDecide) != 0u;
         long long q[3];
-        if (!redo_pair_f64(R, e.x & ((1u << 26) - 1u), (int)(e.x >> 26), x0 + lx, y0 + ly, z0 + lz, q))
-            atomicOr(err, 4);
-        const int p = lx + kSY * ly + kSZ * lz;
+        const int r = redo_pair_f64(R, e.x & ((1u << 26) - 1u), (int)((e.x >> 26) & 7u), decide, x0 + lx, y0 + ly,
+                                    z0 + lz, q);
+        if (r < 0) atomicOr(err, 4);
+        taken = decide && r != 0;
+        if (r != 0) {
+            const int p = lx + kSY * ly + kSZ * lz;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)q[d]);
+            for (int d = 0; d < 3; ++d) atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)q[d]);
+        }
     }
-    if (lane == 0 && R.tally) atomicAdd(R.tally + 1, (unsigned long long)cnt);
+    const unsigned nt = __popc(__ballot_sync(0xffffffffu, taken));
+    if (lane == 0 && R.tally) {
+        atomicAdd(R.tally + 1, (unsigned long long)cnt);
+        if (nt) atomicAdd(R.tally, (unsigned long long)nt);
+    }
     __syncwarp();
     const int rem = rn - cnt;
     const uint2 keep = lane < rem ? Q.e[cnt + lane] : make_uint2(0u, 0u);

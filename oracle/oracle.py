@@ -43,41 +43,71 @@ PI2 = 2.0 * PI
 
 
 def build() -> str:
-    """Compile the C part of the oracle into oracle/_build/liborc.so."""
+    """Compile the C part of the oracle into oracle/_build/liborc.so (and the FMA-contracted
+    variant liborc_fma.so)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
+
+
+def _load(path):
+    """Load one build of the C restatement and declare its entry points."""
+    if not os.path.exists(path):
+        build()
+    L = ctypes.CDLL(path)
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.orc_line_prep.argtypes = [ctypes.c_int, dp, dp, dp, dp, dp, dp, dp]
+    L.orc_line_ntf.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ctypes.c_int, ip, dp, dp, dp]
+    L.orc_line_ntf.restype = ctypes.c_int
+    L.orc_line_subsegs.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ctypes.c_int, dp]
+    L.orc_line_subsegs.restype = ctypes.c_long
+    L.orc_deposit_line.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_int, dp, dp, dp, ctypes.c_int, dp]
+    L.orc_deposit_line.restype = ctypes.c_long
+    L.orc_deposit_line_cond.argtypes = L.orc_deposit_line.argtypes + [dp]
+    L.orc_deposit_line_cond.restype = ctypes.c_long
+    L.orc_sp.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ip, ctypes.c_int, dp, ctypes.c_int]
+    L.orc_philox.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                             ctypes.POINTER(ctypes.c_uint32)]
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    L.orc_philox_raw.argtypes = [u32p, u32p, u32p]
+    L.orc_fbb_gauss.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, dp, dp]
+    L.orc_fbb_shift.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
+    L.orc_fbb_shift.restype = ctypes.c_double
+    L.orc_fbb_sign.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
+    L.orc_fbb_sign.restype = ctypes.c_int
+    return L
 
 
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_LIB_PATH):
-            build()
-        L = ctypes.CDLL(_LIB_PATH)
-        dp = ctypes.POINTER(ctypes.c_double)
-        ip = ctypes.POINTER(ctypes.c_int)
-        L.orc_line_prep.argtypes = [ctypes.c_int, dp, dp, dp, dp, dp, dp, dp]
-        L.orc_line_ntf.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ctypes.c_int, ip, dp, dp, dp]
-        L.orc_line_ntf.restype = ctypes.c_int
-        L.orc_line_subsegs.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ctypes.c_int, dp]
-        L.orc_line_subsegs.restype = ctypes.c_long
-        L.orc_deposit_line.argtypes = [ctypes.c_void_p, ctypes.c_int, dp, dp, dp, ctypes.c_double,
-                                       ctypes.c_double, ctypes.c_int, dp, dp, dp, ctypes.c_int, dp]
-        L.orc_deposit_line.restype = ctypes.c_long
-        L.orc_deposit_line_cond.argtypes = L.orc_deposit_line.argtypes + [dp]
-        L.orc_deposit_line_cond.restype = ctypes.c_long
-        L.orc_sp.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_int, ip, ctypes.c_int, dp, ctypes.c_int]
-        L.orc_philox.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
-                                 ctypes.POINTER(ctypes.c_uint32)]
-        u32p = ctypes.POINTER(ctypes.c_uint32)
-        L.orc_philox_raw.argtypes = [u32p, u32p, u32p]
-        L.orc_fbb_gauss.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, dp, dp]
-        L.orc_fbb_shift.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32]
-        L.orc_fbb_shift.restype = ctypes.c_double
-        L.orc_fbb_sign.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
-        L.orc_fbb_sign.restype = ctypes.c_int
-        _lib = L
+        _lib = _load(_LIB_PATH)
     return _lib
+
+
+_LIB_FMA_PATH = os.path.join(_HERE, "_build", "liborc_fma.so")
+_lib_fma = None
+
+
+def has_fma() -> bool:
+    """Whether this host's CPU has fused multiply-add (the contracted build needs it)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            return any(ln.startswith("flags") and " fma" in ln for ln in f)
+    except OSError:
+        return False
+
+
+def lib_fma():
+    """The same C restatement compiled with FMA contraction (-mfma -ffp-contract=fast): every
+    a*b+c of the plain build fused, the operation order otherwise unchanged.  Two equally valid
+    FP64 evaluations of the reference's algorithm; their distance is the reference's own
+    rounding floor on a workload (its zeta interpolation amplifies ulp-level changes)."""
+    global _lib_fma
+    if _lib_fma is None:
+        _lib_fma = _load(_LIB_FMA_PATH)
+    return _lib_fma
 
 
 def _dp(a):
@@ -201,9 +231,12 @@ def line_subsegs(xyz, ntf_times=50, ntf_pre=1000):
     return out[:cnt * 15].reshape(cnt, 15)
 
 
-def deposit(params: Params, cl: Centerlines, nthreads=None, line_s=None, line_e=None, vor=None, cond=None):
+def deposit(params: Params, cl: Centerlines, nthreads=None, line_s=None, line_e=None, vor=None, cond=None,
+            contracted=False):
     """Deposit lines line_s..line_e (1-based, inclusive) into vor (3,N,N,N); applies the
     per-line spectral filter of lines flagged if_filter (tube.f90:528-946).
+
+    contracted: run the FMA-contracted build (lib_fma) instead of the plain one.
 
     cond: optional (N,N,N) array; each point receives the maximum over its contributions of
     |1/(1 - kappa rho cos theta)|, the curved branch's amplification (1 when straight)."""
@@ -225,11 +258,12 @@ def deposit(params: Params, cl: Centerlines, nthreads=None, line_s=None, line_e=
         args = (ctypes.byref(g), xyz.shape[0], _dp(cx), _dp(cy), _dp(cz), float(params.sigma[il - 1]),
                 float(params.Gamma[il - 1]), int(params.n_T[il - 1]), _dp(vx), _dp(vy), _dp(vz), nthreads,
                 _dp(stats))
+        L = lib_fma() if contracted else lib()
         if cond is None:
-            nsub = lib().orc_deposit_line(*args)
+            nsub = L.orc_deposit_line(*args)
         else:
             assert cond.shape == (N, N, N) and cond.dtype == np.float64 and cond.flags.c_contiguous
-            nsub = lib().orc_deposit_line_cond(*args, _dp(cond))
+            nsub = L.orc_deposit_line_cond(*args, _dp(cond))
         if nsub < 0:
             raise ValueError(f"line {il}: needs at least 2 nodes")
         info.append((il, xyz.shape[0], int(stats[0]) // (xyz.shape[0] + 1), int(stats[1]), int(stats[2])))

@@ -51,3 +51,33 @@ def two_tubes(O, N=24, seed=4):
                  Gamma=np.array([1.0, -0.6]), n_T=np.array([1, 1], dtype=np.int32),
                  if_filter=np.zeros(2, dtype=np.int32))
     return p, O.Centerlines(npoint=np.array([96, 128], dtype=np.int64), xyz=xyz)
+
+
+def sp_close(sp, sp_ref, q, rtol):
+    """S_{q+1}(r) against a reference: |a - b| <= rtol max(|b|, s), s = (max_r S_2)^((q+1)/2) the
+    natural size of |du|^(q+1).  Odd orders change sign and pass through zero, where a purely
+    relative bound would demand agreement far below the rounding of the sum."""
+    sp = np.asarray(sp, dtype=np.float64)
+    sp_ref = np.asarray(sp_ref, dtype=np.float64)
+    s = float(np.max(np.abs(sp_ref[1]))) ** ((q + 1) / 2.0)
+    a, b = sp[q], sp_ref[q]
+    bound = rtol * np.maximum(np.abs(b), s)
+    bad = np.abs(a - b) > bound
+    assert not bad.any(), f"S_{q + 1}: {a[bad]} vs {b[bad]} (bound {bound[bad]})"
+
+
+def fp64_floor(O, p, cl, **kw):
+    """The reference algorithm's own FP64 rounding floor on a workload: the relative L2 distance
+    between the oracle's plain build and its FMA-contracted build (oracle.lib_fma), or None on a
+    host without FMA.  Returns (floor, plain deposit)."""
+    a, _ = O.deposit(p, cl, **kw)
+    if not O.has_fma():
+        return None, a
+    b, _ = O.deposit(p, cl, contracted=True, **kw)
+    return rel_l2(b, a), a
+
+
+def tol64(floor):
+    """FP64 tolerance against the oracle: four times the reference's own rounding floor
+    (fp64_floor), and never below 1e-12; 5e-11 where the floor cannot be measured."""
+    return 5e-11 if floor is None else max(1e-12, 4.0 * floor)

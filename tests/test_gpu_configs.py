@@ -2,22 +2,28 @@
 
 * cfg0 whole (64^3, 3 levels, 84 tubes, 74,752 nodes): omega, u, E(k) of omega and u, the
   normalisation, S_p for p = 2..6 on the reference's separations, the downsampled field
-  output and the numbers of info.dat; FP32 tile path <= 1e-5, FP64 path <= 1e-12.
+  output and the numbers of info.dat; FP32 tile path <= 1e-5.
 * cfg1 (256^3, 6 levels) bounded to the first two tubes of every level (the oracle walks the
   whole box of every sub-segment; the full 5,460 tubes take it about an hour): omega through
-  both tile kernels, FP32 <= 1e-5 and FP64 <= 1e-12.
+  both tile kernels, FP32 <= 1e-5.
 
-Tolerances are relative L2 norms over every grid point (S_p: relative error per entry).
+The FP64 paths are held to four times the reference algorithm's own FP64 rounding floor on the
+same workload (helpers.fp64_floor: the distance between the oracle's plain and FMA-contracted
+builds, 4.6e-12 on cfg0 and 1.7e-11 on the bounded cfg1), and never below 1e-12: zeta is
+interpolated along each chord from projections that cancel, so ulp-level changes anywhere in
+the sample set-up move the reference's own output by about 1e-11.
+
+Tolerances are relative L2 norms over every grid point (S_p: per entry, relative to the larger
+of the entry and the natural size (max S_2)^(p/2)).
 """
 import numpy as np
 import pytest
 
-from helpers import gpu_params, oracle_inputs, rel_l2
+from helpers import fp64_floor, gpu_params, oracle_inputs, rel_l2, sp_close, tol64
 
 pytestmark = pytest.mark.gpu
 
 TOL32 = 1e-5
-TOL64 = 1e-12
 
 
 @pytest.fixture(scope="module")
@@ -27,12 +33,16 @@ def cfg0_case(orc):
     w = cfg0(seed=0)
     p, cl = oracle_inputs(orc, w)
     p.N_downsample = w.N // 4
-    return w, p, cl, orc.run(p, cl)
+    floor, _ = fp64_floor(orc, p, cl)
+    ref = orc.run(p, cl)
+    ref["floor"] = floor
+    return w, p, cl, ref
 
 
-@pytest.mark.parametrize("precision,mode,tol", [(32, 0, TOL32), (64, 0, TOL64), (64, 1, TOL64)])
-def test_cfg0_whole_field_matches_oracle(fwt, orc, cfg0_case, precision, mode, tol):
+@pytest.mark.parametrize("precision,mode", [(32, 0), (64, 0), (64, 1)])
+def test_cfg0_whole_field_matches_oracle(fwt, orc, cfg0_case, precision, mode):
     w, p, cl, ref = cfg0_case
+    tol = TOL32 if precision == 32 else tol64(ref["floor"])
     ctx = fwt.Context(gpu_params(fwt, w, precision=precision, deposit_mode=mode, N_downsample=w.N // 4))
     ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
     ctx.run()
@@ -48,7 +58,7 @@ def test_cfg0_whole_field_matches_oracle(fwt, orc, cfg0_case, precision, mode, t
     r, Sp = ctx.Sp_calculate(pmax=10)
     assert np.array_equal(r, ref["Sp_r"])
     for q in range(1, 6):   # S_2 .. S_6
-        np.testing.assert_allclose(Sp[q], ref["Sp"][q], rtol=tol * 10 if q >= 3 else tol)
+        sp_close(Sp, ref["Sp"], q, tol * 10 if q >= 3 else tol)
     # the downsampled field output (N_downsample = N / 4): REAL(4) values of FP64 or FP32 fields
     fw = ctx.output_v()
     assert fw.shape == ref["field_wh"].shape == (2, 16, 16, 16)
@@ -70,8 +80,7 @@ def test_cfg0_sp_fp64_to_fp64_rounding(fwt, orc, cfg0_case):
     r_o, Sp_o = orc.structure_functions(vel, pmax=10, nthreads=4)
     assert np.array_equal(r, r_o)
     for q in range(10):
-        scale = np.abs(Sp_o[q]).max()
-        assert np.abs(Sp[q] - Sp_o[q]).max() <= 1e-12 * scale, q
+        sp_close(Sp, Sp_o, q, 1e-12)
     ctx.close()
 
 
@@ -87,8 +96,10 @@ def test_cfg0_info_dat_numbers(fwt, orc, cfg0_case, tmp_path):
     for ln in (tmp_path / "output" / "info.dat").read_text().splitlines():
         if "=" in ln:
             k, v = ln.split("=", 1)
-            if v.strip():
+            try:   # rows of '=' characters frame the file
                 rows[k.strip()] = float(v.replace("D", "E").replace("d", "e"))
+            except ValueError:
+                continue
     length = sum(2 * np.pi * orc.line_prep(cl.line(i))[3] for i in range(len(cl.npoint)))
     assert rows["N"] == w.N
     assert rows["Total length of curve"] == pytest.approx(length, rel=1e-12)
@@ -108,15 +119,16 @@ def cfg1_bounded(orc):
     for L in w.levels:
         L.tubes = min(L.tubes, 2)
     p, cl = oracle_inputs(orc, w)
-    vor, _ = orc.deposit(p, cl)
-    return w, p, cl, vor
+    floor, vor = fp64_floor(orc, p, cl)
+    return w, p, cl, vor, floor
 
 
-@pytest.mark.parametrize("precision,mode,tol", [(32, 0, TOL32), (64, 0, TOL64)])
-def test_cfg1_first_tubes_of_every_level(fwt, cfg1_bounded, precision, mode, tol):
+@pytest.mark.parametrize("precision,mode", [(32, 0), (64, 0)])
+def test_cfg1_first_tubes_of_every_level(fwt, cfg1_bounded, precision, mode):
     """Levels 0-2 (truncation radius 12-49 grid spacings) take the sub-segment kernel, levels
     3-5 (1.5-6.1 grid spacings) the chord-piece kernel."""
-    w, p, cl, vor = cfg1_bounded
+    w, p, cl, vor, floor = cfg1_bounded
+    tol = TOL32 if precision == 32 else tol64(floor)
     ctx = fwt.Context(gpu_params(fwt, w, precision=precision, deposit_mode=mode))
     ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
     ctx.deposit()
@@ -192,4 +204,4 @@ def test_ensemble_member_matches_oracle(fwt, orc):
     assert st["up"] == pytest.approx(ref["up"], rel=TOL32)
     assert rel_l2(st["Ek"], ref["spectrum"]) <= TOL32
     for q in range(1, 6):
-        np.testing.assert_allclose(st["Sp"][q], ref["Sp"][q], rtol=10 * TOL32)
+        sp_close(st["Sp"], ref["Sp"], q, 10 * TOL32)

@@ -492,3 +492,20 @@ def test_isosurface_of_a_sphere_is_closed_and_outward(orc):
     assert set(edges.values()) == {2}
     assert orc.isosurface_iso(v) == pytest.approx(np.sqrt(np.mean(v.astype(np.float64) ** 2)) * 3 / np.sqrt(2),
                                                   rel=1e-6)
+
+
+def test_fp64_floor_is_a_rounding_effect(orc):
+    """The oracle's plain and FMA-contracted builds (helpers.fp64_floor) compute the same algorithm
+    in the same order; their fields differ (the reference's zeta interpolation amplifies ulp-level
+    changes) but only at the level of FP64 rounding, far below the FP32 tolerance.  This distance
+    sets the FP64 tolerance of the GPU parity tests."""
+    from fastweavturb_b200.configs import small
+    from helpers import fp64_floor, oracle_inputs
+
+    if not orc.has_fma():
+        pytest.skip("no FMA on this host")
+    w = small(N=32, seed=3, nlev=2, tubes0=2, nodes0=64, sigma0=0.4)
+    p, cl = oracle_inputs(orc, w)
+    floor, vor = fp64_floor(orc, p, cl)
+    assert np.abs(vor).max() > 0
+    assert 0.0 < floor < 1e-10
