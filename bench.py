@@ -461,6 +461,7 @@ def main():
             "config": {"workload": w.name, "N": w.N, "lines": w.ntubes, "nodes": w.nnodes,
                        "sections": counters["sections"], "subsegments": counters["subsegments"],
                        "cell_pairs": counters["pairs"], "accepted_pairs": counters["accepted"],
+                       "pairs_fp64": counters["redone_fp64"],
                        "precision": args.precision,
                        "deposit": "tile-owned cell lists" if args.deposit_mode == 0 else "reference box walk",
                        "l2": "inputs larger than L2 (omega, u, spectra, sub-segment records >> 126 MB)",

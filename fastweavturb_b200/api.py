@@ -348,8 +348,13 @@ class Context:
 
     def set_raster_radius_limit(self, cells):
         """Piece tubes up to this truncation radius (grid spacings) are rasterised once per piece
-        (0: never; negative: the default)."""
+        (0: never, the default; negative: the default)."""
         _check(library().fwt_set_tuning(self._h, 2, float(cells)))
+
+    def set_scatter_radius_limit(self, cells):
+        """FP32 piece tubes up to this truncation radius (grid spacings) are deposited without
+        tiles, with int64 global reductions (0: never; negative: the default, 8)."""
+        _check(library().fwt_set_tuning(self._h, 3, float(cells)))
 
     def counters(self):
         v = np.zeros(7, dtype=np.int64)

@@ -262,6 +262,8 @@ int fwt_destroy(fwt_ctx *h)
     buf_free(c, c->b_aux_acc);
     buf_free(c, c->b_aux_out);
     for (auto &b : c->scratch) buf_free(c, b);
+    buf_free(c, c->b_defer);
+    buf_free(c, c->b_side);
     if (c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return 0;
@@ -471,6 +473,8 @@ int fwt_set_slab(fwt_ctx *h, int z0, int nz)
     // the field buffers change size: the next deposition starts from zero
     buf_free(c, c->b_w);
     buf_free(c, c->b_u);
+    buf_free(c, c->b_side);
+    c->side_dirty = false;
     reset_state(c);
     return 0;
 }
@@ -679,6 +683,10 @@ int fwt_set_tuning(fwt_ctx *h, int key, double value)
     }
     if (key == FWT_TUNE_PIECE_RT_CELLS) {
         c->piece_rt_cells = value;
+        return 0;
+    }
+    if (key == FWT_TUNE_SCATTER_RT_CELLS) {
+        c->scatter_rt_cells = value;
         return 0;
     }
     return fail(FWT_E_ARG, "unknown tuning key");

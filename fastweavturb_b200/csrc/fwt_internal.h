@@ -105,6 +105,13 @@ struct Ctx {
 
     // scratch (centerline set-up, deposition, statistics)
     DevBuf scratch[28];
+    // pairs the FP32 tile kernels defer to FP64 (k_tile_common.cuh): their list, and the int64
+    // fixed-point sums of their contributions (3 x the field), folded into omega by side_fold
+    DevBuf b_defer, b_side;
+    bool side_dirty = false;
+    double defer_per_pair = 0.5;   // deferred pairs per (tile, record) pair of the last tile launch
+    double defer_per_piece = 0.5;  // deferred pairs per piece of the last scatter launch
+    double scatter_rt_cells = -1.0;  // tuning: radius limit of the scatter path in grid spacings (< 0: default)
 
     // state
     bool have_w = false, have_u = false, normalised = false;
@@ -157,6 +164,7 @@ void buf_free(Ctx *c, DevBuf &b);
 
 // centerline set-up + deposition (k_centerline.cu, k_deposit.cu)
 int deposit_lines(Ctx *c, int line_s, int line_e);
+int side_fold(Ctx *c);   // add the deferred pairs' sums into omega (k_deposit_tile.cu)
 
 // spectral (k_spectral.cu)
 int spectral_init(Ctx *c);

@@ -61,6 +61,7 @@ struct CenterlineBatch {
     int64_t npieces = 0;         // chord pieces (piece kernel)
     PieceRec *piece = nullptr;   // npieces FP32 piece records
     bool raster = false;                 // pieces rasterised once (thin tubes), see piece_raster
+    bool scatter = false;                // pieces deposited without tiles (scatter_piece_kernel)
     const int64_t *ras_off = nullptr;    // piece -> first rasterised point (npieces + 1)
     const uint32_t *ras_pts = nullptr;   // chord | x << 3 | y << 12 | z << 21 per accepted point
     const int *rec_map = nullptr;        // record (sub-segment or piece) -> section slot

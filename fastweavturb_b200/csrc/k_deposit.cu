@@ -139,6 +139,10 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
     FWT_TRY(buf_reserve(c, c->b_w, 3 * n3 * real_bytes(c)));
     if (!c->have_w) {
         FWT_CUDA(cudaMemsetAsync(c->b_w.p, 0, 3 * n3 * real_bytes(c), c->stream));
+        if (c->side_dirty) {   // sums left by a deposition that failed part-way
+            FWT_CUDA(cudaMemsetAsync(c->b_side.p, 0, c->b_side.bytes, c->stream));
+            c->side_dirty = false;
+        }
         c->have_w = true;
         c->line_ntf_sum.assign(c->nline, 0);
         c->line_ntf_max.assign(c->nline, 0);
@@ -147,7 +151,8 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
     c->have_u = false;
     c->normalised = false;
     // scratch[19]: [0, 8) accepted points of the box walk, [16, 64) the component range of a
-    // tile deposition, [64, 80) the tile kernels' tallies (accepted pairs, FP64 redone pairs)
+    // tile deposition, [64, 80) the tile kernels' tallies (accepted pairs, FP64 redone pairs),
+    // [96, 100) the error flag of the deferred pairs' FP64 pass
     FWT_TRY(buf_reserve(c, c->scratch[19], 128));
     unsigned long long *d_acc = (unsigned long long *)c->scratch[19].p;
     FWT_CUDA(cudaMemsetAsync(d_acc, 0, 128, c->stream));
@@ -171,6 +176,15 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
     auto rasterised = [&](int l) {
         return thin(l) && c->p.Rtube_ratio * c->p.sigma_ratio * c->sigma[l] <= ras_cells * dxg;
     };
+    // radius limit of the scatter path (FP32 piece lines without tiles): fwt_set_tuning, else
+    // FWT_SCATTER_RT_CELLS, else the default
+    const char *senv = std::getenv("FWT_SCATTER_RT_CELLS");
+    const double sca_cells =
+        c->scatter_rt_cells >= 0.0 ? c->scatter_rt_cells : (senv ? std::atof(senv) : kScatterMaxRtCells);
+    auto scattered = [&](int l) {
+        return thin(l) && c->p.precision == 32 && !rasterised(l) &&
+               c->p.Rtube_ratio * c->p.sigma_ratio * c->sigma[l] <= sca_cells * dxg;
+    };
     int la = line_s - 1;
     while (la < line_e) {
         // batch: consecutive lines up to the node cap, ending after a filtered line and where
@@ -182,7 +196,9 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
             ++lb;
             if (c->if_filter[lb - 1]) break;
             if (lb < line_e && nodes + c->npoint[lb] > cap) break;
-            if (lb < line_e && (thin(lb) != thin(la) || rasterised(lb) != rasterised(la))) break;
+            if (lb < line_e && (thin(lb) != thin(la) || rasterised(lb) != rasterised(la) ||
+                                scattered(lb) != scattered(la)))
+                break;
         }
         const BatchRecords mode =
             !tile_path ? BatchRecords::Walk : (thin(la) ? BatchRecords::Pieces : BatchRecords::SubSeg);
@@ -190,6 +206,7 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
             std::fprintf(stderr, "libfwt: batch lines %d..%d records %d\n", la + 1, lb, (int)mode);
         CenterlineBatch B;
         B.raster = mode == BatchRecords::Pieces && rasterised(la);
+        B.scatter = mode == BatchRecords::Pieces && scattered(la);
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
@@ -214,16 +231,20 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
             FWT_TRY(launch_walk(c, B, d_acc));
         } else {
             int64_t np_ = 0;
-            if (mode == BatchRecords::Pieces) FWT_TRY(launch_piece(c, B, &np_));
+            if (mode == BatchRecords::Pieces && B.scatter) FWT_TRY(launch_scatter(c, B));
+            else if (mode == BatchRecords::Pieces) FWT_TRY(launch_piece(c, B, &np_));
             else FWT_TRY(launch_tile(c, B, &np_));
             pairs += np_;
         }
         if (c->if_filter[lb - 1]) {
+            // the filter acts on the whole field deposited so far
+            FWT_TRY(side_fold(c));
             const double kc = std::ceil(4.0 / c->sigma[lb - 1]);
             FWT_TRY(spectral_filter(c, kc));
         }
         la = lb;
     }
+    FWT_TRY(side_fold(c));
     c->counters[0] = line_e - line_s + 1;
     c->counters[1] = sections;
     c->counters[2] = subsegs;

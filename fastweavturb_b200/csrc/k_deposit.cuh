@@ -221,7 +221,7 @@ __device__ __forceinline__ void redo_locate(const RedoCtx &R, uint32_t rec, int 
 // false: the FP32 tests accepted the pair.  decide = true: an FP32 plane test fell within its
 // rounding bound of zero, and the reference's FP64 tests (tube.f90:806-818) decide; a rejected
 // pair contributes nothing.  Returns 1 (accepted), 0 (rejected) or -1 (fixed-point overflow).
-static __device__ __noinline__ int redo_pair_f64(const RedoCtx &R, uint32_t rec, int ch, bool decide, int gx, int gy,
+__device__ __forceinline__ int redo_pair_f64(const RedoCtx &R, uint32_t rec, int ch, bool decide, int gx, int gy,
                                                  int gz, long long q[3])
 {
     q[0] = q[1] = q[2] = 0;
@@ -269,7 +269,7 @@ __device__ __forceinline__ float plane_eps(const float off[3], const int ext[3],
 }
 
 // Curved-branch amplification |1/(1 - kappa rho cos theta)| (tube.f90:876-879) above which an
-// FP32 evaluation cannot hold 1e-5: such pairs are redone in FP64 by redo_pair_f64.
+// FP32 evaluation cannot hold 1e-5: such pairs are evaluated in FP64 (redo_pair_f64).
 constexpr float kRedoCond = 4.0f;
 
 // FP32 view of one sub-segment, local to its start point ci0 and to a grid-index origin.
@@ -671,14 +671,21 @@ __device__ __forceinline__ void rec_vorticity(const RecT &R, float d0x, float d0
 int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc);
 int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out);
 int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out);
+int launch_scatter(Ctx *c, const CenterlineBatch &B);
 
 // Lines whose truncation radius Rtube_ratio * sigma_max is at most this many grid spacings go
 // through the piece kernel; thicker tubes through the sub-segment kernel, whose analytic
 // row intervals skip most of a large box.
 constexpr double kPieceMaxRtCells = 8.0;
-// Piece lines whose truncation radius is at most this many grid spacings have their pieces
-// rasterised once (piece_raster) instead of searched in every tile: a chord then accepts only a
-// few points, and the per-tile search dominated their cost.
-constexpr double kRasterMaxRtCells = 2.5;
+// Piece lines whose truncation radius is at most this many grid spacings can have their pieces
+// rasterised once (piece_raster) instead of searched in every tile.  Off by default: on the
+// 1024^3 workload the raster pass plus the per-tile filtering of its point lists took 1.3x
+// (radius 1.9 grid spacings) and 2.4x (3.8) the time of the per-tile search; it stays available
+// through fwt_set_tuning.
+constexpr double kRasterMaxRtCells = 0.0;
+// Piece lines whose truncation radius is at most this many grid spacings are deposited without
+// tiles (scatter_piece_kernel, FP32 only): each piece is searched once and its contributions
+// added with int64 global reductions, instead of once in every tile its box meets.
+constexpr double kScatterMaxRtCells = 8.0;
 
 }  // namespace fwt

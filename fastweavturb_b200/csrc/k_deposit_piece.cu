@@ -29,6 +29,7 @@
 namespace fwt {
 
 constexpr int kPieceMax = 8;   // chords per piece
+constexpr int kScatterMaxOff = 254;   // piece-frame offsets of the scatter kernel's 8-bit candidate codes
 
 struct __align__(16) PieceRec {
     float off[3], dx;       // mesh point at box_lo minus the origin o (the piece's first sample)
@@ -202,6 +203,7 @@ __global__ void __launch_bounds__(128, 3) piece_build_kernel(
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         if (bhi[k] - blo[k] > 1023) atomicOr(err, 8);
+        if (bhi[k] - blo[k] > kScatterMaxOff) atomicOr(err, 64);   // too wide for the scatter kernel
         R.box_lo[k] = blo[k];
         R.box_hi[k] = bhi[k];
         // mesh coordinate of the 1-based unwrapped index box_lo: (i - 1) dx + xstart
@@ -333,18 +335,13 @@ struct PBox {
     int pad[3];
 };
 
-// Rows of one chord's box clipped to the tile, along the axis best aligned with the chord; the
-// box is in offsets from the piece's box origin (the piece kernel's rx, ry, rz).
-// The rows of a column (fixed offset along c = (axis+2)%3) are those inside the projection
-// along the axis of the part of chord j's cylinder that the chord can accept: points
-// S_j + t n + v with |v| < Rtube, v . n = 0 and 0 <= t < l + Rtube tan(theta) (theta: the
-// angle between planes j and j + 1; plane j + 1 passes through S_j + l n).  That projection is
-// the projected disk (semi-axes Rtube across n_bc and Rtube |n_a| along it) swept along n_bc,
-// inside the disk's ellipse about the sweep's midpoint scaled by 1 + sweep / (2 minor axis).
-constexpr int kMaxCol = 16;   // a tile is at most 16 points wide
+// Rows of one chord's box (clipped to the tile in the tile kernel, whole in the scatter kernel),
+// along the axis best aligned with the chord; the box is in offsets from the piece's box origin
+// (the kernels' rx, ry, rz).
+constexpr int kMaxCol = 16;   // columns, and rows per column, of a per-column row table
 struct ChordRows {          // lane-major (one entry per chord lane): conflict-free stores
-    uint16_t o[3][32];      // clipped box origin
-    uint8_t n[3][32];       // clipped box extent (at most a tile's)
+    uint16_t o[3][32];      // box origin
+    uint8_t n[3][32];       // box extent
     uint8_t axis[32], nb[32];   // walk axis; rows per column (extent along (axis+1)%3)
     uint8_t ncol[32];       // columns with their own row ranges (0: every row of the box)
     uint8_t pad[32];
@@ -355,13 +352,167 @@ struct ChordRows {          // lane-major (one entry per chord lane): conflict-f
     uint16_t col[kMaxCol][32];  // column jc: first row of the column | first b offset << 12
 };
 
+// Row table of chord j of record R over the box [co, co + cnn) (piece-frame offsets, cnn > 0
+// along every axis when nonempty): the walk axis (the one best aligned with the chord), the
+// plane and cylinder coefficients of the row intervals, and where the chord's projected
+// cylinder allows (at most kMaxCol columns of at most kMaxCol rows) per-column row ranges.
+// The rows of a column (fixed offset along c = (axis+2)%3) are those inside the projection
+// along the axis of the part of chord j's cylinder that the chord can accept: points
+// S_j + t n + v with |v| < Rtube, v . n = 0 and 0 <= t < l + Rtube tan(theta) (theta: the
+// angle between planes j and j + 1; plane j + 1 passes through S_j + l n).  That projection is
+// the projected disk (semi-axes Rtube across n_bc and Rtube |n_a| along it) swept along n_bc,
+// inside the disk's ellipse about the sweep's midpoint scaled by 1 + sweep / (2 minor axis).
+// Writes lane `lane` of C; returns the number of rows.
+__device__ __forceinline__ int chord_row_table(const PieceRec &R, int j, const int co[3], const int cnn[3],
+                                               bool nonempty, ChordRows &C, int lane)
+{
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        C.o[d][lane] = (uint16_t)co[d];
+        C.n[d][lane] = (uint8_t)cnn[d];
+    }
+    int nrows = 0;
+    const float4 pj = R.pl[j], pk = R.pl[j + 1];
+    const float ax = fabsf(pj.x), ay = fabsf(pj.y), az = fabsf(pj.z);
+    const int a = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+    C.axis[lane] = (uint8_t)a;
+    const int nbv = a == 0 ? cnn[1] : (a == 1 ? cnn[2] : cnn[0]);
+    const int ncv = a == 0 ? cnn[2] : (a == 1 ? cnn[0] : cnn[1]);
+    C.nb[lane] = (uint8_t)nbv;
+    C.rnb[lane] = nonempty ? 1.000001f / (float)nbv : 0.0f;
+    const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
+    const float tb = a == 0 ? pk.x : (a == 1 ? pk.y : pk.z);
+    // the bounds below carry margins of 0.05 point and 1 %: approximate reciprocals
+    // (a few ulp) are ample, and the reference's tests decide every candidate
+    C.isa[lane] = __fdividef(1.0f, R.dx * ta);
+    C.isb[lane] = fabsf(tb) > 0.05f ? __fdividef(1.0f, R.dx * tb) : 0.0f;
+    const float q2 = R.dx * R.dx * (1.0f - ta * ta);
+    C.q2[lane] = q2 > 0.01f * R.dx * R.dx ? q2 : 0.0f;
+    C.i2q[lane] = q2 > 0.01f * R.dx * R.dx ? __fdividef(0.5f, q2) : 0.0f;
+    C.ncol[lane] = 0;
+    nrows = nonempty ? nbv * ncv : 0;
+    const float cth = pj.x * pk.x + pj.y * pk.y + pj.z * pk.z;
+    if (nonempty && ncv <= kMaxCol && nbv <= kMaxCol && cth > 0.5f) {
+        // the chord's sweep and the ellipse of its cross-section, in (b, c)
+        const float4 oj = R.po[j], ok1 = R.po[j + 1];
+        const float lx_ = oj.x - ok1.x, ly_ = oj.y - ok1.y, lz_ = oj.z - ok1.z;
+        const float rt = sqrtf(R.chq[j].y);
+        const float sweep = sqrtf(lx_ * lx_ + ly_ * ly_ + lz_ * lz_) +
+                            __fdividef(rt * sqrtf(fmaxf(1.0f - cth * cth, 0.0f)), cth);
+        const int b = a == 2 ? 0 : a + 1, cc = a == 0 ? 2 : a - 1;
+        const float nb_ = b == 0 ? pj.x : (b == 1 ? pj.y : pj.z);
+        const float nc_ = cc == 0 ? pj.x : (cc == 1 ? pj.y : pj.z);
+        const float nbc = sqrtf(nb_ * nb_ + nc_ * nc_);
+        const float inbc = nbc > 1e-4f ? __fdividef(1.0f, nbc) : 0.0f;
+        const float wb = nbc > 1e-4f ? nb_ * inbc : 1.0f, wc = nbc > 1e-4f ? nc_ * inbc : 0.0f;
+        const float Bm = rt * fabsf(ta);
+        const float f = 1.0f + __fdividef(sweep * nbc, 2.0f * Bm);
+        const float Ae = fmaf(f * rt, 1.01f, 0.05f * R.dx), Be = fmaf(f * Bm, 1.01f, 0.05f * R.dx);
+        const float ia2 = __fdividef(1.0f, Ae * Ae), ib2 = __fdividef(1.0f, Be * Be);
+        // centre: S_j + (sweep / 2) n, with S_j = -po[j] (mesh-point offsets times dx)
+        const float sb = -(b == 0 ? oj.x : (b == 1 ? oj.y : oj.z)), sc = -(cc == 0 ? oj.x : (cc == 1 ? oj.y : oj.z));
+        const float Cb = fmaf(0.5f * sweep, nb_, sb), Cc = fmaf(0.5f * sweep, nc_, sc);
+        const int ob = b == 0 ? co[0] : (b == 1 ? co[1] : co[2]);
+        const int oc = cc == 0 ? co[0] : (cc == 1 ? co[1] : co[2]);
+        const float al = fmaf(wc * wc, ia2, wb * wb * ib2);
+        const float cross_ = 2.0f * wb * wc * (ib2 - ia2);
+        const float g2 = fmaf(wb * wb, ia2, wc * wc * ib2);
+        const float i2a = __fdividef(0.5f, al);
+        int rows = 0;
+        const float idx = __fdividef(1.0f, R.dx);
+#pragma unroll 1
+        for (int jc = 0; jc < ncv; ++jc) {
+            const float z = fmaf((float)(oc + jc), R.dx, -Cc);
+            const float be = cross_ * z, ga = fmaf(g2 * z, z, -1.0f);
+            const float disc = fmaf(be, be, -4.0f * al * ga);
+            int jb0 = 0, nrow = 0;
+            if (disc >= 0.0f) {
+                const float sq = sqrtf(disc);
+                const float y1 = (-be - sq) * i2a, y2 = (-be + sq) * i2a;
+                const float u1 = fmaf(Cb + y1, idx, -(float)ob), u2 = fmaf(Cb + y2, idx, -(float)ob);
+                jb0 = max(0, (int)ceilf(fmaxf(u1, -2.0f) - 0.05f));
+                const int jb1 = min(nbv - 1, (int)floorf(fminf(u2, (float)nbv + 1.0f) + 0.05f));
+                nrow = max(0, jb1 - jb0 + 1);
+            }
+            C.col[jc][lane] = (uint16_t)(rows | (jb0 << 12));
+            rows += nrow;
+        }
+        C.ncol[lane] = (uint8_t)ncv;
+        nrows = rows;
+    }
+    return nrows;
+}
+
+// Row rr of chord lane c (chord j of record R, row table C): the row's base point (bx, by, bz)
+// (offsets from the piece's box origin), its axis a and the index interval [i, ihi] along the
+// axis where the row can pass chord j's two planes and its cylinder (with a 0.05-point margin
+// and Rtube^2 widened by 2e-3, far above the FP32 rounding of the bounds).
+__device__ __forceinline__ void chord_row_span(const PieceRec &R, const ChordRows &C, int c, int j, int rr, int &bx,
+                                               int &by, int &bz, int &a, int &i, int &ihi)
+{
+    a = C.axis[c];
+    int jc, jb;
+    if (C.ncol[c] > 0) {
+        // column of row rr: last column whose first row is <= rr (ncol <= 16)
+        jc = 0;
+#pragma unroll
+        for (int step = 8; step > 0; step >>= 1) {
+            const int t = jc + step;
+            if (t < C.ncol[c] && (int)(C.col[t][c] & 0xfffu) <= rr) jc = t;
+        }
+        jb = (int)(C.col[jc][c] >> 12) + (rr - (int)(C.col[jc][c] & 0xfffu));
+    } else {
+        jc = (int)((float)rr * C.rnb[c]);
+        if (jc * C.nb[c] > rr) --jc;
+        jb = rr - jc * C.nb[c];
+    }
+    bx = C.o[0][c] + (a == 0 ? 0 : (a == 1 ? jc : jb));
+    by = C.o[1][c] + (a == 0 ? jb : (a == 1 ? 0 : jc));
+    bz = C.o[2][c] + (a == 0 ? jc : (a == 1 ? jb : 0));
+    const float4 pj = R.pl[j], pk = R.pl[j + 1], oj = R.po[j], ok1 = R.po[j + 1];
+    // row base relative to sample j and to sample j + 1
+    const float ex = fmaf((float)bx, R.dx, oj.x), ey = fmaf((float)by, R.dx, oj.y),
+                ez = fmaf((float)bz, R.dx, oj.z);
+    const float T0 = fmaf(ez, pj.z, fmaf(ey, pj.y, ex * pj.x));
+    const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
+    const int na = a == 0 ? C.n[0][c] : (a == 1 ? C.n[1][c] : C.n[2][c]);
+    float lo = -2.0f, hi = (float)na + 1.0f;
+    const float r0f = -T0 * C.isa[c];          // t_j >= 0
+    if (ta > 0.0f) lo = fmaxf(lo, r0f);
+    else hi = fminf(hi, r0f);
+    if (C.isb[c] != 0.0f) {                     // t_{j+1} < 0
+        const float fx = fmaf((float)bx, R.dx, ok1.x), fy = fmaf((float)by, R.dx, ok1.y),
+                    fz = fmaf((float)bz, R.dx, ok1.z);
+        const float T1 = fmaf(fz, pk.z, fmaf(fy, pk.y, fx * pk.x));
+        const float r1f = -T1 * C.isb[c];
+        if (C.isb[c] > 0.0f) hi = fminf(hi, r1f);
+        else lo = fmaxf(lo, r1f);
+    }
+    if (C.q2[c] > 0.0f) {                       // rho^2 < Rtube^2 about chord line j
+        const float ea = a == 0 ? ex : (a == 1 ? ey : ez);
+        const float e2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
+        const float Q1 = 2.0f * R.dx * (ea - T0 * ta);
+        const float Q0 = e2 - T0 * T0;
+        const float R2w = fmaf(R.chq[j].y, 1.002f, 1e-6f * e2);
+        const float disc = Q1 * Q1 - 4.0f * C.q2[c] * (Q0 - R2w);
+        if (disc < 0.0f) {
+            hi = -3.0f;
+        } else {
+            const float sq = sqrtf(disc);
+            lo = fmaxf(lo, (-Q1 - sq) * C.i2q[c]);
+            hi = fminf(hi, (-Q1 + sq) * C.i2q[c]);
+        }
+    }
+    i = max(0, (int)ceilf(lo - 0.05f));
+    ihi = min(na - 1, (int)floorf(hi + 0.05f));
+}
+
 struct PieceStage {
     PieceRec rec[kPChunk];
     PBox box[kPChunk];
     ChordRows cr;
     uint32_t cq[kPQueue];  // candidates: chord lane (piece << 3 | chord) | x << 5 | y << 9 | z << 12 (tile-local)
     uint32_t q[kPQueue];   // piece | chord << 3 | x << 6 | y << 10 | z << 13 (tile-local) | kPQDecide
-    RedoQueue redo;        // ill-conditioned pairs awaiting their FP64 evaluation
     uint32_t id[kPChunk];  // global record ids of the staged pieces
     uint64_t bar;
     uint64_t pad;
@@ -535,21 +686,23 @@ __global__ void __launch_bounds__(128) piece_raster_kernel(const PieceRec *__res
 
 // Evaluate the first `cnt` queued (point, chord) pairs, one per lane, into the tile cells;
 // pairs whose curved-branch amplification exceeds kRedoCond, and pairs left to the FP64 tests
-// (kPQDecide), go to the redo queue instead.
+// (kPQDecide), are deferred to FP64 (DeferList) instead.  In the emit-only pass nothing is
+// added and only the deferred pairs are listed again.
 template <bool General, bool F64>
 __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAccN], int lane, int cnt, int &qn,
-                                             int &rn, unsigned &nacc, float fscale, float fmaxq, int *__restrict__ err,
-    const RedoCtx &redo, int x0, int y0, int z0)
+                                             unsigned &nacc, float fscale, float fmaxq, int *__restrict__ err,
+                                             const RedoCtx &redo, const DeferList &D, int x0, int y0, int z0)
 {
     bool flag = false, ok64 = false, counted = false;
-    uint32_t rrec = 0, rcode = 0;
+    uint32_t rrec = 0;
+    int lx = 0, ly = 0, lz = 0;
     if (F64 && lane < cnt) {
         // FP64 path: the candidate passed the widened FP32 tests; the reference's FP64 tests
         // decide, at the point's index in the chord's own box (the piece frame differs from it by
         // whole periods)
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 7u), j = (int)((e >> 3) & 7u);
-        const int lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)((e >> 13) & 7u);
+        lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)((e >> 13) & 7u);
         const PBox &B = S.box[k];
         const PieceRec &R = S.rec[k];
         int slot, jj;
@@ -563,12 +716,11 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
     } else if (lane < cnt) {
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 7u), j = (int)((e >> 3) & 7u);
-        const int lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)((e >> 13) & 7u);
+        lx = (int)((e >> 6) & 15u), ly = (int)((e >> 10) & 7u), lz = (int)((e >> 13) & 7u);
         if (e & kPQDecide) {
             flag = true;
-            rrec = (S.id[k] & ((1u << 26) - 1u)) | ((uint32_t)j << 26) | kRedoDecide;
-            rcode = redo_code(lx, ly, lz);
-        } else {
+            rrec = (S.id[k] & ((1u << 26) - 1u)) | ((uint32_t)j << 26) | kDeferDecide;
+        } else if (General || !D.emit_only) {
             counted = true;
             const PBox &B = S.box[k];
             const PieceRec &R = S.rec[k];
@@ -583,8 +735,7 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
             flag = General && !(cond <= kRedoCond);
             if (flag) {
                 rrec = (S.id[k] & ((1u << 26) - 1u)) | ((uint32_t)j << 26);
-                rcode = redo_code(lx, ly, lz);
-            } else {
+            } else if (!D.emit_only) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     float sv = vv[d] * fscale;
@@ -597,11 +748,11 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
             }
         }
     }
-    if constexpr (F64) nacc += __popc(__ballot_sync(0xffffffffu, ok64));
-    else nacc += __popc(__ballot_sync(0xffffffffu, counted));
-    if constexpr (!F64) {
-        redo_push(S.redo, lane, flag, rrec, rcode, rn);
-        if (rn >= 32) redo_drain(S.redo, redo, acc, lane, 32, rn, x0, y0, z0, err);
+    if constexpr (F64) {
+        nacc += __popc(__ballot_sync(0xffffffffu, ok64));
+    } else {
+        nacc += __popc(__ballot_sync(0xffffffffu, counted));
+        defer_push(D, lane, flag, rrec, x0 + lx, y0 + ly, z0 + lz);
     }
     __syncwarp();
     const int rem = qn - cnt;
@@ -617,8 +768,9 @@ __device__ __forceinline__ void drain_pieces(PieceStage &S, long long (*acc)[kAc
 // queue when it holds 32 pairs.
 template <bool General, bool F64>
 __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[kAccN], int lane, int cnt, int &cn,
-                                                int &qn, int &rn, unsigned &nacc, float fscale, float fmaxq,
-                                                int *__restrict__ err, const RedoCtx &redo, int x0, int y0, int z0)
+                                                int &qn, unsigned &nacc, float fscale, float fmaxq,
+                                                int *__restrict__ err, const RedoCtx &redo, const DeferList &D, int x0,
+                                                int y0, int z0)
 {
     bool ok = false;
     uint32_t code = 0u;
@@ -642,7 +794,7 @@ __device__ __forceinline__ void test_candidates(PieceStage &S, long long (*acc)[
     if (lane < rem) S.cq[lane] = keep;
     __syncwarp();
     cn = rem;
-    if (qn >= 32) drain_pieces<General, F64>(S, acc, lane, 32, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+    if (qn >= 32) drain_pieces<General, F64>(S, acc, lane, 32, qn, nacc, fscale, fmaxq, err, redo, D, x0, y0, z0);
 }
 
 // One CTA per tile.  Each warp claims chunks of kPChunk pieces (32 chords), stages their
@@ -655,8 +807,8 @@ template <bool General, bool Accumulate, bool F64, bool Raster>
 __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel(
     const PieceRec *__restrict__ rec, int N, int ntx, int nty, int tz0, const int64_t *__restrict__ tile_off,
     const uint32_t *__restrict__ list, double scale, void *__restrict__ wx, void *__restrict__ wy,
-    void *__restrict__ wz, int *__restrict__ err, const RedoCtx redo, const int64_t *__restrict__ ras_off,
-    const uint32_t *__restrict__ ras_pts)
+    void *__restrict__ wz, int *__restrict__ err, const RedoCtx redo, const DeferList D,
+    const int64_t *__restrict__ ras_off, const uint32_t *__restrict__ ras_pts)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     long long(*acc)[kAccN] = reinterpret_cast<long long(*)[kAccN]>(dsm);
@@ -679,7 +831,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
     if constexpr (F64)
         tile_acc_init_f64<Accumulate>(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, zs, zlim, (const double *)wx,
                                       (const double *)wy, (const double *)wz);
-    else
+    else if (!D.emit_only)
         tile_acc_init<Accumulate>(acc, N, x0, y0, z0, zs, zlim, scale, (const float *)wx, (const float *)wy,
                                   (const float *)wz);
     __syncthreads();
@@ -690,7 +842,6 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
     uint32_t phase = 0;
     bool failed = false;
     int qn = 0;
-    int rn = 0;   // queued FP64 redo pairs of this warp (warp-uniform)
     unsigned nacc = 0;   // pairs evaluated by this warp (warp-uniform)
     for (int ch = warp; ch < nchunks && !failed;) {
         const int64_t base = c0 + (int64_t)ch * kPChunk;
@@ -751,7 +902,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
                 qn += __popc(bal);
                 __syncwarp();
                 if (qn >= 32)
-                    drain_pieces<General, F64>(S, acc, lane, 32, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+                    drain_pieces<General, F64>(S, acc, lane, 32, qn, nacc, fscale, fmaxq, err, redo, D, x0, y0, z0);
             }
         } else {
             // lane = (piece k, chord j): chord j's box clipped to the tile and its rows
@@ -771,78 +922,9 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
                         const int lo = max(tlo, unpack3(blo, d)), hi = min(thi, unpack3(bhi, d));
                         co[d] = lo;
                         cnn[d] = max(0, hi - lo + 1);
-                        C.o[d][lane] = (uint16_t)lo;
-                        C.n[d][lane] = (uint8_t)cnn[d];
                         nonempty = nonempty && cnn[d] > 0;
                     }
-                    const float4 pj = R.pl[j], pk = R.pl[j + 1];
-                    const float ax = fabsf(pj.x), ay = fabsf(pj.y), az = fabsf(pj.z);
-                    const int a = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
-                    C.axis[lane] = (uint8_t)a;
-                    const int nbv = a == 0 ? cnn[1] : (a == 1 ? cnn[2] : cnn[0]);
-                    const int ncv = a == 0 ? cnn[2] : (a == 1 ? cnn[0] : cnn[1]);
-                    C.nb[lane] = (uint8_t)nbv;
-                    C.rnb[lane] = nonempty ? 1.000001f / (float)nbv : 0.0f;
-                    const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
-                    const float tb = a == 0 ? pk.x : (a == 1 ? pk.y : pk.z);
-                    // the bounds below carry margins of 0.05 point and 1 %: approximate reciprocals
-                    // (a few ulp) are ample, and the reference's tests decide every candidate
-                    C.isa[lane] = __fdividef(1.0f, R.dx * ta);
-                    C.isb[lane] = fabsf(tb) > 0.05f ? __fdividef(1.0f, R.dx * tb) : 0.0f;
-                    const float q2 = R.dx * R.dx * (1.0f - ta * ta);
-                    C.q2[lane] = q2 > 0.01f * R.dx * R.dx ? q2 : 0.0f;
-                    C.i2q[lane] = q2 > 0.01f * R.dx * R.dx ? __fdividef(0.5f, q2) : 0.0f;
-                    C.ncol[lane] = 0;
-                    nrows = nonempty ? nbv * ncv : 0;
-                    const float cth = pj.x * pk.x + pj.y * pk.y + pj.z * pk.z;
-                    if (nonempty && ncv <= kMaxCol && cth > 0.5f) {
-                        // the chord's sweep and the ellipse of its cross-section, in (b, c)
-                        const float4 oj = R.po[j], ok1 = R.po[j + 1];
-                        const float lx_ = oj.x - ok1.x, ly_ = oj.y - ok1.y, lz_ = oj.z - ok1.z;
-                        const float rt = sqrtf(R.chq[j].y);
-                        const float sweep = sqrtf(lx_ * lx_ + ly_ * ly_ + lz_ * lz_) +
-                                            __fdividef(rt * sqrtf(fmaxf(1.0f - cth * cth, 0.0f)), cth);
-                        const int b = a == 2 ? 0 : a + 1, cc = a == 0 ? 2 : a - 1;
-                        const float nb_ = b == 0 ? pj.x : (b == 1 ? pj.y : pj.z);
-                        const float nc_ = cc == 0 ? pj.x : (cc == 1 ? pj.y : pj.z);
-                        const float nbc = sqrtf(nb_ * nb_ + nc_ * nc_);
-                        const float inbc = nbc > 1e-4f ? __fdividef(1.0f, nbc) : 0.0f;
-                        const float wb = nbc > 1e-4f ? nb_ * inbc : 1.0f, wc = nbc > 1e-4f ? nc_ * inbc : 0.0f;
-                        const float Bm = rt * fabsf(ta);
-                        const float f = 1.0f + __fdividef(sweep * nbc, 2.0f * Bm);
-                        const float Ae = fmaf(f * rt, 1.01f, 0.05f * R.dx), Be = fmaf(f * Bm, 1.01f, 0.05f * R.dx);
-                        const float ia2 = __fdividef(1.0f, Ae * Ae), ib2 = __fdividef(1.0f, Be * Be);
-                        // centre: S_j + (sweep / 2) n, with S_j = -po[j] (mesh-point offsets times dx)
-                        const float sb = -(b == 0 ? oj.x : (b == 1 ? oj.y : oj.z)), sc = -(cc == 0 ? oj.x : (cc == 1 ? oj.y : oj.z));
-                        const float Cb = fmaf(0.5f * sweep, nb_, sb), Cc = fmaf(0.5f * sweep, nc_, sc);
-                        const int ob = b == 0 ? co[0] : (b == 1 ? co[1] : co[2]);
-                        const int oc = cc == 0 ? co[0] : (cc == 1 ? co[1] : co[2]);
-                        const float al = fmaf(wc * wc, ia2, wb * wb * ib2);
-                        const float cross_ = 2.0f * wb * wc * (ib2 - ia2);
-                        const float g2 = fmaf(wb * wb, ia2, wc * wc * ib2);
-                        const float i2a = __fdividef(0.5f, al);
-                        int rows = 0;
-                        const float idx = __fdividef(1.0f, R.dx);
-    #pragma unroll 1
-                        for (int jc = 0; jc < ncv; ++jc) {
-                            const float z = fmaf((float)(oc + jc), R.dx, -Cc);
-                            const float be = cross_ * z, ga = fmaf(g2 * z, z, -1.0f);
-                            const float disc = fmaf(be, be, -4.0f * al * ga);
-                            int jb0 = 0, nrow = 0;
-                            if (disc >= 0.0f) {
-                                const float sq = sqrtf(disc);
-                                const float y1 = (-be - sq) * i2a, y2 = (-be + sq) * i2a;
-                                const float u1 = fmaf(Cb + y1, idx, -(float)ob), u2 = fmaf(Cb + y2, idx, -(float)ob);
-                                jb0 = max(0, (int)ceilf(fmaxf(u1, -2.0f) - 0.05f));
-                                const int jb1 = min(nbv - 1, (int)floorf(fminf(u2, (float)nbv + 1.0f) + 0.05f));
-                                nrow = max(0, jb1 - jb0 + 1);
-                            }
-                            C.col[jc][lane] = (uint16_t)(rows | (jb0 << 12));
-                            rows += nrow;
-                        }
-                        C.ncol[lane] = (uint8_t)ncv;
-                        nrows = rows;
-                    }
+                    nrows = chord_row_table(R, j, co, cnn, nonempty, C, lane);
                 }
             }
             int incl = nrows;
@@ -875,65 +957,11 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
                     const ChordRows &C = S.cr;
                     const PieceRec &R = S.rec[k];
                     const PBox &B = S.box[k];
-                    a = C.axis[c];
-                    const int rr = r - rc;
-                    int jc, jb;
-                    if (C.ncol[c] > 0) {
-                        // column of row rr: last column whose first row is <= rr (ncol <= 16)
-                        jc = 0;
-    #pragma unroll
-                        for (int step = 8; step > 0; step >>= 1) {
-                            const int t = jc + step;
-                            if (t < C.ncol[c] && (int)(C.col[t][c] & 0xfffu) <= rr) jc = t;
-                        }
-                        jb = (int)(C.col[jc][c] >> 12) + (rr - (int)(C.col[jc][c] & 0xfffu));
-                    } else {
-                        jc = (int)((float)rr * C.rnb[c]);
-                        if (jc * C.nb[c] > rr) --jc;
-                        jb = rr - jc * C.nb[c];
-                    }
-                    const int bx = C.o[0][c] + (a == 0 ? 0 : (a == 1 ? jc : jb));
-                    const int by = C.o[1][c] + (a == 0 ? jb : (a == 1 ? 0 : jc));
-                    const int bz = C.o[2][c] + (a == 0 ? jc : (a == 1 ? jb : 0));
+                    int bx, by, bz;
+                    chord_row_span(R, C, c, j, r - rc, bx, by, bz, a, i, ihi);
                     lx = bx - B.dl[0];
                     ly = by - B.dl[1];
                     lz = bz - B.dl[2];
-                    const float4 pj = R.pl[j], pk = R.pl[j + 1], oj = R.po[j], ok1 = R.po[j + 1];
-                    // row base relative to sample j and to sample j + 1
-                    const float ex = fmaf((float)bx, R.dx, oj.x), ey = fmaf((float)by, R.dx, oj.y),
-                                ez = fmaf((float)bz, R.dx, oj.z);
-                    const float T0 = fmaf(ez, pj.z, fmaf(ey, pj.y, ex * pj.x));
-                    const float ta = a == 0 ? pj.x : (a == 1 ? pj.y : pj.z);
-                    const int na = a == 0 ? C.n[0][c] : (a == 1 ? C.n[1][c] : C.n[2][c]);
-                    float lo = -2.0f, hi = (float)na + 1.0f;
-                    const float r0f = -T0 * C.isa[c];          // t_j >= 0
-                    if (ta > 0.0f) lo = fmaxf(lo, r0f);
-                    else hi = fminf(hi, r0f);
-                    if (C.isb[c] != 0.0f) {                     // t_{j+1} < 0
-                        const float fx = fmaf((float)bx, R.dx, ok1.x), fy = fmaf((float)by, R.dx, ok1.y),
-                                    fz = fmaf((float)bz, R.dx, ok1.z);
-                        const float T1 = fmaf(fz, pk.z, fmaf(fy, pk.y, fx * pk.x));
-                        const float r1f = -T1 * C.isb[c];
-                        if (C.isb[c] > 0.0f) hi = fminf(hi, r1f);
-                        else lo = fmaxf(lo, r1f);
-                    }
-                    if (C.q2[c] > 0.0f) {                       // rho^2 < Rtube^2 about chord line j
-                        const float ea = a == 0 ? ex : (a == 1 ? ey : ez);
-                        const float e2 = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-                        const float Q1 = 2.0f * R.dx * (ea - T0 * ta);
-                        const float Q0 = e2 - T0 * T0;
-                        const float R2w = fmaf(R.chq[j].y, 1.002f, 1e-6f * e2);
-                        const float disc = Q1 * Q1 - 4.0f * C.q2[c] * (Q0 - R2w);
-                        if (disc < 0.0f) {
-                            hi = -3.0f;
-                        } else {
-                            const float sq = sqrtf(disc);
-                            lo = fmaxf(lo, (-Q1 - sq) * C.i2q[c]);
-                            hi = fminf(hi, (-Q1 + sq) * C.i2q[c]);
-                        }
-                    }
-                    i = max(0, (int)ceilf(lo - 0.05f));
-                    ihi = min(na - 1, (int)floorf(hi + 0.05f));
                 }
                 while (__any_sync(0xffffffffu, i <= ihi)) {
                     const bool has = i <= ihi;
@@ -947,27 +975,231 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
                     if (has) S.cq[cn + __popc(bal & ((1u << lane) - 1u))] = code;
                     cn += __popc(bal);
                     __syncwarp();
-                    if (cn >= 32) test_candidates<General, F64>(S, acc, lane, 32, cn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+                    if (cn >= 32) test_candidates<General, F64>(S, acc, lane, 32, cn, qn, nacc, fscale, fmaxq, err, redo, D, x0, y0, z0);
                 }
             }
-            if (cn > 0) test_candidates<General, F64>(S, acc, lane, cn, cn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+            if (cn > 0) test_candidates<General, F64>(S, acc, lane, cn, cn, qn, nacc, fscale, fmaxq, err, redo, D, x0, y0, z0);
         }
-        if (qn > 0) drain_pieces<General, F64>(S, acc, lane, qn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+        if (qn > 0) drain_pieces<General, F64>(S, acc, lane, qn, qn, nacc, fscale, fmaxq, err, redo, D, x0, y0, z0);
         __syncwarp();   // the warp's stage is reused by its next chunk
         int nxt = 0;
         if (lane == 0) nxt = atomicAdd(&next_chunk, 1);
         ch = __shfl_sync(0xffffffffu, nxt, 0);
     }
-    if constexpr (!F64)
-        if (rn > 0) redo_drain(S.redo, redo, acc, lane, rn, rn, x0, y0, z0, err);
     if (failed && lane == 0) atomicOr(err, 2);
-    if (lane == 0 && redo.tally) atomicAdd(redo.tally, (unsigned long long)nacc);
+    if (lane == 0 && redo.tally && !D.emit_only) atomicAdd(redo.tally, (unsigned long long)nacc);
     __syncthreads();
     if constexpr (F64)
         tile_epilogue_f64(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, zs, zlim, (double *)wx, (double *)wy,
                           (double *)wz);
-    else
+    else if (!D.emit_only)
         tile_epilogue(acc, N, x0, y0, z0, zs, zlim, scale, (float *)wx, (float *)wy, (float *)wz);
+}
+
+// ------------------------------------------------------------------------------ scatter
+// Thin tubes without tiles.  The tile kernels pay, for every (tile, piece) pair, a record copy
+// and every chord's set-up within that tile; a thin chord accepts a few points and its box
+// meets two to six tiles, so that overhead outweighs the evaluations.  The scatter kernel takes
+// each piece once: a warp stages kPChunk pieces (32 chords, one per lane), each lane builds its
+// chord's row table over the chord's whole box (chord_row_table), the rows are spread over the
+// lanes (chord_row_span), their candidates tested 32 at a time (piece_classify) and the accepted
+// pairs evaluated 32 at a time; each contribution is added as int64 fixed point into the side
+// accumulator with global reductions.  Integer sums do not depend on the order, so the field is
+// deterministic; side_fold adds the sums into omega after the batch loop.  Pairs for the FP64
+// tests or arithmetic are deferred as in the tile kernels.
+constexpr int kScatterWarps = 8;
+constexpr uint32_t kSQDecide = 1u << 31;     // queued pair left to the reference's FP64 tests
+struct ScatterStage {
+    PieceRec rec[kPChunk];
+    ChordRows cr;
+    uint32_t cq[kPQueue];   // candidates: chord lane | x << 5 | y << 13 | z << 21 (offsets from the piece's box origin)
+    uint32_t q[kPQueue];    // accepted pairs: the same | kSQDecide
+};
+constexpr size_t kScatterSmem = sizeof(ScatterStage) * kScatterWarps;
+
+// Test the first cnt candidates (piece_classify), queue the accepted pairs and those left to
+// the FP64 tests, and drop the candidates.
+__device__ __forceinline__ void scatter_test(ScatterStage &S, int lane, int cnt, int &cn, int &qn)
+{
+    bool ok = false;
+    uint32_t code = 0u;
+    if (lane < cnt) {
+        const uint32_t e = S.cq[lane];
+        const int c = (int)(e & 31u);
+        const int cls = piece_classify(S.rec[c >> 3], c & 7, (int)((e >> 5) & 255u), (int)((e >> 13) & 255u),
+                                       (int)((e >> 21) & 255u));
+        ok = cls != 0;
+        code = e | (cls == 2 ? kSQDecide : 0u);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+    if (ok) S.q[qn + __popc(bal & ((1u << lane) - 1u))] = code;
+    qn += __popc(bal);
+    const int rem = cn - cnt;
+    const uint32_t keep = lane < rem ? S.cq[cnt + lane] : 0u;
+    __syncwarp();
+    if (lane < rem) S.cq[lane] = keep;
+    __syncwarp();
+    cn = rem;
+}
+
+// Evaluate the first cnt queued pairs, one per lane, and add them into the side accumulator;
+// the pairs left to FP64 (kSQDecide, or a curved-branch amplification above kRedoCond) are
+// deferred.  Points outside the context's planes (a z-slab context) are dropped.
+template <bool General>
+__device__ __forceinline__ void scatter_drain(ScatterStage &S, int lane, int cnt, int &qn, int64_t p0, int N, int zs,
+                                              int nz, float fscale, unsigned long long *__restrict__ side, size_t n3,
+                                              int *__restrict__ err, const DeferList &D, unsigned long long &nacc)
+{
+    bool flag = false, counted = false;
+    uint32_t rrec = 0;
+    int gx = 0, gy = 0, gz = 0;
+    if (lane < cnt) {
+        const uint32_t e = S.q[lane];
+        const int c = (int)(e & 31u), k = c >> 3, j = c & 7;
+        const int rx = (int)((e >> 5) & 255u), ry = (int)((e >> 13) & 255u), rz = (int)((e >> 21) & 255u);
+        const PieceRec &R = S.rec[k];
+        gx = (R.box_lo[0] - 1 + rx) % N;
+        gy = (R.box_lo[1] - 1 + ry) % N;
+        gz = (R.box_lo[2] - 1 + rz) % N;
+        gx += gx < 0 ? N : 0;
+        gy += gy < 0 ? N : 0;
+        gz += gz < 0 ? N : 0;
+        const bool inslab = gz >= zs && gz < zs + nz;
+        const uint32_t id = ((uint32_t)(p0 + k) & ((1u << 26) - 1u)) | ((uint32_t)j << 26);
+        if (inslab && (e & kSQDecide)) {
+            flag = true;
+            rrec = id | kDeferDecide;
+        } else if (inslab && (General || !D.emit_only)) {
+            counted = true;
+            const float4 cp = R.po[j], cq = R.chq[j], pn = R.pl[j];
+            const float ex = fmaf((float)rx, R.dx, cp.x);
+            const float ey = fmaf((float)ry, R.dx, cp.y);
+            const float ez = fmaf((float)rz, R.dx, cp.z);
+            const float t0 = fmaf(ez, pn.z, fmaf(ey, pn.y, ex * pn.x));
+            float vv[3], cond;
+            vort_w<General, true>(R, ex, ey, ez, cp.w, t0 * cq.x, cq.y, vv, cond);
+            flag = General && !(cond <= kRedoCond);
+            if (flag) {
+                rrec = id;
+            } else if (!D.emit_only) {
+                const size_t g = (size_t)gx + (size_t)N * ((size_t)gy + (size_t)N * (size_t)(gz - zs));
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    float sv = vv[d] * fscale;
+                    if (!(fabsf(sv) < 4.0e18f)) {
+                        atomicOr(err, 4);
+                        sv = sv != sv ? 0.0f : copysignf(4.0e18f, sv);
+                    }
+                    atomicAdd(side + (size_t)d * n3 + g, (unsigned long long)__float2ll_rn(sv));
+                }
+            }
+        }
+    }
+    nacc += (unsigned long long)__popc(__ballot_sync(0xffffffffu, counted));
+    defer_push(D, lane, flag, rrec, gx, gy, gz);
+    __syncwarp();
+    const int rem = qn - cnt;
+    const uint32_t keep = lane < rem ? S.q[cnt + lane] : 0u;
+    __syncwarp();
+    if (lane < rem) S.q[lane] = keep;
+    __syncwarp();
+    qn = rem;
+}
+
+template <bool General>
+__global__ void __launch_bounds__(kScatterWarps * 32, 3) scatter_piece_kernel(
+    const PieceRec *__restrict__ rec, int64_t npieces, int N, int zs, int nz, float fscale,
+    unsigned long long *__restrict__ side, size_t n3, int *__restrict__ err, const DeferList D,
+    unsigned long long *__restrict__ tally)
+{
+    extern __shared__ __align__(16) unsigned char dsm[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    ScatterStage &S = reinterpret_cast<ScatterStage *>(dsm)[warp];
+    const int64_t nchunks = (npieces + kPChunk - 1) / kPChunk;
+    const int64_t nw = (int64_t)gridDim.x * kScatterWarps;
+    unsigned long long nacc = 0;   // pairs evaluated by this warp (warp-uniform)
+    for (int64_t ch = (int64_t)blockIdx.x * kScatterWarps + warp; ch < nchunks; ch += nw) {
+        const int64_t p0 = ch * kPChunk;
+        const int nc = (int)min((int64_t)kPChunk, npieces - p0);
+        {   // stage the chunk's records: coalesced 16-byte loads
+            const uint4 *src = reinterpret_cast<const uint4 *>(rec + p0);
+            uint4 *dst = reinterpret_cast<uint4 *>(S.rec);
+            const int n16 = nc * (int)(sizeof(PieceRec) / 16);
+            for (int t = lane; t < n16; t += 32) dst[t] = __ldg(src + t);
+        }
+        __syncwarp();
+        // lane = (piece k, chord j): the chord's whole box and its rows
+        int nrows = 0;
+        {
+            const int k = lane >> 3, j = lane & 7;
+            if (k < nc && j < S.rec[k].nch) {
+                const PieceRec &R = S.rec[k];
+                const uint32_t blo = __float_as_uint(R.chq[j].z), bhi = __float_as_uint(R.chq[j].w);
+                int co[3], cnn[3];
+                bool nonempty = true, fits = true;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    co[d] = unpack3(blo, d);
+                    const int hi = unpack3(bhi, d);
+                    cnn[d] = max(0, hi - co[d] + 1);
+                    nonempty = nonempty && cnn[d] > 0;
+                    fits = fits && hi <= kScatterMaxOff;
+                }
+                if (!fits) {   // the host sends only pieces whose boxes fit: never expected
+                    atomicOr(err, 64);
+                    nonempty = false;
+                }
+                nrows = chord_row_table(R, j, co, cnn, nonempty, S.cr, lane);
+            }
+        }
+        int incl = nrows;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int roff = incl - nrows;
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        __syncwarp();
+        int cn = 0, qn = 0;   // queued candidates and pairs (warp-uniform)
+        for (int r0 = 0; r0 < total; r0 += 32) {
+            const int r = r0 + lane;
+            int c = 0;   // chord lane of row r: last lane whose first row is <= r
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int t = c + step;
+                const int ot = __shfl_sync(0xffffffffu, roff, t);
+                if (ot <= r) c = t;
+            }
+            const int rc = __shfl_sync(0xffffffffu, roff, c);
+            int i = 1, ihi = 0, a = 0, bx = 0, by = 0, bz = 0;
+            if (r < total) chord_row_span(S.rec[c >> 3], S.cr, c, c & 7, r - rc, bx, by, bz, a, i, ihi);
+            while (__any_sync(0xffffffffu, i <= ihi)) {
+                const bool has = i <= ihi;
+                uint32_t code = 0u;
+                if (has) {
+                    code = (uint32_t)c | ((uint32_t)(bx + (a == 0 ? i : 0)) << 5) |
+                           ((uint32_t)(by + (a == 1 ? i : 0)) << 13) | ((uint32_t)(bz + (a == 2 ? i : 0)) << 21);
+                    ++i;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, has);
+                if (has) S.cq[cn + __popc(bal & ((1u << lane) - 1u))] = code;
+                cn += __popc(bal);
+                __syncwarp();
+                if (cn >= 32) {
+                    scatter_test(S, lane, 32, cn, qn);
+                    if (qn >= 32) scatter_drain<General>(S, lane, 32, qn, p0, N, zs, nz, fscale, side, n3, err, D, nacc);
+                }
+            }
+        }
+        while (cn > 0) {
+            scatter_test(S, lane, min(cn, 32), cn, qn);
+            if (qn >= 32) scatter_drain<General>(S, lane, 32, qn, p0, N, zs, nz, fscale, side, n3, err, D, nacc);
+        }
+        while (qn > 0) scatter_drain<General>(S, lane, min(qn, 32), qn, p0, N, zs, nz, fscale, side, n3, err, D, nacc);
+        __syncwarp();   // the warp's stage is reused by its next chunk
+    }
+    if (lane == 0 && tally && !D.emit_only && nacc) atomicAdd(tally, nacc);
 }
 
 // ------------------------------------------------------------------------------ host
@@ -1011,6 +1243,8 @@ int piece_setup(Ctx *c, CenterlineBatch &B)
     FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     FWT_CUDA(cudaStreamSynchronize(c->stream));
     if (herr & 8) return fail(FWT_E_RANGE, "piece box wider than 1023 grid points");
+    if (herr & 64) B.scatter = false;   // a piece too wide for the scatter kernel's offsets
+    if (B.scatter) B.raster = false;
     if (B.raster && np_ > 0) FWT_TRY(piece_raster(c, B, d_err));
     return 0;
 }
@@ -1125,30 +1359,37 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     const double scale = fixed_point_scale(c);
     RedoCtx rctx = redo_ctx(c, B, scale, true);
     rctx.tally = (unsigned long long *)((char *)C.scratch[19].p + 64);
-    km = kt_begin(c, KT_DEPOSIT);
-#define FWT_PIECE_LAUNCH(G, A, D, R)                                                                       \
+    DeferList D{};
+    if (!f64) FWT_TRY(defer_list(c, npairs, c->defer_per_pair, D));
+    auto launch = [&](const DeferList &L) -> int {
+#define FWT_PIECE_LAUNCH(G, A, F, R)                                                                       \
     do {                                                                                                   \
-        FWT_CUDA(cudaFuncSetAttribute(deposit_piece_kernel<G, A, D, R>,                                    \
+        FWT_CUDA(cudaFuncSetAttribute(deposit_piece_kernel<G, A, F, R>,                                    \
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPieceSmem));      \
-        deposit_piece_kernel<G, A, D, R><<<(unsigned)ntiles, kDepThreads, kPieceSmem, c->stream>>>(       \
-            B.piece, N, ntx, nty, tz0, d_toff, d_list, scale, wx, wy, wz, d_err, rctx, B.ras_off, B.ras_pts);    \
+        deposit_piece_kernel<G, A, F, R><<<(unsigned)ntiles, kDepThreads, kPieceSmem, c->stream>>>(       \
+            B.piece, N, ntx, nty, tz0, d_toff, d_list, scale, wx, wy, wz, d_err, rctx, L, B.ras_off, B.ras_pts); \
         FWT_CUDA(cudaGetLastError());                                                                      \
     } while (0)
-#define FWT_PIECE_LAUNCH_R(G, A, D)                                                                        \
+#define FWT_PIECE_LAUNCH_R(G, A, F)                                                                        \
     do {                                                                                                   \
-        if (B.raster) FWT_PIECE_LAUNCH(G, A, D, true); else FWT_PIECE_LAUNCH(G, A, D, false);              \
+        if (B.raster) FWT_PIECE_LAUNCH(G, A, F, true); else FWT_PIECE_LAUNCH(G, A, F, false);              \
     } while (0)
-    if (f64) {
-        if (accumulate) FWT_PIECE_LAUNCH_R(true, true, true); else FWT_PIECE_LAUNCH_R(true, false, true);
-    } else if (general) {
-        if (accumulate) FWT_PIECE_LAUNCH_R(true, true, false); else FWT_PIECE_LAUNCH_R(true, false, false);
-    } else {
-        if (accumulate) FWT_PIECE_LAUNCH_R(false, true, false); else FWT_PIECE_LAUNCH_R(false, false, false);
-    }
+        const int m = kt_begin(c, KT_DEPOSIT);
+        if (f64) {
+            if (accumulate) FWT_PIECE_LAUNCH_R(true, true, true); else FWT_PIECE_LAUNCH_R(true, false, true);
+        } else if (general) {
+            if (accumulate) FWT_PIECE_LAUNCH_R(true, true, false); else FWT_PIECE_LAUNCH_R(true, false, false);
+        } else {
+            if (accumulate) FWT_PIECE_LAUNCH_R(false, true, false); else FWT_PIECE_LAUNCH_R(false, false, false);
+        }
 #undef FWT_PIECE_LAUNCH_R
 #undef FWT_PIECE_LAUNCH
-    kt_end(c, km);
-    c->launches += 2;
+        kt_end(c, m);
+        c->launches += 1;
+        return 0;
+    };
+    FWT_TRY(launch(D));
+    c->launches += 1;
     c->w_written = true;
     FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     FWT_CUDA(cudaStreamSynchronize(c->stream));
@@ -1157,7 +1398,61 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     c->wmm_valid = false;
     if (herr & 2) return fail(FWT_E_TIMEOUT, "deposit: bulk copy wait ran out");
     if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
+    if (!f64) FWT_TRY(defer_finish(c, rctx, D, npairs, c->defer_per_pair, launch));
     return 0;
+}
+
+int launch_scatter(Ctx *c, const CenterlineBatch &B)
+{
+    if (B.npieces == 0) return 0;
+    if (B.npieces >= ((int64_t)1 << 26)) return fail(FWT_E_RANGE, "piece batch exceeds 2^26");
+    Ctx &C = *c;
+    const int N = c->p.N;
+    const size_t n3 = field_elems(c);
+    FWT_TRY(side_ensure(c));
+    FWT_TRY(buf_reserve(c, C.scratch[19], 128));   // deposit_lines cleared the tallies at 64
+    int *d_err = (int *)((char *)C.scratch[19].p + 104);
+    FWT_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
+    const bool general = !(c->p.sigma_ratio == 1.0 && c->p.eta_t == 0.0);
+    const double scale = fixed_point_scale(c);
+    RedoCtx rctx = redo_ctx(c, B, scale, true);
+    rctx.tally = (unsigned long long *)((char *)C.scratch[19].p + 64);
+    const int zs = c->slab_nz ? c->slab_z0 : 0, nz = c->slab_nz ? c->slab_nz : N;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+    const int64_t nchunks = (B.npieces + kPChunk - 1) / kPChunk;
+    const unsigned grid = (unsigned)std::min<int64_t>((int64_t)sms * 3, (nchunks + kScatterWarps - 1) / kScatterWarps);
+    unsigned long long *side = (unsigned long long *)c->b_side.p;
+    DeferList D{};
+    FWT_TRY(defer_list(c, B.npieces, c->defer_per_piece, D));
+    auto launch = [&](const DeferList &L) -> int {
+        const int m = kt_begin(c, KT_DEPOSIT);
+        if (general) {
+            FWT_CUDA(cudaFuncSetAttribute(scatter_piece_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kScatterSmem));
+            scatter_piece_kernel<true><<<grid, kScatterWarps * 32, kScatterSmem, c->stream>>>(
+                B.piece, B.npieces, N, zs, nz, (float)scale, side, n3, d_err, L, rctx.tally);
+        } else {
+            FWT_CUDA(cudaFuncSetAttribute(scatter_piece_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kScatterSmem));
+            scatter_piece_kernel<false><<<grid, kScatterWarps * 32, kScatterSmem, c->stream>>>(
+                B.piece, B.npieces, N, zs, nz, (float)scale, side, n3, d_err, L, rctx.tally);
+        }
+        FWT_CUDA(cudaGetLastError());
+        kt_end(c, m);
+        c->launches += 1;
+        return 0;
+    };
+    FWT_TRY(launch(D));
+    c->side_dirty = true;
+    c->w_written = true;
+    c->wmm_valid = false;
+    int herr = 0;
+    FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    if (herr & 64) return fail(FWT_E_STATE, "scatter: a piece box wider than the candidate codes");
+    if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
+    return defer_finish(c, rctx, D, B.npieces, c->defer_per_piece, launch);
 }
 
 }  // namespace fwt

@@ -196,7 +196,6 @@ struct WarpStage {
     CandBox box[kWarpChunk];
     uint32_t q[kQueue];         // accepted points: candidate | x << 4 | y << 8 | z << 11 (tile-local)
                                 // | kQDecide (a plane test within its rounding bound)
-    RedoQueue redo;             // ill-conditioned pairs awaiting their FP64 evaluation
     uint32_t id[kWarpChunk];    // global record ids of the staged candidates
     uint64_t bar;
     uint64_t pad;
@@ -207,21 +206,22 @@ constexpr uint32_t kQDecide = 1u << 15;
 // Evaluate the first `cnt` queued points of the warp, one per lane (rec_tests again for t0,
 // then the vorticity), add them into the tile's fixed-point cells and drop them from the queue.
 // Pairs whose curved-branch amplification exceeds kRedoCond, and pairs with a plane test
-// within its rounding bound (kQDecide), go to the warp's redo queue instead, for the
-// reference's FP64 tests and evaluation.
+// within its rounding bound (kQDecide), are deferred to FP64 (DeferList) instead.  In the
+// emit-only pass (D.emit_only) nothing is added and only the deferred pairs are listed again.
 template <bool General, bool F64>
 __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN], int lane, int cnt, int &qn,
-                                            int &rn, unsigned &nacc, float fscale, float fmaxq, int *__restrict__ err,
-                                            const RedoCtx &redo, int x0, int y0, int z0)
+                                            unsigned &nacc, float fscale, float fmaxq, int *__restrict__ err,
+                                            const RedoCtx &redo, const DeferList &D, int x0, int y0, int z0)
 {
     bool flag = false, ok64 = false, counted = false;
-    uint32_t rcode = 0, rrec = 0;
+    uint32_t rrec = 0;
+    int lx = 0, ly = 0, lz = 0;
     if (F64 && lane < cnt) {
         // FP64 tile path: the candidate passed the widened FP32 tests; the reference's FP64
         // tests decide, at its index in the sub-segment's own box
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 15u);
-        const int lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)((e >> 11) & 7u);
+        lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)((e >> 11) & 7u);
         const CandBox &B = S.box[k];
         const SegRec &R = S.rec[k];
         ok64 = eval_pair_f64(redo, (int64_t)(S.id[k] & ((1u << 26) - 1u)), R.box_lo[0] + lx + B.dl[0],
@@ -230,12 +230,11 @@ __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN
     } else if (lane < cnt) {
         const uint32_t e = S.q[lane];
         const int k = (int)(e & 15u);
-        const int lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)((e >> 11) & 7u);
+        lx = (int)((e >> 4) & 15u), ly = (int)((e >> 8) & 7u), lz = (int)((e >> 11) & 7u);
         if (e & kQDecide) {
             flag = true;
-            rrec = (S.id[k] & ((1u << 26) - 1u)) | kRedoDecide;
-            rcode = redo_code(lx, ly, lz);
-        } else {
+            rrec = (S.id[k] & ((1u << 26) - 1u)) | kDeferDecide;
+        } else if (General || !D.emit_only) {
             counted = true;
             const CandBox &B = S.box[k];
             const SegRec &R = S.rec[k];
@@ -249,8 +248,7 @@ __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN
             flag = General && !(cond <= kRedoCond);
             if (flag) {
                 rrec = S.id[k] & ((1u << 26) - 1u);
-                rcode = redo_code(lx, ly, lz);
-            } else {
+            } else if (!D.emit_only) {
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     float sv = vv[d] * fscale;
@@ -263,11 +261,11 @@ __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN
             }
         }
     }
-    if constexpr (F64) nacc += __popc(__ballot_sync(0xffffffffu, ok64));
-    else nacc += __popc(__ballot_sync(0xffffffffu, counted));
-    if constexpr (!F64) {
-        redo_push(S.redo, lane, flag, rrec, rcode, rn);
-        if (rn >= 32) redo_drain(S.redo, redo, acc, lane, 32, rn, x0, y0, z0, err);
+    if constexpr (F64) {
+        nacc += __popc(__ballot_sync(0xffffffffu, ok64));
+    } else {
+        nacc += __popc(__ballot_sync(0xffffffffu, counted));
+        defer_push(D, lane, flag, rrec, x0 + lx, y0 + ly, z0 + lz);
     }
     __syncwarp();
     const int rem = qn - cnt;
@@ -297,7 +295,7 @@ template <bool General, bool Accumulate, bool F64>
 __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
     const SegRec *__restrict__ rec, int N, int ntx, int nty, int tz0, const int64_t *__restrict__ tile_off,
     const uint32_t *__restrict__ list, double scale, void *__restrict__ wx, void *__restrict__ wy,
-    void *__restrict__ wz, int *__restrict__ err, const RedoCtx redo)
+    void *__restrict__ wz, int *__restrict__ err, const RedoCtx redo, const DeferList D)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     long long(*acc)[kAccN] = reinterpret_cast<long long(*)[kAccN]>(dsm);
@@ -320,7 +318,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
     if constexpr (F64)
         tile_acc_init_f64<Accumulate>(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, zs, zlim, (const double *)wx,
                                       (const double *)wy, (const double *)wz);
-    else
+    else if (!D.emit_only)
         tile_acc_init<Accumulate>(acc, N, x0, y0, z0, zs, zlim, scale, (const float *)wx, (const float *)wy,
                                   (const float *)wz);
     __syncthreads();
@@ -331,7 +329,6 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
     uint32_t phase = 0;
     bool failed = false;
     int qn = 0;   // queued points of this warp (warp-uniform)
-    int rn = 0;   // queued FP64 redo pairs of this warp (warp-uniform)
     unsigned nacc = 0;   // pairs evaluated by this warp (warp-uniform)
     for (int ch = warp; ch < nchunks && !failed;) {
         const int64_t base = c0 + (int64_t)ch * kWarpChunk;
@@ -424,24 +421,22 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
                 if (ok) S.q[qn + __popc(bal & ((1u << lane) - 1u))] = code;
                 qn += __popc(bal);
                 __syncwarp();
-                if (qn >= 32) drain_queue<General, F64>(S, acc, lane, 32, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+                if (qn >= 32) drain_queue<General, F64>(S, acc, lane, 32, qn, nacc, fscale, fmaxq, err, redo, D, x0, y0, z0);
             }
         }
-        if (qn > 0) drain_queue<General, F64>(S, acc, lane, qn, qn, rn, nacc, fscale, fmaxq, err, redo, x0, y0, z0);
+        if (qn > 0) drain_queue<General, F64>(S, acc, lane, qn, qn, nacc, fscale, fmaxq, err, redo, D, x0, y0, z0);
         __syncwarp();   // the warp's stage is reused by its next chunk
         int nxt = 0;
         if (lane == 0) nxt = atomicAdd(&next_chunk, 1);
         ch = __shfl_sync(0xffffffffu, nxt, 0);
     }
-    if constexpr (!F64)
-        if (rn > 0) redo_drain(S.redo, redo, acc, lane, rn, rn, x0, y0, z0, err);
     if (failed && lane == 0) atomicOr(err, 2);
-    if (lane == 0 && redo.tally) atomicAdd(redo.tally, (unsigned long long)nacc);
+    if (lane == 0 && redo.tally && !D.emit_only) atomicAdd(redo.tally, (unsigned long long)nacc);
     __syncthreads();
     if constexpr (F64)
         tile_epilogue_f64(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, zs, zlim, (double *)wx, (double *)wy,
                           (double *)wz);
-    else
+    else if (!D.emit_only)
         tile_epilogue(acc, N, x0, y0, z0, zs, zlim, scale, (float *)wx, (float *)wy, (float *)wz);
 }
 
@@ -487,6 +482,134 @@ double fixed_point_scale(const Ctx *c)
     b *= 16.0;
     const int e = (int)std::floor(48.0 - std::log2(b));
     return std::ldexp(1.0, e);
+}
+
+// ------------------------------------------------------------------ deferred pairs
+// One thread per deferred pair: the reference's FP64 tests (decided pairs) and vorticity
+// (redo_pair_f64), added as int64 fixed point into the side accumulator side[3][n3].
+__global__ void __launch_bounds__(128) redo_apply_kernel(const RedoCtx R, const Deferred *__restrict__ e, int64_t n,
+                                                         unsigned long long *__restrict__ side, size_t n3,
+                                                         int *__restrict__ err)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool taken = false;
+    if (i < n) {
+        const Deferred d = e[i];
+        const bool decide = (d.rec & kDeferDecide) != 0u;
+        const int gx = (int)(d.gxy & 0xffffu), gy = (int)(d.gxy >> 16), gz = (int)d.gz;
+        long long q[3];
+        const int r = redo_pair_f64(R, d.rec & ((1u << 26) - 1u), (int)((d.rec >> 26) & 7u), decide, gx, gy, gz, q);
+        if (r < 0) atomicOr(err, 4);
+        if (r != 0) {
+            const size_t g = (size_t)gx + (size_t)R.N * ((size_t)gy + (size_t)R.N * (size_t)(gz - R.zs));
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+                if (q[k] != 0) atomicAdd(side + (size_t)k * n3 + g, (unsigned long long)q[k]);
+        }
+        taken = decide && r != 0;
+    }
+    // tallies: decided pairs the FP64 tests accept (the cond pairs were counted by the tile
+    // kernel), and every pair evaluated here
+    const unsigned nt = __popc(__ballot_sync(0xffffffffu, taken));
+    const unsigned nv = __popc(__ballot_sync(0xffffffffu, i < n));
+    if ((threadIdx.x & 31) == 0 && R.tally) {
+        if (nt) atomicAdd(R.tally, (unsigned long long)nt);
+        if (nv) atomicAdd(R.tally + 1, (unsigned long long)nv);
+    }
+}
+
+// omega += side / scale where side holds a sum, and side back to zero.
+__global__ void side_fold_kernel(float *__restrict__ w, unsigned long long *__restrict__ side, size_t n, double inv)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const long long v = (long long)side[i];
+        if (v != 0) {
+            w[i] = (float)((double)w[i] + (double)v * inv);
+            side[i] = 0ull;
+        }
+    }
+}
+
+int defer_list(Ctx *c, int64_t units, double rate, DeferList &D)
+{
+    const double want = std::max(1.0 * (1 << 20), 1.5 * rate * (double)units);
+    const unsigned long long cap = (unsigned long long)want;
+    FWT_TRY(buf_reserve(c, c->b_defer, 16 + sizeof(Deferred) * (size_t)cap));
+    D.count = (unsigned long long *)c->b_defer.p;
+    D.e = (Deferred *)((char *)c->b_defer.p + 16);
+    D.cap = (c->b_defer.bytes - 16) / sizeof(Deferred);
+    D.emit_only = 0;
+    D.pad = 0;
+    FWT_CUDA(cudaMemsetAsync(D.count, 0, sizeof(unsigned long long), c->stream));
+    return 0;
+}
+
+int defer_grow(Ctx *c, unsigned long long n, DeferList &D)
+{
+    // the list's old entries are rewritten by the refill pass: a fresh buffer will do
+    buf_free(c, c->b_defer);
+    FWT_TRY(buf_reserve(c, c->b_defer, 16 + sizeof(Deferred) * (size_t)(n + n / 8)));
+    D.count = (unsigned long long *)c->b_defer.p;
+    D.e = (Deferred *)((char *)c->b_defer.p + 16);
+    D.cap = (c->b_defer.bytes - 16) / sizeof(Deferred);
+    FWT_CUDA(cudaMemsetAsync(D.count, 0, sizeof(unsigned long long), c->stream));
+    return 0;
+}
+
+void defer_rate(double &rate, unsigned long long n, int64_t units)
+{
+    if (units > 0) rate = std::max(1e-3, (double)n / (double)units);
+}
+
+int side_ensure(Ctx *c)
+{
+    const size_t bytes = 3 * field_elems(c) * sizeof(unsigned long long);
+    if (!c->b_side.p || c->b_side.bytes < bytes) {
+        buf_free(c, c->b_side);
+        FWT_TRY(buf_reserve(c, c->b_side, bytes));
+        FWT_CUDA(cudaMemsetAsync(c->b_side.p, 0, c->b_side.bytes, c->stream));
+        c->side_dirty = false;
+    }
+    return 0;
+}
+
+int defer_apply(Ctx *c, const RedoCtx &R, const DeferList &D, unsigned long long n)
+{
+    if (n == 0) return 0;
+    const size_t n3 = field_elems(c);
+    FWT_TRY(side_ensure(c));
+    FWT_TRY(buf_reserve(c, c->scratch[19], 128));
+    int *d_err = (int *)((char *)c->scratch[19].p + 96);
+    FWT_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
+    const int km = kt_begin(c, KT_DEPOSIT);
+    redo_apply_kernel<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(R, D.e, (int64_t)n,
+                                                                          (unsigned long long *)c->b_side.p, n3, d_err);
+    kt_end(c, km);
+    c->launches += 1;
+    FWT_CUDA(cudaGetLastError());
+    c->side_dirty = true;
+    int herr = 0;
+    FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    if (herr & 4) return fail(FWT_E_RANGE, "deposit: FP64 contribution outside the fixed-point range");
+    return 0;
+}
+
+int side_fold(Ctx *c)
+{
+    if (!c->side_dirty) return 0;
+    const size_t n = 3 * field_elems(c);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
+    const int km = kt_begin(c, KT_DEPOSIT);
+    side_fold_kernel<<<(unsigned)(sms * 8), 256, 0, c->stream>>>((float *)c->b_w.p, (unsigned long long *)c->b_side.p,
+                                                                n, 1.0 / fixed_point_scale(c));
+    kt_end(c, km);
+    c->launches += 1;
+    FWT_CUDA(cudaGetLastError());
+    c->side_dirty = false;
+    c->wmm_valid = false;
+    return 0;
 }
 
 int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
@@ -558,26 +681,33 @@ int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     const double scale = fixed_point_scale(c);
     RedoCtx rctx = redo_ctx(c, B, scale, false);
     rctx.tally = (unsigned long long *)((char *)C.scratch[19].p + 64);
-    km = kt_begin(c, KT_DEPOSIT);
-#define FWT_TILE_LAUNCH(G, A, D)                                                                          \
+    DeferList D{};
+    if (!f64) FWT_TRY(defer_list(c, npairs, c->defer_per_pair, D));
+    auto launch = [&](const DeferList &L) -> int {
+#define FWT_TILE_LAUNCH(G, A, F)                                                                          \
     do {                                                                                                  \
-        FWT_CUDA(cudaFuncSetAttribute(deposit_tile_kernel<G, A, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+        FWT_CUDA(cudaFuncSetAttribute(deposit_tile_kernel<G, A, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                       (int)kDepSmem));                                                    \
-        deposit_tile_kernel<G, A, D><<<(unsigned)ntiles, kDepThreads, kDepSmem, c->stream>>>(             \
-            B.rec, N, ntx, nty, tz0, d_toff, d_list, scale, wx, wy, wz, d_err, rctx);                     \
+        deposit_tile_kernel<G, A, F><<<(unsigned)ntiles, kDepThreads, kDepSmem, c->stream>>>(             \
+            B.rec, N, ntx, nty, tz0, d_toff, d_list, scale, wx, wy, wz, d_err, rctx, L);                  \
         FWT_CUDA(cudaGetLastError());                                                                     \
     } while (0)
-    if (f64) {
-        // the FP64 path evaluates every pair in FP64: the General distinction is only the FP32 one
-        if (accumulate) FWT_TILE_LAUNCH(true, true, true); else FWT_TILE_LAUNCH(true, false, true);
-    } else if (general) {
-        if (accumulate) FWT_TILE_LAUNCH(true, true, false); else FWT_TILE_LAUNCH(true, false, false);
-    } else {
-        if (accumulate) FWT_TILE_LAUNCH(false, true, false); else FWT_TILE_LAUNCH(false, false, false);
-    }
+        const int m = kt_begin(c, KT_DEPOSIT);
+        if (f64) {
+            // the FP64 path evaluates every pair in FP64: the General distinction is only the FP32 one
+            if (accumulate) FWT_TILE_LAUNCH(true, true, true); else FWT_TILE_LAUNCH(true, false, true);
+        } else if (general) {
+            if (accumulate) FWT_TILE_LAUNCH(true, true, false); else FWT_TILE_LAUNCH(true, false, false);
+        } else {
+            if (accumulate) FWT_TILE_LAUNCH(false, true, false); else FWT_TILE_LAUNCH(false, false, false);
+        }
 #undef FWT_TILE_LAUNCH
-    kt_end(c, km);
-    c->launches += 2;
+        kt_end(c, m);
+        c->launches += 1;
+        return 0;
+    };
+    FWT_TRY(launch(D));
+    c->launches += 1;
     c->w_written = true;
     FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     FWT_CUDA(cudaStreamSynchronize(c->stream));
@@ -586,6 +716,7 @@ int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     c->wmm_valid = false;
     if (herr & 2) return fail(FWT_E_TIMEOUT, "deposit: bulk copy wait ran out");
     if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
+    if (!f64) FWT_TRY(defer_finish(c, rctx, D, npairs, c->defer_per_pair, launch));
     return 0;
 }
 

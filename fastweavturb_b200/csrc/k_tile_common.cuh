@@ -322,72 +322,90 @@ __device__ __forceinline__ int box_index(int i, int lo, int N)
 
 
 
-// ---------------------------------------------------------------- FP64 redo of pairs
-// A warp queues two kinds of (point, chord) pairs and evaluates them 32 at a time, one per lane,
-// in the reference's FP64 arithmetic from the batch's FP64 spline data (redo_pair_f64), adding
-// the fixed-point result into the same tile cells:
+// ---------------------------------------------------------------- pairs deferred to FP64
+// Two kinds of (point, chord) pairs are not evaluated by the FP32 tile kernels:
 // * accepted pairs whose curved-branch amplification |1/(1 - kappa rho cos theta)| exceeds
 //   kRedoCond (tube.f90:876-879: the FP32 value carries the amplified rounding of kappa, rho and
 //   cos theta); only tubes with a varying core or a twist have that term;
-// * pairs with a plane test within its FP32 rounding bound of zero, which the reference's FP64
-//   tests decide (the decide bit).
-struct RedoQueue {
-    uint2 e[64];   // x: record id | chord << 26 | decide << 31; y: tile-local point x | y << 4 | z << 7
+// * pairs with a plane test within its FP32 rounding bound of zero (the decide bit), which the
+//   reference's FP64 tests decide.
+// The kernels append them to a global list (a warp-aggregated counter; every pair is counted,
+// stored or not); after the kernel, redo_apply_kernel evaluates each in the reference's FP64
+// arithmetic (redo_pair_f64) and adds its int64 fixed-point contribution into a side
+// accumulator, which side_fold adds into omega once the batch loop is done.  Integer sums make
+// the field independent of the order; no FP64 code, and so no call, sits in the FP32 kernels.
+// A list that overflows is refilled by a second, emit-only pass of the same kernel at the
+// counted size.
+struct Deferred {
+    uint32_t rec;   // record id | chord << 26 | kDeferDecide
+    uint32_t gxy;   // grid point x | y << 16 (0-based, wrapped)
+    uint32_t gz;    // grid plane z (0-based, global)
+    uint32_t pad;
 };
-constexpr uint32_t kRedoDecide = 1u << 31;
+constexpr uint32_t kDeferDecide = 1u << 31;
 
-__device__ __forceinline__ uint32_t redo_code(int lx, int ly, int lz)
-{
-    return (uint32_t)lx | ((uint32_t)ly << 4) | ((uint32_t)lz << 7);
-}
+struct DeferList {
+    Deferred *e;
+    unsigned long long *count;   // pairs pushed (may exceed cap)
+    unsigned long long cap;
+    int emit_only;               // 1: the refill pass after an overflow (no field update)
+    int pad;
+};
 
-// Append the lanes' flagged pairs (at most 32) to the queue; rn is warp-uniform and stays
-// below 64 when the caller drains at 32.
-__device__ __forceinline__ void redo_push(RedoQueue &Q, int lane, bool flag, uint32_t rec, uint32_t code, int &rn)
+// Append the lanes' flagged pairs (warp-uniform call).
+__device__ __forceinline__ void defer_push(const DeferList &D, int lane, bool flag, uint32_t rec, int gx, int gy,
+                                           int gz)
 {
     const unsigned bal = __ballot_sync(0xffffffffu, flag);
-    if (flag) Q.e[rn + __popc(bal & ((1u << lane) - 1u))] = make_uint2(rec, code);
-    rn += __popc(bal);
-    __syncwarp();
-}
-
-// Evaluate the first cnt queued pairs in FP64 and drop them from the queue.  Decided pairs
-// that the FP64 tests accept are added to the tally of accepted pairs.
-__device__ __forceinline__ void redo_drain(RedoQueue &Q, const RedoCtx &R, long long (*acc)[kAccN], int lane, int cnt,
-                                           int &rn, int x0, int y0, int z0, int *__restrict__ err)
-{
-    bool taken = false;
-    if (lane < cnt) {
-        const uint2 e = Q.e[lane];
-        const int lx = (int)(e.y & 15u), ly = (int)((e.y >> 4) & 7u), lz = (int)((e.y >> 7) & 7u);
-        const bool decide = (e.x & kRedoDecide) != 0u;
-        long long q[3];
-        const int r = redo_pair_f64(R, e.x & ((1u << 26) - 1u), (int)((e.x >> 26) & 7u), decide, x0 + lx, y0 + ly,
-                                    z0 + lz, q);
-        if (r < 0) atomicOr(err, 4);
-        taken = decide && r != 0;
-        if (r != 0) {
-            const int p = lx + kSY * ly + kSZ * lz;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) atomicAdd((unsigned long long *)&acc[d][p], (unsigned long long)q[d]);
-        }
+    if (bal == 0u) return;
+    const int leader = __ffs(bal) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(D.count, (unsigned long long)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (flag) {
+        const unsigned long long i = base + (unsigned long long)__popc(bal & ((1u << lane) - 1u));
+        if (i < D.cap) D.e[i] = Deferred{rec, (uint32_t)gx | ((uint32_t)gy << 16), (uint32_t)gz, 0u};
     }
-    const unsigned nt = __popc(__ballot_sync(0xffffffffu, taken));
-    if (lane == 0 && R.tally) {
-        atomicAdd(R.tally + 1, (unsigned long long)cnt);
-        if (nt) atomicAdd(R.tally, (unsigned long long)nt);
-    }
-    __syncwarp();
-    const int rem = rn - cnt;
-    const uint2 keep = lane < rem ? Q.e[cnt + lane] : make_uint2(0u, 0u);
-    __syncwarp();
-    if (lane < rem) Q.e[lane] = keep;
-    __syncwarp();
-    rn = rem;
 }
 
 // The redo context of a batch (records: sub-segments, or chord pieces when `pieces`).
 RedoCtx redo_ctx(const Ctx *c, const CenterlineBatch &B, double scale, bool pieces);
+
+// The deferred-pair list of a launch over `units` work units ((tile, record) pairs, or pieces),
+// sized from the running rate of deferred pairs per unit (k_deposit_tile.cu).
+int defer_list(Ctx *c, int64_t units, double rate, DeferList &D);
+// The side accumulator (3 x the field, int64), allocated and zeroed on first use.
+int side_ensure(Ctx *c);
+
+// Evaluate the first n pairs of the list in FP64 into the side accumulator (k_deposit_tile.cu).
+int defer_apply(Ctx *c, const RedoCtx &R, const DeferList &D, unsigned long long n);
+// Make the list hold n pairs (n > its capacity) and reset its count.
+int defer_grow(Ctx *c, unsigned long long n, DeferList &D);
+void defer_rate(double &rate, unsigned long long n, int64_t units);
+
+// After a tile launch: read the list's count; if it overflowed, make room for the counted pairs
+// and refill the list through rescan(D) (the same launch in emit-only mode); then evaluate every
+// deferred pair in FP64 into the side accumulator.
+template <typename F>
+int defer_finish(Ctx *c, const RedoCtx &R, DeferList &D, int64_t units, double &rate, F &&rescan)
+{
+    unsigned long long n = 0;
+    FWT_CUDA(cudaMemcpyAsync(&n, D.count, sizeof(n), cudaMemcpyDeviceToHost, c->stream));
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    defer_rate(rate, n, units);
+    if (n == 0) return 0;
+    if (n > D.cap) {
+        FWT_TRY(defer_grow(c, n, D));
+        D.emit_only = 1;
+        FWT_TRY(rescan(D));
+        D.emit_only = 0;
+        unsigned long long n2 = 0;
+        FWT_CUDA(cudaMemcpyAsync(&n2, D.count, sizeof(n2), cudaMemcpyDeviceToHost, c->stream));
+        FWT_CUDA(cudaStreamSynchronize(c->stream));
+        if (n2 != n) return fail(FWT_E_STATE, "deferred pairs: the refill pass counted a different number");
+    }
+    return defer_apply(c, R, D, n);
+}
 
 // Shared kernels of the binning (defined in k_deposit_tile.cu).
 __global__ void tile_scatter_kernel(const uint32_t *__restrict__ key, const uint32_t *__restrict__ val, int64_t n,

@@ -224,8 +224,9 @@ int fwt_field_uw(fwt_ctx *ctx, float *host_out);
 int fwt_field_wd(fwt_ctx *ctx, float *host_out);
 /* Counters of the last deposition: c[0] lines, c[1] sections, c[2] sub-segments,
  * c[3] candidate (tile, record) pairs, c[4] kernel launches of the last fwt_run, c[5] accepted
- * (grid point, sub-segment) pairs, i.e. vorticity evaluations, c[6] of those, the pairs the
- * FP32 path evaluated in FP64 because of their curved-branch amplification. */
+ * (grid point, sub-segment) pairs, i.e. vorticity evaluations, c[6] the pairs the FP32 path
+ * handed to FP64: those with a plane test within its FP32 rounding bound (decided by the FP64
+ * tests) and accepted ones with a large curved-branch amplification. */
 int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
 
 /* Tuning knobs of the context (no counterpart in the reference).  FWT_TUNE_PIECE_RT_CELLS:
@@ -236,9 +237,15 @@ int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
 #define FWT_TUNE_PIECE_RT_CELLS 1
 /* FWT_TUNE_RASTER_RT_CELLS: piece lines whose truncation radius is at most `value` grid
  * spacings are rasterised once per piece (their accepted points listed before the deposition)
- * instead of searched within every tile; 0 switches it off, value < 0 restores the default, 2.5.
- * The accepted points and their values are the same either way. */
+ * instead of searched within every tile; 0 (the default; value < 0 restores it) switches it
+ * off.  The accepted points and their values are the same either way. */
 #define FWT_TUNE_RASTER_RT_CELLS 2
+/* FWT_TUNE_SCATTER_RT_CELLS: on the FP32 path, piece lines whose truncation radius is at most
+ * `value` grid spacings are deposited without tiles: each piece is searched once and its
+ * contributions are added as int64 fixed point with global reductions (the sums do not depend
+ * on the order); thicker piece lines go through the tiles.  0 switches it off, value < 0
+ * restores the default, 8.  The field is the same either way to FP32 rounding. */
+#define FWT_TUNE_SCATTER_RT_CELLS 3
 int fwt_set_tuning(fwt_ctx *ctx, int key, double value);
 
 /* Message of the last error on this thread. */

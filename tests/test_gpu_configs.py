@@ -52,7 +52,8 @@ def test_cfg0_whole_field_matches_oracle(fwt, orc, cfg0_case, precision, mode):
     s = ctx.cal_helicity()
     assert s["up"] == pytest.approx(ref["up"], rel=tol)
     assert s["Enstrophy"] == pytest.approx(ref["Enstrophy"], rel=tol)
-    assert s["Etot"] == pytest.approx(1.5, rel=tol)      # Etot / u'^2 = 3/2 after normalisation
+    assert s["Etot"] == pytest.approx(ref["Etot"], rel=tol)   # the energy before normalisation
+    assert s["Etot"] / s["up"] ** 2 == pytest.approx(1.5, rel=1e-12)   # u' = sqrt(2 Etot / 3)
     assert rel_l2(ctx.spectrum(0), ref["spectrum_vor"]) <= tol
     assert rel_l2(ctx.spectrum(1), ref["spectrum"]) <= tol
     r, Sp = ctx.Sp_calculate(pmax=10)

@@ -108,27 +108,27 @@ def test_ntf_bit_exact_across_curvatures(fwt, orc, H, dB_over_sigma):
 @pytest.mark.parametrize("precision", [32, 64])
 def test_rasterised_pieces_equal_searched_pieces(fwt, orc, precision):
     """Thin tubes (truncation radius 0.6-1.2 grid spacings on 64^3): the pieces rasterised once
-    (the default below 2.5 grid spacings) and the pieces searched in every tile accept the same
+    (radius limit 4 grid spacings) and the pieces searched in every tile (limit 0) accept the same
     points with the same test, so the FP32 fields are identical (int64 fixed-point sums) and the
     FP64 fields agree to the order of their FP64 additions; both match the oracle."""
     from fastweavturb_b200.configs import small
     w = small(N=64, seed=7, nlev=2, tubes0=3, nodes0=128, sigma0=0.04)
     p, cl = oracle_inputs(orc, w)
     fields = {}
-    for cells in (-1.0, 0.0):
+    for cells in (4.0, 0.0):
         ctx = fwt.Context(gpu_params(fwt, w, precision=precision, deposit_mode=0))
         ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
         ctx.set_raster_radius_limit(cells)
         ctx.deposit(1, w.ntubes)
         fields[cells] = ctx.field(0).copy()
         ctx.close()
-    assert np.abs(fields[-1.0]).max() > 0
+    assert np.abs(fields[4.0]).max() > 0
     if precision == 32:
-        assert np.array_equal(fields[-1.0], fields[0.0])
+        assert np.array_equal(fields[4.0], fields[0.0])
     else:
-        assert rel_l2(fields[-1.0], fields[0.0]) <= 1e-15
+        assert rel_l2(fields[4.0], fields[0.0]) <= 1e-15
     floor, vor = fp64_floor(orc, p, cl)
-    assert rel_l2(fields[-1.0], vor) <= (TOL32 if precision == 32 else tol64(floor))
+    assert rel_l2(fields[4.0], vor) <= (TOL32 if precision == 32 else tol64(floor))
 
 
 def test_piece_and_subsegment_kernels_agree(fwt, orc):
@@ -202,3 +202,33 @@ def test_optional_field_outputs_match_oracle(fwt, orc, small_case, precision, mo
     assert np.array_equal(np.fromfile(tmp_path / "output" / "field_uw.dat", dtype=np.float32), uw.ravel())
     assert np.array_equal(np.fromfile(tmp_path / "output" / "field_wd.dat", dtype=np.float32), wd.ravel())
     ctx.close()
+
+
+@pytest.mark.parametrize("sigma_ratio", [1.0, 4.0])
+def test_scatter_equals_tile_pieces(fwt, orc, sigma_ratio):
+    """Thin tubes (truncation radius 1.8-3.7 grid spacings on 64^3) through the scatter kernel
+    (each piece searched once, int64 global sums; the FP32 default for piece lines) and through
+    the piece tile kernel: the same accepted pairs and FP64 hand-overs, fields equal to FP32
+    rounding (the tile path rounds omega to FP32 after every batch, the scatter path once), both
+    matching the FP64 oracle.  sigma_ratio 4 takes the curved-branch terms (General)."""
+    from fastweavturb_b200.configs import small
+    w = small(N=64, seed=11, nlev=2, tubes0=3, nodes0=128, sigma0=0.12 / sigma_ratio)
+    w.sigma_ratio = sigma_ratio
+    p, cl = oracle_inputs(orc, w)
+    fields, counts = {}, {}
+    for cells in (8.0, 0.0):
+        ctx = fwt.Context(gpu_params(fwt, w, precision=32, deposit_mode=0))
+        ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+        ctx.set_scatter_radius_limit(cells)
+        ctx.deposit(1, w.ntubes)
+        fields[cells] = ctx.field(0).copy()
+        counts[cells] = ctx.counters()
+        ctx.close()
+    assert np.abs(fields[8.0]).max() > 0
+    assert counts[8.0]["accepted"] == counts[0.0]["accepted"]
+    assert counts[8.0]["redone_fp64"] == counts[0.0]["redone_fp64"]
+    assert counts[8.0]["pairs"] == 0 < counts[0.0]["pairs"]
+    assert rel_l2(fields[8.0], fields[0.0]) <= 1e-6
+    vor, _ = orc.deposit(p, cl)
+    assert rel_l2(fields[8.0], vor) <= TOL32
+    assert rel_l2(fields[0.0], vor) <= TOL32
