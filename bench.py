@@ -261,11 +261,12 @@ def timed_runs(ctx, stream, steps, torch):
 
 
 def rel_l2_device(a, b, torch):
-    """||a - b|| / ||b|| of two device fields (3, N, N, N) of any precision, in FP64, by z-slabs."""
+    """||a - b|| / ||b|| of two fields (3, N, N, N) of any precision, in FP64 on b's device, by
+    z-slabs (a may be held in host memory)."""
     num = den = 0.0
     for c in range(3):
         for z in range(0, a.shape[1], 64):
-            x = a[c, z:z + 64].double()
+            x = a[c, z:z + 64].to(b.device).double()
             y = b[c, z:z + 64].double()
             num += float(torch.sum((x - y) ** 2))
             den += float(torch.sum(y * y))
@@ -388,7 +389,14 @@ def main():
     # end to end through the public API from pinned host memory
     e2e = None
     if not args.no_e2e:
-        host = xyz.T.contiguous().cpu().pin_memory()
+        # the nodes to pinned host memory, one coordinate at a time; the generator's device copy
+        # is released first, since the library now holds its own (at 1024^3 both do not fit)
+        host = torch.empty((w.nnodes, 3), dtype=torch.float64, pin_memory=True)
+        for d in range(3):
+            host[:, d].copy_(xyz[d])
+        xyz = None
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
         hx = host.numpy()
         nd = params.N_downsample
         ne = args.e2e_steps or min(args.steps, 3)
@@ -418,11 +426,13 @@ def main():
         ew32, eu32 = ctx.spectrum(0), ctx.spectrum(1)
         ctx.cal_helicity()
         _, sp32 = ctx.Sp_calculate(pmax=10)
-        w32 = ctx.field_tensor(0).clone()
-        u32 = ctx.field_tensor(1).clone()
+        # the FP32 fields wait in host memory while the FP64 context holds the device
+        w32 = ctx.field_tensor(0).cpu()
+        u32 = ctx.field_tensor(1).cpu()
         ctx.close()
-        del xyz
+        xyz = None
         torch.cuda.synchronize()
+        torch.cuda.empty_cache()
         _, ctx64, xyz64, _ = make_ctx(64, 0)
         ms64, kt64, _ = timed_runs(ctx64, stream, args.fp64_steps, torch)
         ew64, eu64 = ctx64.spectrum(0), ctx64.spectrum(1)

@@ -353,7 +353,7 @@ class Context:
 
     def set_scatter_radius_limit(self, cells):
         """FP32 piece tubes up to this truncation radius (grid spacings) are deposited without
-        tiles, with int64 global reductions (0: never; negative: the default, 8)."""
+        tiles, with int64 global reductions (0: never; negative: the default, 5)."""
         _check(library().fwt_set_tuning(self._h, 3, float(cells)))
 
     def counters(self):

@@ -116,10 +116,10 @@ int kt_collect(Ctx *c)
     return 0;
 }
 
-// de-interleave row-major xyz (n x 3) into SoA x[], y[], z[]
-__global__ void deinterleave_kernel(const double *__restrict__ aos, int64_t n, double *__restrict__ soa)
+// de-interleave m rows of row-major xyz (m x 3) into SoA x[], y[], z[] of stride n
+__global__ void deinterleave_kernel(const double *__restrict__ aos, int64_t m, int64_t n, double *__restrict__ soa)
 {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
         soa[i] = aos[3 * i];
         soa[n + i] = aos[3 * i + 1];
         soa[2 * n + i] = aos[3 * i + 2];
@@ -300,14 +300,22 @@ int fwt_set_centerlines(fwt_ctx *h, int nline, const int64_t *npoint, const doub
     cudaSetDevice(c->dev);
     FWT_TRY(set_lines_common(c, nline, npoint, sigma, Gamma, n_T, if_filter));
     const int64_t n = c->node_off[nline];
-    // one copy of the caller's row-major array (fast when it is pinned), then SoA on the device
-    FWT_TRY(buf_reserve(c, c->b_nodes, sizeof(double) * 6 * (size_t)n));
+    // the caller's row-major array in chunks of up to 32 Mi nodes (fast when it is pinned)
+    // through a staging buffer (scratch[27]), each chunk made SoA on the device
+    FWT_TRY(buf_reserve(c, c->b_nodes, sizeof(double) * 3 * (size_t)n));
     double *d = (double *)c->b_nodes.p;
-    double *stage = d + 3 * n;
-    FWT_CUDA(cudaMemcpyAsync(stage, xyz, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
-    deinterleave_kernel<<<(unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16), 256, 0, c->stream>>>(stage, n, d);
-    c->launches += 1;
-    FWT_CUDA(cudaGetLastError());
+    const int64_t chunk = std::min<int64_t>(n, (int64_t)1 << 25);
+    FWT_TRY(buf_reserve(c, c->scratch[27], sizeof(double) * 3 * (size_t)std::max<int64_t>(chunk, 1)));
+    double *stage = (double *)c->scratch[27].p;
+    for (int64_t o = 0; o < n; o += chunk) {
+        const int64_t m = std::min(chunk, n - o);
+        FWT_CUDA(cudaMemcpyAsync(stage, xyz + 3 * o, sizeof(double) * 3 * (size_t)m, cudaMemcpyHostToDevice,
+                                 c->stream));
+        deinterleave_kernel<<<(unsigned)std::min<int64_t>((m + 255) / 256, 148 * 16), 256, 0, c->stream>>>(
+            stage, m, n, d + o);
+        c->launches += 1;
+        FWT_CUDA(cudaGetLastError());
+    }
     FWT_CUDA(cudaStreamSynchronize(c->stream));
     c->d_x = d;
     c->d_y = d + n;

@@ -244,7 +244,7 @@ int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
  * `value` grid spacings are deposited without tiles: each piece is searched once and its
  * contributions are added as int64 fixed point with global reductions (the sums do not depend
  * on the order); thicker piece lines go through the tiles.  0 switches it off, value < 0
- * restores the default, 8.  The field is the same either way to FP32 rounding. */
+ * restores the default, 5.  The field is the same either way to FP32 rounding. */
 #define FWT_TUNE_SCATTER_RT_CELLS 3
 int fwt_set_tuning(fwt_ctx *ctx, int key, double value);
 
