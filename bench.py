@@ -127,6 +127,13 @@ def whole_job_rate(world, steps, N, ms):
 # 116 B per point (232 in FP64).  Deposition adds the centerline data: about 200 B per node
 # (coordinates, arc length, derivatives, the section's spline and sub-segment set-up).
 PATH_BYTES_PER_POINT = {32: 116, 64: 232}
+# FP32 operations of one accepted (point, chord) pair of the constant-core path (FMA = 2): the
+# three plane/cylinder tests (about 20), the quintic and its derivative by Horner (54), the
+# divided-difference offset of the piece kernels (34), x - c(zeta), rho^2, |c'|^2, the tangent,
+# the Burgers profile and the fixed-point scaling (about 37), with two hardware rsqrt/exp
+FLOPS_PER_PAIR = 145
+# nominal FP32 FMA peak of a B200: 148 SMs x 128 lanes x 2 flops x 1.965 GHz
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 DEPOSIT_BYTES_PER_POINT = {32: 12, 64: 24}
 BYTES_PER_NODE = 200
 
@@ -382,6 +389,11 @@ def main():
         if dom_name == "deposit" and acc:
             roofline["accepted_pairs_per_step"] = acc
             roofline["accepted_pairs_per_s"] = acc / (dom_ms / args.steps / 1e3)
+            # the deposition is instruction-bound, not HBM-bound: its FP32 arithmetic ceiling
+            tf = roofline["accepted_pairs_per_s"] * FLOPS_PER_PAIR / 1e12
+            roofline["fp32_ceiling"] = {"flops_per_pair": FLOPS_PER_PAIR, "achieved_tflops": tf,
+                                        "peak_tflops": FP32_PEAK_TFLOPS, "peak_kind": "nominal",
+                                        "frac": tf / FP32_PEAK_TFLOPS}
     whole_path = {"bytes_per_step": PATH_BYTES_PER_POINT[args.precision] * w.N ** 3 + BYTES_PER_NODE * w.nnodes}
     whole_path["achieved_gbs"] = whole_path["bytes_per_step"] / (ms_step / 1e3) / 1e9
     whole_path["frac"] = whole_path["achieved_gbs"] / peaks["hbm_gbs"]

@@ -502,7 +502,7 @@ __device__ __forceinline__ void segrec_from(const SegF &G, const SubSeg &S, SegR
     // per-record constants of the constant-core profile (tube.f90:845-847 with sigma = smin)
     const float s2 = G.smin * G.smin;
     R.inv2s2 = 0.5f / s2;
-    R.ftd = expf(-G.R2 * R.inv2s2);
+    R.ftd = __expf(-G.R2 * R.inv2s2);   // the same exponential as the per-point term
     R.amp = G.Gamma * (0.159154943091895336f / s2);
     // No-wrap flag (kq[0] = kNoWrap): for every point that passes the tests, |W| <= Wm, so
     // |P| stays clear of both wrap thresholds and |x - c| < pi; the wrap bookkeeping of
@@ -525,25 +525,13 @@ __device__ __forceinline__ void segrec_from(const SegF &G, const SubSeg &S, SegR
 }
 
 // The three acceptance tests of tube.f90:806-818 for the grid point at offset d = x - ci0 in
-// the record's local frame: t0 >= 0, t1 < 0 and rho^2 < Rtube^2.  The arithmetic is spelled
-// out with explicit fmaf so that every caller (the row filter and the evaluation of the tile
-// kernel) decides a point identically.  t0 is returned for the spline argument.
-template <typename RecT>
-__device__ __forceinline__ bool rec_tests(const RecT &R, float d0x, float d0y, float d0z, float &t0)
-{
-    t0 = fmaf(d0z, R.tc0[2], fmaf(d0y, R.tc0[1], d0x * R.tc0[0]));
-    if (!(t0 >= 0.0f)) return false;
-    const float ex = d0x - R.dci[0], ey = d0y - R.dci[1], ez = d0z - R.dci[2];
-    const float t1 = fmaf(ez, R.tc1[2], fmaf(ey, R.tc1[1], ex * R.tc1[0]));
-    if (!(t1 < 0.0f)) return false;
-    const float r2 = fmaf(-t0, t0, fmaf(d0z, d0z, fmaf(d0y, d0y, d0x * d0x)));
-    return r2 < R.R2;
-}
-
-// rec_tests with the planes' rounding bound pe (plane_eps): 0 rejected, 1 accepted, 2 a plane
-// test within pe of zero.  The reference's field jumps across the plane shared by two
-// consecutive chords (zeta is interpolated along each chord separately), so such a pair is
-// decided by the reference's FP64 tests; beyond pe the FP32 signs are the FP64 signs.
+// the record's local frame (t0 >= 0, t1 < 0 and rho^2 < Rtube^2), with the planes' rounding
+// bound pe (plane_eps): 0 rejected, 1 accepted, 2 a plane test within pe of zero.  The
+// arithmetic is spelled out with explicit fmaf, and t0 is recomputed the same way for the
+// spline argument of an accepted pair.  The reference's field jumps across the plane shared
+// by two consecutive chords (zeta is interpolated along each chord separately), so a pair of
+// the third kind is decided by the reference's FP64 tests; beyond pe the FP32 signs are the
+// FP64 signs.
 template <typename RecT>
 __device__ __forceinline__ int rec_classify(const RecT &R, float d0x, float d0y, float d0z, float pe)
 {
@@ -577,9 +565,15 @@ __device__ __forceinline__ void vort_w(const RecT &R, float d0x, float d0y, floa
     float P[3], c1[3], Q[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
+        // P(W) by Horner's scheme, and P'(W) from its partial sums h_k by the derivative
+        // recurrence h0 + W (h1 + W (h2 + W (h3 + W b4))) = b0 + 2 b1 W + ... + 5 b4 W^4
         const float *b = R.b + 5 * d;
-        P[d] = W * fmaf(W, fmaf(W, fmaf(W, fmaf(W, b[4], b[3]), b[2]), b[1]), b[0]);
-        c1[d] = fmaf(W, fmaf(W, fmaf(W, fmaf(W, 5.0f * b[4], 4.0f * b[3]), 3.0f * b[2]), 2.0f * b[1]), b[0]);
+        const float h3 = fmaf(W, b[4], b[3]);
+        const float h2 = fmaf(W, h3, b[2]);
+        const float h1 = fmaf(W, h2, b[1]);
+        const float h0 = fmaf(W, h1, b[0]);
+        P[d] = W * h0;
+        c1[d] = fmaf(W, fmaf(W, fmaf(W, fmaf(W, b[4], h3), h2), h1), h0);
     }
     if constexpr (Delta) {
         const float u = zb, v = W;
@@ -612,7 +606,7 @@ __device__ __forceinline__ void vort_w(const RecT &R, float d0x, float d0y, floa
     const float in1 = rsqrtf(c1[0] * c1[0] + c1[1] * c1[1] + c1[2] * c1[2]);
     const float T[3] = {c1[0] * in1, c1[1] * in1, c1[2] * in1};
     if constexpr (!General) {
-        const float tp = (expf(-rho2 * R.inv2s2) - R.ftd) * R.amp;
+        const float tp = (__expf(-rho2 * R.inv2s2) - R.ftd) * R.amp;
         out[0] = tp * T[0];
         out[1] = tp * T[1];
         out[2] = tp * T[2];
@@ -629,7 +623,7 @@ __device__ __forceinline__ void vort_w(const RecT &R, float d0x, float d0y, floa
         const float sigma = fmaf(R.A, sn + 1.0f, R.smin);
         const float s2 = sigma * sigma;
         const float inv2s2 = 0.5f / s2;
-        const float tp = (expf(-rho2 * inv2s2) - expf(-R2 * inv2s2)) * (0.159154943f / s2) * R.Gamma;
+        const float tp = (__expf(-rho2 * inv2s2) - __expf(-R2 * inv2s2)) * (0.159154943f / s2) * R.Gamma;
         const float dsds = R.q * cs * in1 * R.Linv;
         const float rho = sqrtf(rho2);
         const float X[3] = {c1[1] * c2[2] - c1[2] * c2[1], c1[2] * c2[0] - c1[0] * c2[2], c1[0] * c2[1] - c1[1] * c2[0]};
@@ -659,7 +653,7 @@ __device__ __forceinline__ void vort_w(const RecT &R, float d0x, float d0y, floa
     }
 }
 
-// The vorticity of tube.f90:819-892 for a point that passed rec_tests with argument t0
+// The vorticity of tube.f90:819-892 for a point that passed rec_classify with argument t0
 // (sub-segment record: W = t0 g), and its curved-branch amplification.
 template <bool General, typename RecT>
 __device__ __forceinline__ void rec_vorticity(const RecT &R, float d0x, float d0y, float d0z, float t0, float out[3],

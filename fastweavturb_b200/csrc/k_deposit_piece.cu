@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(128, 3) piece_build_kernel(
     const double rt = Rtube_ratio * P.sigma_min;
     const float s2 = R.smin * R.smin;
     R.inv2s2 = 0.5f / s2;
-    R.ftd = expf(-(float)(rt * rt) * R.inv2s2);
+    R.ftd = __expf(-(float)(rt * rt) * R.inv2s2);   // the same exponential as the per-point term
     R.amp = R.Gamma * (0.159154943091895336f / s2);
     R.pad1 = 0;
 }
@@ -1058,12 +1058,14 @@ __device__ __forceinline__ void scatter_drain(ScatterStage &S, int lane, int cnt
         const int c = (int)(e & 31u), k = c >> 3, j = c & 7;
         const int rx = (int)((e >> 5) & 255u), ry = (int)((e >> 13) & 255u), rz = (int)((e >> 21) & 255u);
         const PieceRec &R = S.rec[k];
-        gx = (R.box_lo[0] - 1 + rx) % N;
-        gy = (R.box_lo[1] - 1 + ry) % N;
-        gz = (R.box_lo[2] - 1 + rz) % N;
-        gx += gx < 0 ? N : 0;
-        gy += gy < 0 ? N : 0;
-        gz += gz < 0 ? N : 0;
+        // unwrapped 0-based indices lie within one period of the domain (checked with the chord
+        // boxes): one conditional shift wraps them, no integer division
+        gx = R.box_lo[0] - 1 + rx;
+        gy = R.box_lo[1] - 1 + ry;
+        gz = R.box_lo[2] - 1 + rz;
+        gx += gx < 0 ? N : (gx >= N ? -N : 0);
+        gy += gy < 0 ? N : (gy >= N ? -N : 0);
+        gz += gz < 0 ? N : (gz >= N ? -N : 0);
         const bool inslab = gz >= zs && gz < zs + nz;
         const uint32_t id = ((uint32_t)(p0 + k) & ((1u << 26) - 1u)) | ((uint32_t)j << 26);
         if (inslab && (e & kSQDecide)) {
@@ -1143,7 +1145,9 @@ __global__ void __launch_bounds__(kScatterWarps * 32, 3) scatter_piece_kernel(
                     const int hi = unpack3(bhi, d);
                     cnn[d] = max(0, hi - co[d] + 1);
                     nonempty = nonempty && cnn[d] > 0;
-                    fits = fits && hi <= kScatterMaxOff;
+                    // 8-bit offsets, and unwrapped indices within one period of the domain
+                    const int u0 = R.box_lo[d] - 1 + co[d], u1 = R.box_lo[d] - 1 + hi;
+                    fits = fits && hi <= kScatterMaxOff && u0 >= -N && u1 < 2 * N;
                 }
                 if (!fits) {   // the host sends only pieces whose boxes fit: never expected
                     atomicOr(err, 64);
@@ -1450,7 +1454,7 @@ int launch_scatter(Ctx *c, const CenterlineBatch &B)
     int herr = 0;
     FWT_CUDA(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     FWT_CUDA(cudaStreamSynchronize(c->stream));
-    if (herr & 64) return fail(FWT_E_STATE, "scatter: a piece box wider than the candidate codes");
+    if (herr & 64) return fail(FWT_E_STATE, "scatter: a chord box beyond the candidate codes or one period");
     if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
     return defer_finish(c, rctx, D, B.npieces, c->defer_per_piece, launch);
 }

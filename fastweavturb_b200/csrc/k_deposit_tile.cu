@@ -203,8 +203,8 @@ struct WarpStage {
 constexpr size_t kDepSmem = kAccBytes + sizeof(WarpStage) * kDepWarps;
 constexpr uint32_t kQDecide = 1u << 15;
 
-// Evaluate the first `cnt` queued points of the warp, one per lane (rec_tests again for t0,
-// then the vorticity), add them into the tile's fixed-point cells and drop them from the queue.
+// Evaluate the first `cnt` queued points of the warp, one per lane (t0 again, then the
+// vorticity), add them into the tile's fixed-point cells and drop them from the queue.
 // Pairs whose curved-branch amplification exceeds kRedoCond, and pairs with a plane test
 // within its rounding bound (kQDecide), are deferred to FP64 (DeferList) instead.  In the
 // emit-only pass (D.emit_only) nothing is added and only the deferred pairs are listed again.
@@ -241,8 +241,9 @@ __device__ __forceinline__ void drain_queue(WarpStage &S, long long (*acc)[kAccN
             const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
             const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
             const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
-            float t0, vv[3], cond;
-            rec_tests(R, d0x, d0y, d0z, t0);
+            // the pair passed rec_classify: only t0 (the spline argument) is needed again
+            const float t0 = fmaf(d0z, R.tc0[2], fmaf(d0y, R.tc0[1], d0x * R.tc0[0]));
+            float vv[3], cond;
             rec_vorticity<General>(R, d0x, d0y, d0z, t0, vv, cond);
             const int p = lx + kSY * ly + kSZ * lz;
             flag = General && !(cond <= kRedoCond);

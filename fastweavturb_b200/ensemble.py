@@ -12,8 +12,9 @@ device, the field is built and its statistics stay on the device until read.
 Autotuner: before the first realisation of a grid size, the deposition of a probe
 realisation is timed over the deposition kernels' selection limits, one after the other: the
 tube radius (grid spacings) up to which lines take the chord-piece kernel instead of the
-sub-segment kernel, then the radius up to which pieces are rasterised once instead of searched
-per tile.  The fastest setting of each is kept for the rest of that size.  Every choice gives
+sub-segment kernel, then the radius up to which pieces are deposited without tiles (the
+scatter kernel), then the radius up to which the remaining pieces are rasterised once instead
+of searched per tile.  The fastest setting of each is kept for the rest of that size.  Every choice gives
 the same field within FP32 rounding; only the speed differs.  (The tile shape itself,
 16 x 8 x 8 points, is fixed at compile time.)
 
@@ -35,6 +36,7 @@ from .api import Context, Params, sp_exponents
 from .configs import build_workload
 
 TUNE_CANDIDATES = (0.0, 2.5, 5.0, 8.0)          # chord-piece kernel radius limit
+SCATTER_CANDIDATES = (0.0, 2.5, 5.0, 8.0)       # scatter kernel (no tiles) radius limit
 RASTER_CANDIDATES = (0.0, 1.5, 2.5, 4.0)        # rasterised pieces radius limit
 
 
@@ -58,16 +60,22 @@ class Ensemble:
                                                device=self.device, pdf_bins=201, Sp_order=self.Sp_order,
                                                vorticity_output=0))
                 if N in self.tuned:
-                    self.ctx[key].set_piece_radius_limit(self.tuned[N][0])
-                    self.ctx[key].set_raster_radius_limit(self.tuned[N][1])
+                    self._apply(self.ctx[key], self.tuned[N])
             return self.ctx[key]
+
+    @staticmethod
+    def _apply(ctx, tuned):
+        piece, scatter, raster = tuned
+        ctx.set_piece_radius_limit(piece)
+        ctx.set_scatter_radius_limit(scatter)
+        ctx.set_raster_radius_limit(raster)
 
     def _load(self, ctx, w):
         return build_workload(ctx, w)
 
     def autotune(self, w):
-        """Time the deposition of workload w over the piece limit, then over the raster limit
-        (at the best piece limit); keep the fastest of each."""
+        """Time the deposition of workload w over the piece limit, then the scatter limit, then
+        the raster limit (each at the best of the earlier ones); keep the fastest of each."""
         import torch
         ctx = self.context(w.N)
         keep = self._load(ctx, w)
@@ -82,21 +90,27 @@ class Ensemble:
 
         times = {}
         ctx.set_raster_radius_limit(-1.0)
+        ctx.set_scatter_radius_limit(-1.0)
         for cells in TUNE_CANDIDATES:
             ctx.set_piece_radius_limit(cells)
             times[("piece", cells)] = timed()
         best_piece = min(TUNE_CANDIDATES, key=lambda v: times[("piece", v)])
         ctx.set_piece_radius_limit(best_piece)
+        for cells in SCATTER_CANDIDATES:
+            ctx.set_scatter_radius_limit(cells)
+            times[("scatter", cells)] = timed()
+        best_scatter = min(SCATTER_CANDIDATES, key=lambda v: times[("scatter", v)])
+        ctx.set_scatter_radius_limit(best_scatter)
         for cells in RASTER_CANDIDATES:
             ctx.set_raster_radius_limit(cells)
             times[("raster", cells)] = timed()
         best_raster = min(RASTER_CANDIDATES, key=lambda v: times[("raster", v)])
+        tuned = (best_piece, best_scatter, best_raster)
         with self._lock:
             for (n, _), c in self.ctx.items():
                 if n == w.N:
-                    c.set_piece_radius_limit(best_piece)
-                    c.set_raster_radius_limit(best_raster)
-        self.tuned[w.N] = (best_piece, best_raster)
+                    self._apply(c, tuned)
+        self.tuned[w.N] = tuned
         self.tune_log[w.N] = times
         del keep
         return self.tuned[w.N]
