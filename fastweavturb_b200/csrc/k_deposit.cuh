@@ -506,7 +506,9 @@ __device__ __forceinline__ void segrec_from(const SegF &G, const SubSeg &S, SegR
     R.amp = G.Gamma * (0.159154943091895336f / s2);
     // No-wrap flag (kq[0] = kNoWrap): for every point that passes the tests, |W| <= Wm, so
     // |P| stays clear of both wrap thresholds and |x - c| < pi; the wrap bookkeeping of
-    // point_rec then reduces to x - c = d0 - P.
+    // point_rec then reduces to x - c = d0 - P.  An accepted point has 0 <= t0 <= dl + Rt
+    // (bends below 45 degrees, checked below) and a distance below Rt from the chord line, so
+    // |d0| <= sqrt((dl + Rt)^2 + Rt^2) and |x - c| <= |d0| + |P|.
     const float dl = sqrtf(G.dci[0] * G.dci[0] + G.dci[1] * G.dci[1] + G.dci[2] * G.dci[2]);
     const float Wm = (dl + G.Rt) * fabsf(G.g) * 1.01f;
     bool nowrap = true;
@@ -518,7 +520,7 @@ __device__ __forceinline__ void segrec_from(const SegF &G, const SubSeg &S, SegR
         pmax = fmaxf(pmax, pb);
         if (G.kq[d] != 0 || !(G.thi[d] > pb * 1.01f + 1e-5f) || !(G.tlo[d] < -pb * 1.01f - 1e-5f)) nowrap = false;
     }
-    if ((dl + 2.0f * G.Rt) * 1.7321f + pmax > 3.0f) nowrap = false;
+    if (sqrtf((dl + G.Rt) * (dl + G.Rt) + G.R2) + pmax > 3.0f) nowrap = false;
     // t0 <= dl + Rt tan(bend) <= dl + Rt holds for bends below 45 degrees
     if (G.tc0[0] * G.tc1[0] + G.tc0[1] * G.tc1[1] + G.tc0[2] * G.tc1[2] < 0.75f) nowrap = false;
     if (nowrap) R.kq[0] = kNoWrap;

@@ -1047,7 +1047,7 @@ __device__ __forceinline__ void scatter_test(ScatterStage &S, int lane, int cnt,
 // deferred.  Points outside the context's planes (a z-slab context) are dropped.
 template <bool General>
 __device__ __forceinline__ void scatter_drain(ScatterStage &S, int lane, int cnt, int &qn, int64_t p0, int N, int zs,
-                                              int nz, float fscale, unsigned long long *__restrict__ side, size_t n3,
+                                              int nz, float fscale, unsigned long long *__restrict__ side,
                                               int *__restrict__ err, const DeferList &D, unsigned long long &nacc)
 {
     bool flag = false, counted = false;
@@ -1092,7 +1092,7 @@ __device__ __forceinline__ void scatter_drain(ScatterStage &S, int lane, int cnt
                         atomicOr(err, 4);
                         sv = sv != sv ? 0.0f : copysignf(4.0e18f, sv);
                     }
-                    atomicAdd(side + (size_t)d * n3 + g, (unsigned long long)__float2ll_rn(sv));
+                    atomicAdd(side + kSideStride * g + d, (unsigned long long)__float2ll_rn(sv));
                 }
             }
         }
@@ -1111,7 +1111,7 @@ __device__ __forceinline__ void scatter_drain(ScatterStage &S, int lane, int cnt
 template <bool General>
 __global__ void __launch_bounds__(kScatterWarps * 32, 3) scatter_piece_kernel(
     const PieceRec *__restrict__ rec, int64_t npieces, int N, int zs, int nz, float fscale,
-    unsigned long long *__restrict__ side, size_t n3, int *__restrict__ err, const DeferList D,
+    unsigned long long *__restrict__ side, int *__restrict__ err, const DeferList D,
     unsigned long long *__restrict__ tally)
 {
     extern __shared__ __align__(16) unsigned char dsm[];
@@ -1192,15 +1192,15 @@ __global__ void __launch_bounds__(kScatterWarps * 32, 3) scatter_piece_kernel(
                 __syncwarp();
                 if (cn >= 32) {
                     scatter_test(S, lane, 32, cn, qn);
-                    if (qn >= 32) scatter_drain<General>(S, lane, 32, qn, p0, N, zs, nz, fscale, side, n3, err, D, nacc);
+                    if (qn >= 32) scatter_drain<General>(S, lane, 32, qn, p0, N, zs, nz, fscale, side, err, D, nacc);
                 }
             }
         }
         while (cn > 0) {
             scatter_test(S, lane, min(cn, 32), cn, qn);
-            if (qn >= 32) scatter_drain<General>(S, lane, 32, qn, p0, N, zs, nz, fscale, side, n3, err, D, nacc);
+            if (qn >= 32) scatter_drain<General>(S, lane, 32, qn, p0, N, zs, nz, fscale, side, err, D, nacc);
         }
-        while (qn > 0) scatter_drain<General>(S, lane, min(qn, 32), qn, p0, N, zs, nz, fscale, side, n3, err, D, nacc);
+        while (qn > 0) scatter_drain<General>(S, lane, min(qn, 32), qn, p0, N, zs, nz, fscale, side, err, D, nacc);
         __syncwarp();   // the warp's stage is reused by its next chunk
     }
     if (lane == 0 && tally && !D.emit_only && nacc) atomicAdd(tally, nacc);
@@ -1412,7 +1412,6 @@ int launch_scatter(Ctx *c, const CenterlineBatch &B)
     if (B.npieces >= ((int64_t)1 << 26)) return fail(FWT_E_RANGE, "piece batch exceeds 2^26");
     Ctx &C = *c;
     const int N = c->p.N;
-    const size_t n3 = field_elems(c);
     FWT_TRY(side_ensure(c));
     FWT_TRY(buf_reserve(c, C.scratch[19], 128));   // deposit_lines cleared the tallies at 64
     int *d_err = (int *)((char *)C.scratch[19].p + 104);
@@ -1435,12 +1434,12 @@ int launch_scatter(Ctx *c, const CenterlineBatch &B)
             FWT_CUDA(cudaFuncSetAttribute(scatter_piece_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)kScatterSmem));
             scatter_piece_kernel<true><<<grid, kScatterWarps * 32, kScatterSmem, c->stream>>>(
-                B.piece, B.npieces, N, zs, nz, (float)scale, side, n3, d_err, L, rctx.tally);
+                B.piece, B.npieces, N, zs, nz, (float)scale, side, d_err, L, rctx.tally);
         } else {
             FWT_CUDA(cudaFuncSetAttribute(scatter_piece_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)kScatterSmem));
             scatter_piece_kernel<false><<<grid, kScatterWarps * 32, kScatterSmem, c->stream>>>(
-                B.piece, B.npieces, N, zs, nz, (float)scale, side, n3, d_err, L, rctx.tally);
+                B.piece, B.npieces, N, zs, nz, (float)scale, side, d_err, L, rctx.tally);
         }
         FWT_CUDA(cudaGetLastError());
         kt_end(c, m);

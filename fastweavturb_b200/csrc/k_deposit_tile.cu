@@ -111,9 +111,14 @@ struct CandBox {
 
 // Index interval [ilo, ihi] (clamped to [0, n-1]) of the grid row d0 + i dx e_a that can pass
 // t0 >= 0, t1 < 0 and rho^2 < R2; a one-point margin covers the FP32 rounding of the bounds.
+// [clo, chi] is the row's core, where all three tests hold for certain: two points inside every
+// bound (the bounds' rounding is far below a point, and a plane two points away is far beyond
+// its rounding bound pe), and only when the row is bounded by both planes and the cylinder.
 __device__ __forceinline__ void row_interval(const SegRec &R, const CandBox &B, float d0x, float d0y, float d0z, int a,
-                                             int n, int &ilo, int &ihi)
+                                             int n, int &ilo, int &ihi, int &clo, int &chi)
 {
+    clo = 1;
+    chi = 0;
     const float dx = R.dx;
     const float T0 = d0x * R.tc0[0] + d0y * R.tc0[1] + d0z * R.tc0[2];
     const float ta = R.tc0[a];
@@ -143,6 +148,10 @@ __device__ __forceinline__ void row_interval(const SegRec &R, const CandBox &B, 
         const float sq = sqrtf(fmaxf(Q1 * Q1 - 4.0f * B.q2 * (Q0 - R.R2), 0.0f));
         lo = fmaxf(lo, (-Q1 - sq) * B.i2q);
         hi = fminf(hi, (-Q1 + sq) * B.i2q);
+        if (B.isb != 0.0f) {
+            clo = max(0, (int)ceilf(lo) + 2);
+            chi = min(n - 1, (int)floorf(hi) - 2);
+        }
     }
     ilo = max(0, (int)ceilf(lo) - 1);
     ihi = min(n - 1, (int)floorf(hi) + 1);
@@ -376,7 +385,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
                 if (t < nc && ot <= r) k = t;
             }
             const int rk = __shfl_sync(0xffffffffu, rowoff, k);
-            int i = 1, ihi = 0;
+            int i = 1, ihi = 0, clo = 1, chi = 0;
             int a = 0, lb0 = 0, lb1 = 0, lb2 = 0;
             if (r < total) {
                 const CandBox &B = S.box[k];
@@ -397,7 +406,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
                 const float d0z = fmaf((float)(B.dorg[2] + ez), R.dx, R.off[2]);
                 const int na = a == 0 ? B.n[0] : (a == 1 ? B.n[1] : B.n[2]);
                 int ilo;
-                row_interval(R, B, d0x, d0y, d0z, a, na, ilo, ihi);
+                row_interval(R, B, d0x, d0y, d0z, a, na, ilo, ihi, clo, chi);
                 i = ilo;
             }
             while (__any_sync(0xffffffffu, i <= ihi)) {
@@ -407,12 +416,14 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
                     const CandBox &B = S.box[k];
                     const SegRec &R = S.rec[k];
                     const int lx = lb0 + (a == 0 ? i : 0), ly = lb1 + (a == 1 ? i : 0), lz = lb2 + (a == 2 ? i : 0);
-                    const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
-                    const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
-                    const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
-                    int cls;
-                    if constexpr (F64) cls = rec_tests_wide(R, d0x, d0y, d0z) ? 1 : 0;
-                    else cls = rec_classify(R, d0x, d0y, d0z, B.pe);
+                    int cls = 1;   // the row's core passes for certain
+                    if (F64 || i < clo || i > chi) {
+                        const float d0x = fmaf((float)(lx + B.dl[0]), R.dx, R.off[0]);
+                        const float d0y = fmaf((float)(ly + B.dl[1]), R.dx, R.off[1]);
+                        const float d0z = fmaf((float)(lz + B.dl[2]), R.dx, R.off[2]);
+                        if constexpr (F64) cls = rec_tests_wide(R, d0x, d0y, d0z) ? 1 : 0;
+                        else cls = rec_classify(R, d0x, d0y, d0z, B.pe);
+                    }
                     ok = cls != 0;
                     code = (uint32_t)k | ((uint32_t)lx << 4) | ((uint32_t)ly << 8) | ((uint32_t)lz << 11) |
                            (cls == 2 ? kQDecide : 0u);
@@ -487,9 +498,10 @@ double fixed_point_scale(const Ctx *c)
 
 // ------------------------------------------------------------------ deferred pairs
 // One thread per deferred pair: the reference's FP64 tests (decided pairs) and vorticity
-// (redo_pair_f64), added as int64 fixed point into the side accumulator side[3][n3].
+// (redo_pair_f64), added as int64 fixed point into the side accumulator (kSideStride int64 per
+// grid point: x, y, z and a pad, one 32-byte sector).
 __global__ void __launch_bounds__(128) redo_apply_kernel(const RedoCtx R, const Deferred *__restrict__ e, int64_t n,
-                                                         unsigned long long *__restrict__ side, size_t n3,
+                                                         unsigned long long *__restrict__ side,
                                                          int *__restrict__ err)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -505,7 +517,7 @@ __global__ void __launch_bounds__(128) redo_apply_kernel(const RedoCtx R, const 
             const size_t g = (size_t)gx + (size_t)R.N * ((size_t)gy + (size_t)R.N * (size_t)(gz - R.zs));
 #pragma unroll
             for (int k = 0; k < 3; ++k)
-                if (q[k] != 0) atomicAdd(side + (size_t)k * n3 + g, (unsigned long long)q[k]);
+                if (q[k] != 0) atomicAdd(side + kSideStride * g + k, (unsigned long long)q[k]);
         }
         taken = decide && r != 0;
     }
@@ -519,15 +531,20 @@ __global__ void __launch_bounds__(128) redo_apply_kernel(const RedoCtx R, const 
     }
 }
 
-// omega += side / scale where side holds a sum, and side back to zero.
-__global__ void side_fold_kernel(float *__restrict__ w, unsigned long long *__restrict__ side, size_t n, double inv)
+// omega += side / scale where side holds a sum (n3 grid points, three components of omega
+// n3 apart), and side back to zero.
+__global__ void side_fold_kernel(float *__restrict__ w, unsigned long long *__restrict__ side, size_t n3, double inv)
 {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const long long v = (long long)side[i];
-        if (v != 0) {
-            w[i] = (float)((double)w[i] + (double)v * inv);
-            side[i] = 0ull;
-        }
+    for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n3; g += (size_t)gridDim.x * blockDim.x) {
+        ulonglong2 *s2 = reinterpret_cast<ulonglong2 *>(side + kSideStride * g);
+        const ulonglong2 a = s2[0], b = s2[1];
+        const long long v[3] = {(long long)a.x, (long long)a.y, (long long)b.x};
+        if ((v[0] | v[1] | v[2]) == 0) continue;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (v[d] != 0) w[(size_t)d * n3 + g] = (float)((double)w[(size_t)d * n3 + g] + (double)v[d] * inv);
+        s2[0] = make_ulonglong2(0ull, 0ull);
+        s2[1] = make_ulonglong2(0ull, 0ull);
     }
 }
 
@@ -564,7 +581,7 @@ void defer_rate(double &rate, unsigned long long n, int64_t units)
 
 int side_ensure(Ctx *c)
 {
-    const size_t bytes = 3 * field_elems(c) * sizeof(unsigned long long);
+    const size_t bytes = kSideStride * field_elems(c) * sizeof(unsigned long long);
     if (!c->b_side.p || c->b_side.bytes < bytes) {
         buf_free(c, c->b_side);
         FWT_TRY(buf_reserve(c, c->b_side, bytes));
@@ -584,7 +601,7 @@ int defer_apply(Ctx *c, const RedoCtx &R, const DeferList &D, unsigned long long
     FWT_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), c->stream));
     const int km = kt_begin(c, KT_DEPOSIT);
     redo_apply_kernel<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(R, D.e, (int64_t)n,
-                                                                          (unsigned long long *)c->b_side.p, n3, d_err);
+                                                                          (unsigned long long *)c->b_side.p, d_err);
     kt_end(c, km);
     c->launches += 1;
     FWT_CUDA(cudaGetLastError());
@@ -599,7 +616,7 @@ int defer_apply(Ctx *c, const RedoCtx &R, const DeferList &D, unsigned long long
 int side_fold(Ctx *c)
 {
     if (!c->side_dirty) return 0;
-    const size_t n = 3 * field_elems(c);
+    const size_t n = field_elems(c);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
     const int km = kt_begin(c, KT_DEPOSIT);

@@ -343,6 +343,10 @@ struct Deferred {
     uint32_t pad;
 };
 constexpr uint32_t kDeferDecide = 1u << 31;
+// int64 words per grid point of the side accumulator: x, y, z and a pad, so that the three
+// reductions of a pair meet one 32-byte sector (three arrays would touch three, each a DRAM
+// read-modify-write when the accumulator is larger than L2)
+constexpr size_t kSideStride = 4;
 
 struct DeferList {
     Deferred *e;
@@ -374,7 +378,7 @@ RedoCtx redo_ctx(const Ctx *c, const CenterlineBatch &B, double scale, bool piec
 // The deferred-pair list of a launch over `units` work units ((tile, record) pairs, or pieces),
 // sized from the running rate of deferred pairs per unit (k_deposit_tile.cu).
 int defer_list(Ctx *c, int64_t units, double rate, DeferList &D);
-// The side accumulator (3 x the field, int64), allocated and zeroed on first use.
+// The side accumulator (kSideStride int64 per grid point), allocated and zeroed on first use.
 int side_ensure(Ctx *c);
 
 // Evaluate the first n pairs of the list in FP64 into the side accumulator (k_deposit_tile.cu).
