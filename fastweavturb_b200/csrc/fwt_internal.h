@@ -104,13 +104,13 @@ struct Ctx {
     size_t fft_ws_bytes = 0;
 
     // scratch (centerline set-up, deposition, statistics)
-    DevBuf scratch[28];
+    DevBuf scratch[29];
     // pairs the FP32 tile kernels defer to FP64 (k_tile_common.cuh): their list, and the int64
     // fixed-point sums of their contributions (3 x the field), folded into omega by side_fold
     DevBuf b_defer, b_side;
     bool side_dirty = false;
-    double defer_per_pair = 0.5;   // deferred pairs per (tile, record) pair of the last tile launch
-    double defer_per_piece = 0.5;  // deferred pairs per piece of the last scatter launch
+    double defer_per_pair = 0.2;   // deferred pairs per (tile, record) pair of the last tile launch
+    double defer_per_piece = 0.05; // deferred pairs per piece of the last scatter launch
     double scatter_rt_cells = -1.0;  // tuning: radius limit of the scatter path in grid spacings (< 0: default)
 
     // state

@@ -1,8 +1,9 @@
 // k_centerline.cu -- centerline set-up on the device, all FP64 (one B200 runs FP64 at half
 // the FP32 rate, and the integer sub-segment counts must follow the reference):
 //   line_prep_kernel   periodic arc length cze, Len_Disc, c', c''       tube.f90:392-515
-//   section_kernel     quintic coefficients + turning-angle ntf/dtf      tube.f90:561-657,
-//                                                                       subroutine.f90:440-488
+//   section_coe_kernel quintic coefficients                              subroutine.f90:440-488
+//   section_kernel     turning-angle sum, one warp per section           tube.f90:625-657
+//   section_ntf_kernel ntf/dtf, FP64 recompute list near a step of ceil  tube.f90:655-657
 //   sample_kernel      sample points ci with the endpoint copy          tube.f90:706-723
 //   chord_kernel       chords dci, |dci|, unit chords tci               tube.f90:740-751
 //   subseg_kernel      sub-segment records (unwrap, Rtube, box)          tube.f90:766-798
@@ -141,21 +142,26 @@ __device__ __forceinline__ float turning_integrand(const float *cf, float z)
     return __fdividef(nx, ndc2);
 }
 
-// One warp per section slot (n_sec + 1 slots per line; slot n_sec is the periodic copy).
-__global__ void section_kernel(const LineParam *__restrict__ lp, const int *__restrict__ slot_line, int64_t nslots,
-                               const double *__restrict__ X, const double *__restrict__ Y,
-                               const double *__restrict__ Z, const double *__restrict__ cze,
-                               const double *__restrict__ ck, const double *__restrict__ ckk,
-                               const double *__restrict__ Len, int64_t node_base, int ntf_times, int ntf_pre,
-                               double *__restrict__ coe_out, int *__restrict__ ntf_out, double *__restrict__ dtf_out,
-                               unsigned *__restrict__ near)   // near[0]: count, near[4 + i]: marked slots
+// Sections in three passes (n_sec + 1 slots per line; slot n_sec is the periodic copy): the
+// quintic coefficients and the sample step, one thread per slot (section_coe_kernel); the
+// turning-angle sum, one warp per slot (section_kernel); ntf and dtf, one thread per slot
+// (section_ntf_kernel).  The FP64 arithmetic of the first and last pass runs on every lane
+// instead of three lanes of the summing warp.
+
+// get_spline_5th_coe (subroutine.f90:440-461) for the three coordinates of slot s, and the FP32
+// sample step dtf_pre * Len of the turning-angle sum.
+__global__ void section_coe_kernel(const LineParam *__restrict__ lp, const int *__restrict__ slot_line, int64_t nslots,
+                                   const double *__restrict__ X, const double *__restrict__ Y,
+                                   const double *__restrict__ Z, const double *__restrict__ cze,
+                                   const double *__restrict__ ck, const double *__restrict__ ckk,
+                                   const double *__restrict__ Len, int64_t node_base, int ntf_pre,
+                                   double *__restrict__ coe_out, float *__restrict__ zstep_out)
 {
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= nslots) return;
-    const int l = slot_line[warp];
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const int l = slot_line[s];
     const LineParam P = lp[l];
-    const int t = (int)(warp - P.slot_off);
+    const int t = (int)(s - P.slot_off);
     const int np = P.n_sec;
     const int64_t o = P.node_off - node_base;
     const double L = Len[l];
@@ -166,11 +172,9 @@ __global__ void section_kernel(const LineParam *__restrict__ lp, const int *__re
     const double zl = cze_pl_at(cz_line, np, t), zr_ = cze_pl_at(cz_line, np, t + 1);
     // spline argument is cze_pl*Len (tube.f90:598)
     const double zr = zr_ * L - zl * L;
-    // lane d < 3 builds coordinate d's coefficients in FP64 (get_spline_5th_coe,
-    // subroutine.f90:440-461); the other lanes get their FP32 copies by shuffles
-    double a6[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (lane < 3) {
-        const int d = lane;
+    const double z2 = zr * zr, z3 = z2 * zr, z4 = z3 * zr, z5 = z4 * zr;
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
         const double *cd = (d == 0 ? X : (d == 1 ? Y : Z)) + P.node_off;
         const double xl = cd[il], xr = cd[ir];
         const double vl = ck[3 * (o + il) + d], vr = ck[3 * (o + ir) + d];
@@ -178,27 +182,33 @@ __global__ void section_kernel(const LineParam *__restrict__ lp, const int *__re
         double xpl = xl, xpr = xr;
         if (xl - xr > dev_pi()) xpr = xr + dev_pi2();
         else if (xl - xr < -dev_pi()) xpl = xl + dev_pi2();
-        const double z2 = zr * zr, z3 = z2 * zr, z4 = z3 * zr, z5 = z4 * zr;
+        double *a6 = coe_out + 18 * s + 6 * d;
         a6[0] = xl;
         a6[1] = vl;
         a6[2] = al / 2.0;
         a6[3] = (20.0 * (xpr - xpl) - (12.0 * vl + 8.0 * vr) * zr - (3.0 * al - ar) * z2) / (2.0 * z3);
         a6[4] = (-30.0 * (xpr - xpl) + (16.0 * vl + 14.0 * vr) * zr + (3.0 * al - 2.0 * ar) * z2) / (2.0 * z4);
         a6[5] = (12.0 * (xpr - xpl) - 6.0 * (vl + vr) * zr - (al - ar) * z2) / (2.0 * z5);
-#pragma unroll
-        for (int m = 0; m < 6; ++m) coe_out[18 * warp + 6 * d + m] = a6[m];
     }
-    // turning angle theta = sum |c' x c''| / |c'|^2 * dtf_pre * Len over ntf_pre+1 samples.
-    // The integrand is evaluated in FP32 and summed in FP64; a result that falls near a step of
-    // ceil(ntf_times theta / 2 pi) is marked (ntf = 0) and recomputed in FP64 by
-    // section_fp64_kernel, which keeps the FP64 code and its registers out of this loop.
     const double dtfp = (zr_ - zl) / (1.0 * ntf_pre);
+    zstep_out[s] = (float)(dtfp * L);
+}
+
+// The turning-angle sum of slot `warp` (tube.f90:625-657): sum |c' x c''| / |c'|^2 over
+// ntf_pre + 1 samples, the integrand in FP32 from the FP32 coefficients, the sum in FP64
+// (without the factor dtf_pre * Len, applied by section_ntf_kernel).
+__global__ void section_kernel(int64_t nslots, int ntf_pre, const double *__restrict__ coe,
+                               const float *__restrict__ zstep_in, double *__restrict__ tsum_out)
+{
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= nslots) return;
+    // lane m < 18 loads coefficient m; every lane takes the FP32 copies by shuffles
+    const float mine = lane < 18 ? (float)coe[18 * warp + lane] : 0.0f;
     float cf[18];
 #pragma unroll
-    for (int d = 0; d < 3; ++d)
-#pragma unroll
-        for (int m = 0; m < 6; ++m) cf[6 * d + m] = __shfl_sync(0xffffffffu, (float)a6[m], d);
-    const float zstep = (float)(dtfp * L), z64 = 64.0f * zstep;
+    for (int m = 0; m < 18; ++m) cf[m] = __shfl_sync(0xffffffffu, mine, m);
+    const float zstep = zstep_in[warp], z64 = 64.0f * zstep;
     float th0 = 0.0f, th1 = 0.0f;
     int tj = lane;
     float za = zstep * (float)lane, zb = zstep * (float)(lane + 32);
@@ -209,16 +219,37 @@ __global__ void section_kernel(const LineParam *__restrict__ lp, const int *__re
         zb += z64;
     }
     if (tj <= ntf_pre) th0 += turning_integrand(cf, za);
-    const double th32 = warp_sum((double)th0 + (double)th1) * dtfp * L;
+    const double sum = warp_sum((double)th0 + (double)th1);
+    if (lane == 0) tsum_out[warp] = sum;
+}
+
+// ntf = ceil(ntf_times theta / 2 pi) + 1 and dtf of slot s, theta = sum * dtf_pre * Len.  The
+// integrand was evaluated in FP32; a result that falls near a step of ceil is marked (ntf = 0)
+// and recomputed in FP64 by section_fp64_kernel.
+__global__ void section_ntf_kernel(const LineParam *__restrict__ lp, const int *__restrict__ slot_line, int64_t nslots,
+                                   const double *__restrict__ cze, const double *__restrict__ Len, int64_t node_base,
+                                   int ntf_times, int ntf_pre, const double *__restrict__ tsum,
+                                   int *__restrict__ ntf_out, double *__restrict__ dtf_out,
+                                   unsigned *__restrict__ near)   // near[0]: count, near[4 + i]: marked slots
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const int l = slot_line[s];
+    const LineParam P = lp[l];
+    const int t = (int)(s - P.slot_off);
+    const int np = P.n_sec;
+    const double L = Len[l];
+    const double *cz_line = cze + (P.node_off - node_base);
+    const double zl = cze_pl_at(cz_line, np, t), zr_ = cze_pl_at(cz_line, np, t + 1);
+    const double dtfp = (zr_ - zl) / (1.0 * ntf_pre);
+    const double th32 = tsum[s] * dtfp * L;
     const double xr = ntf_times * th32 / dev_pi2();
     const double fr = xr - floor(xr);
     const bool near_step = fmin(fr, 1.0 - fr) < 1e-4 * (xr + 1.0) || !(xr == xr);
-    if (lane == 0) {
-        const int ntf = near_step ? 0 : (int)ceil(xr) + 1;
-        if (near_step) near[4 + atomicAdd(near, 1u)] = (unsigned)warp;
-        ntf_out[warp] = ntf;
-        dtf_out[warp] = near_step ? 0.0 : (zr_ - zl) / (1.0 * ntf);
-    }
+    const int ntf = near_step ? 0 : (int)ceil(xr) + 1;
+    if (near_step) near[4 + atomicAdd(near, 1u)] = (unsigned)s;
+    ntf_out[s] = ntf;
+    dtf_out[s] = near_step ? 0.0 : (zr_ - zl) / (1.0 * ntf);
 }
 
 // FP64 turning angle of the sections section_kernel marked (ntf = 0), taken from its list of
@@ -791,13 +822,19 @@ int centerline_setup(Ctx *c, int la, int lb, CenterlineBatch &B, BatchRecords mo
     FWT_TRY(buf_reserve(c, C.scratch[24], sizeof(unsigned) * (size_t)(slots + 4)));   // near-step list
     unsigned *d_near = (unsigned *)C.scratch[24].p;
     FWT_CUDA(cudaMemsetAsync(d_near, 0, sizeof(unsigned), c->stream));
-    section_kernel<<<wblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, c->d_x, c->d_y, c->d_z, B.cze, B.ck,
-                                                   B.ckk, B.Len, B.node_base, c->p.ntf_times, c->p.ntf_pre,
-                                                   B.coe, B.ntf, B.dtf, d_near);
+    FWT_TRY(buf_reserve(c, C.scratch[28], (sizeof(double) + sizeof(float)) * (size_t)std::max<int64_t>(slots, 1)));
+    double *d_tsum = (double *)C.scratch[28].p;
+    float *d_zstep = (float *)(d_tsum + slots);
+    const unsigned tblocks = (unsigned)((slots + 255) / 256);
+    section_coe_kernel<<<tblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, c->d_x, c->d_y, c->d_z, B.cze, B.ck,
+                                                      B.ckk, B.Len, B.node_base, c->p.ntf_pre, B.coe, d_zstep);
+    section_kernel<<<wblocks, 256, 0, c->stream>>>(slots, c->p.ntf_pre, B.coe, d_zstep, d_tsum);
+    section_ntf_kernel<<<tblocks, 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.cze, B.Len, B.node_base,
+                                                      c->p.ntf_times, c->p.ntf_pre, d_tsum, B.ntf, B.dtf, d_near);
     // a fixed grid: the list holds a few sections per thousand
     section_fp64_kernel<<<4 * 148, 256, 0, c->stream>>>(B.lp, B.slot_line, B.cze, B.Len, B.node_base,
                                                         c->p.ntf_times, c->p.ntf_pre, B.coe, d_near, B.ntf, B.dtf);
-    c->launches += 2;
+    c->launches += 4;
     kt_end(c, km);
     km = kt_begin(c, KT_CENTERLINE);
     slot_counts_kernel<<<(unsigned)((slots + 255) / 256), 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf,

@@ -85,17 +85,18 @@ __global__ void piece_map_kernel(const LineParam *__restrict__ lp, const int *__
 // One thread per piece: FP64 samples, chords and boxes as the sub-segment set-up
 // (tube.f90:703-798), then the FP32 record in the piece's frame.  err bit 8: a piece box
 // wider than 1023 points (the 10-bit chord box offsets).
-__global__ void __launch_bounds__(128, 3) piece_build_kernel(
+constexpr int kBuildThreads = 64;   // piece_build_kernel's block: 32 KB of shared memory, six per SM
+__global__ void __launch_bounds__(kBuildThreads, 6) piece_build_kernel(
     const LineParam *__restrict__ lp, const int *__restrict__ slot_line, const int *__restrict__ map, int64_t npieces,
     const double *__restrict__ X, const double *__restrict__ Y, const double *__restrict__ Z,
     const double *__restrict__ cze, int64_t node_base, const double *__restrict__ coe, const int *__restrict__ ntf,
     const double *__restrict__ dtf, const int64_t *__restrict__ poff, int N, double Rtube_ratio, double dzeta_sup,
     double eta, PieceRec *__restrict__ rec, int *__restrict__ err)
 {
-    // the section's 18 coefficients are read by every sample evaluation of both passes: one
+    // the section's 18 coefficients are read by every sample evaluation of the walk: one
     // global read each into this thread's row of shared memory (rows of 19 doubles spread the
     // banks), instead of about 20 x 18 global loads that throttled the load/store unit
-    __shared__ double s_cf[128][19];
+    __shared__ double s_cf[kBuildThreads][19];
     const int64_t pc = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pc >= npieces) return;
     const int slot = map[pc];
@@ -177,13 +178,22 @@ __global__ void __launch_bounds__(128, 3) piece_build_kernel(
             sample(j + 2, cb);   // j + 2 <= j0 + n + 1 <= ntf + 1
         }
     };
-    // pass 1: the piece box (union of the chord boxes), the largest Rtube, extent and bend
+    // One walk: per chord its plane (pl), its constants (chq) and its sample's z offset, and
+    // the piece box (union of the chord boxes), the largest Rtube, the extent and the bend.  The
+    // records' offsets depend on the piece box, so the samples' piece-frame offsets pj and the
+    // chord boxes (relative to chord 0's) wait in shared memory until the walk is done.
+    __shared__ double s_pj[kBuildThreads][kPieceMax + 1][3];
+    __shared__ float s_zoff[kBuildThreads][kPieceMax + 1];
+    __shared__ short s_box[kBuildThreads][kPieceMax][6];
+    const int tid = threadIdx.x;
+    PieceRec &R = rec[pc];
     int blo[3] = {1 << 30, 1 << 30, 1 << 30}, bhi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
+    int b0[3] = {0, 0, 0};   // chord 0's box origin: the reference of s_box
     double Rmax = 0.0, dlen = 0.0;
-    float bendmin = 1.0f;
+    float bendmin = 1.0f, Wm = 0.0f, cmax = 0.0f;
     double tprev[3] = {0.0, 0.0, 0.0};
-    walk([&](int jj, const double *ch, double nd, const double *pj, const int *lo3, const int *hi3, double, double,
-             double Rt) {
+    walk([&](int jj, const double *ch, double nd, const double *pj, const int *lo3, const int *hi3, double s0,
+             double s1, double Rt) {
         const double inv = 1.0 / nd;
         const double tc[3] = {ch[0] * inv, ch[1] * inv, ch[2] * inv};
         if (jj > 0) bendmin = fminf(bendmin, (float)(tc[0] * tprev[0] + tc[1] * tprev[1] + tc[2] * tprev[2]));
@@ -191,15 +201,32 @@ __global__ void __launch_bounds__(128, 3) piece_build_kernel(
         tprev[1] = tc[1];
         tprev[2] = tc[2];
         dlen = fmax(dlen, sqrt(pj[0] * pj[0] + pj[1] * pj[1] + pj[2] * pj[2]));
+        const float ck = (float)(tc[0] * pj[0] + tc[1] * pj[1] + tc[2] * pj[2]);
+        R.pl[jj] = make_float4((float)tc[0], (float)tc[1], (float)tc[2], ck);
+        cmax = fmaxf(cmax, fabsf(ck));
+        const float zoff = (float)((s0 - zj0) * L);
+        s_zoff[tid][jj] = zoff;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) s_pj[tid][jj][k] = pj[k];
         if (jj == n) return;
         Rmax = fmax(Rmax, Rt);
+        if (jj == 0) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) b0[k] = lo3[k];
+        }
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             blo[k] = min(blo[k], lo3[k]);
             bhi[k] = max(bhi[k], hi3[k]);
+            // within +-32767 of chord 0's origin: the piece box is checked below 1024 wide
+            s_box[tid][jj][k] = (short)max(-32767, min(32767, lo3[k] - b0[k]));
+            s_box[tid][jj][3 + k] = (short)max(-32767, min(32767, hi3[k] - b0[k]));
         }
+        const float g = (float)((s1 - s0) * L * inv);
+        R.chq[jj] = make_float4(g, (float)(Rt * Rt), 0.0f, 0.0f);
+        Wm = fmaxf(Wm, (zoff + (float)(nd + Rt) * fabsf(g)) * 1.01f);
     });
-    PieceRec &R = rec[pc];
+    double X0[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         if (bhi[k] - blo[k] > 1023) atomicOr(err, 8);
@@ -207,37 +234,23 @@ __global__ void __launch_bounds__(128, 3) piece_build_kernel(
         R.box_lo[k] = blo[k];
         R.box_hi[k] = bhi[k];
         // mesh coordinate of the 1-based unwrapped index box_lo: (i - 1) dx + xstart
-        const double X0 = dadd(dmul((double)blo[k] - 1.0, dev_pi2() / N), xstart);
-        R.off[k] = (float)(X0 - o[k]);
+        X0[k] = dadd(dmul((double)blo[k] - 1.0, dev_pi2() / N), xstart);
+        R.off[k] = (float)(X0[k] - o[k]);
     }
     R.dx = (float)(dev_pi2() / N);
     R.nch = n;
-    // pass 2: planes, per-sample frames and chords
-    float Wm = 0.0f, cmax = 0.0f;
-    walk([&](int jj, const double *ch, double nd, const double *pj, const int *lo3, const int *hi3, double s0,
-             double s1, double Rt) {
-        const double inv = 1.0 / nd;
-        const double tc[3] = {ch[0] * inv, ch[1] * inv, ch[2] * inv};
-        const float ck = (float)(tc[0] * pj[0] + tc[1] * pj[1] + tc[2] * pj[2]);
-        R.pl[jj] = make_float4((float)tc[0], (float)tc[1], (float)tc[2], ck);
-        cmax = fmaxf(cmax, fabsf(ck));
-        // mesh point at box_lo minus sample jj (FP64, then FP32): the sample's own local frame,
-        // as accurate as a sub-segment record's
+    // per sample: mesh point at box_lo minus sample jj (FP64, then FP32), the sample's own local
+    // frame, as accurate as a sub-segment record's; per chord: its box relative to box_lo
+    for (int jj = 0; jj <= n; ++jj) {
         float offj[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const double X0 = dadd(dmul((double)blo[k] - 1.0, dev_pi2() / N), xstart);
-            offj[k] = (float)(X0 - (o[k] + pj[k]));
-        }
-        const float zoff = (float)((s0 - zj0) * L);
-        R.po[jj] = make_float4(offj[0], offj[1], offj[2], zoff);
-        if (jj == n) return;
-        const float g = (float)((s1 - s0) * L * inv);
-        R.chq[jj] = make_float4(g, (float)(Rt * Rt),
-                                __uint_as_float(pack3(lo3[0] - blo[0], lo3[1] - blo[1], lo3[2] - blo[2])),
-                                __uint_as_float(pack3(hi3[0] - blo[0], hi3[1] - blo[1], hi3[2] - blo[2])));
-        Wm = fmaxf(Wm, (zoff + (float)(nd + Rt) * fabsf(g)) * 1.01f);
-    });
+        for (int k = 0; k < 3; ++k) offj[k] = (float)(X0[k] - (o[k] + s_pj[tid][jj][k]));
+        R.po[jj] = make_float4(offj[0], offj[1], offj[2], s_zoff[tid][jj]);
+        if (jj == n) break;
+        const int sh[3] = {b0[0] - blo[0], b0[1] - blo[1], b0[2] - blo[2]};
+        R.chq[jj].z = __uint_as_float(pack3(s_box[tid][jj][0] + sh[0], s_box[tid][jj][1] + sh[1], s_box[tid][jj][2] + sh[2]));
+        R.chq[jj].w = __uint_as_float(pack3(s_box[tid][jj][3] + sh[0], s_box[tid][jj][4] + sh[1], s_box[tid][jj][5] + sh[2]));
+    }
     // FP32 rounding of the piece-frame plane test d . tci_k - c_k: the offsets d (off, dx and
     // the fma, at most 4 u max|d_k| per axis), the normal (u |d|_1), c_k (u |c_k|) and the three
     // fused sums (u (|d|_1 + |c_k|) each) add up to 8 u (|d|_1 + |c_k|) with u = 2^-24, below
@@ -1237,7 +1250,7 @@ int piece_setup(Ctx *c, CenterlineBatch &B)
     piece_map_kernel<<<(unsigned)((slots + 255) / 256), 256, 0, c->stream>>>(B.lp, B.slot_line, slots, B.ntf,
                                                                               d_poff, d_map);
     if (np_ > 0)
-        piece_build_kernel<<<(unsigned)((np_ + 127) / 128), 128, 0, c->stream>>>(
+        piece_build_kernel<<<(unsigned)((np_ + kBuildThreads - 1) / kBuildThreads), kBuildThreads, 0, c->stream>>>(
             B.lp, B.slot_line, d_map, np_, c->d_x, c->d_y, c->d_z, B.cze, B.node_base, B.coe, B.ntf, B.dtf, d_poff,
             c->p.N, c->p.Rtube_ratio, c->p.dzeta_sup, c->p.eta_t, B.piece, d_err);
     kt_end(c, km);

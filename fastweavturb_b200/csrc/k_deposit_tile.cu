@@ -550,7 +550,9 @@ __global__ void side_fold_kernel(float *__restrict__ w, unsigned long long *__re
 
 int defer_list(Ctx *c, int64_t units, double rate, DeferList &D)
 {
-    const double want = std::max(1.0 * (1 << 20), 1.5 * rate * (double)units);
+    // 1.5 times the last launch's rate, between 1 Mi and 16 Mi pairs (256 MB) unless a larger
+    // list is already held; an overflow is refilled at its counted size (defer_finish)
+    const double want = std::min(std::max(1.0 * (1 << 20), 1.5 * rate * (double)units), 1.0 * (1 << 24));
     const unsigned long long cap = (unsigned long long)want;
     FWT_TRY(buf_reserve(c, c->b_defer, 16 + sizeof(Deferred) * (size_t)cap));
     D.count = (unsigned long long *)c->b_defer.p;
