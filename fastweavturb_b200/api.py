@@ -356,6 +356,11 @@ class Context:
         tiles, with int64 global reductions (0: never; negative: the default, 5)."""
         _check(library().fwt_set_tuning(self._h, 3, float(cells)))
 
+    def set_defer_limit(self, pairs):
+        """Most entries the list of pairs handed from FP32 to FP64 grows to; more are listed
+        and evaluated in windows of tiles or pieces (below 1: the default, 2^26)."""
+        _check(library().fwt_set_tuning(self._h, 4, float(pairs)))
+
     def counters(self):
         v = np.zeros(7, dtype=np.int64)
         library().fwt_counters(self._h, _ptr(v, ctypes.c_int64), 7)

@@ -697,6 +697,10 @@ int fwt_set_tuning(fwt_ctx *h, int key, double value)
         c->scatter_rt_cells = value;
         return 0;
     }
+    if (key == FWT_TUNE_DEFER_MAX_PAIRS) {
+        c->defer_max_pairs = value;
+        return 0;
+    }
     return fail(FWT_E_ARG, "unknown tuning key");
 }
 

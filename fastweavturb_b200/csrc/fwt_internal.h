@@ -106,12 +106,14 @@ struct Ctx {
     // scratch (centerline set-up, deposition, statistics)
     DevBuf scratch[29];
     // pairs the FP32 tile kernels defer to FP64 (k_tile_common.cuh): their list, and the int64
-    // fixed-point sums of their contributions (3 x the field), folded into omega by side_fold
+    // fixed-point sums of their contributions (kSideStride int64 per grid point), folded into
+    // omega by side_fold
     DevBuf b_defer, b_side;
     bool side_dirty = false;
     double defer_per_pair = 0.2;   // deferred pairs per (tile, record) pair of the last tile launch
     double defer_per_piece = 0.05; // deferred pairs per piece of the last scatter launch
     double scatter_rt_cells = -1.0;  // tuning: radius limit of the scatter path in grid spacings (< 0: default)
+    double defer_max_pairs = 0.0;    // tuning: entries an overflowed deferred list grows to (<= 0: 2^26)
 
     // state
     bool have_w = false, have_u = false, normalised = false;

@@ -825,7 +825,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_piece_kernel
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     long long(*acc)[kAccN] = reinterpret_cast<long long(*)[kAccN]>(dsm);
-    const int tile = blockIdx.x;
+    const int tile = (int)D.w0 + blockIdx.x;
     const int64_t c0 = tile_off[tile], c1 = tile_off[tile + 1];
     // a tile that no record of this batch meets keeps its values: earlier batches wrote them,
     // or the field was cleared before the first
@@ -1133,7 +1133,8 @@ __global__ void __launch_bounds__(kScatterWarps * 32, 3) scatter_piece_kernel(
     const int64_t nchunks = (npieces + kPChunk - 1) / kPChunk;
     const int64_t nw = (int64_t)gridDim.x * kScatterWarps;
     unsigned long long nacc = 0;   // pairs evaluated by this warp (warp-uniform)
-    for (int64_t ch = (int64_t)blockIdx.x * kScatterWarps + warp; ch < nchunks; ch += nw) {
+    const int64_t chend = min(nchunks, (int64_t)D.w1);
+    for (int64_t ch = (int64_t)D.w0 + (int64_t)blockIdx.x * kScatterWarps + warp; ch < chend; ch += nw) {
         const int64_t p0 = ch * kPChunk;
         const int nc = (int)min((int64_t)kPChunk, npieces - p0);
         {   // stage the chunk's records: coalesced 16-byte loads
@@ -1383,7 +1384,7 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     do {                                                                                                   \
         FWT_CUDA(cudaFuncSetAttribute(deposit_piece_kernel<G, A, F, R>,                                    \
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPieceSmem));      \
-        deposit_piece_kernel<G, A, F, R><<<(unsigned)ntiles, kDepThreads, kPieceSmem, c->stream>>>(       \
+        deposit_piece_kernel<G, A, F, R><<<grid, kDepThreads, kPieceSmem, c->stream>>>(                   \
             B.piece, N, ntx, nty, tz0, d_toff, d_list, scale, wx, wy, wz, d_err, rctx, L, B.ras_off, B.ras_pts); \
         FWT_CUDA(cudaGetLastError());                                                                      \
     } while (0)
@@ -1391,6 +1392,7 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     do {                                                                                                   \
         if (B.raster) FWT_PIECE_LAUNCH(G, A, F, true); else FWT_PIECE_LAUNCH(G, A, F, false);              \
     } while (0)
+        const unsigned grid = (unsigned)(std::min<int64_t>(ntiles, L.w1) - L.w0);
         const int m = kt_begin(c, KT_DEPOSIT);
         if (f64) {
             if (accumulate) FWT_PIECE_LAUNCH_R(true, true, true); else FWT_PIECE_LAUNCH_R(true, false, true);
@@ -1415,7 +1417,7 @@ int launch_piece(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     c->wmm_valid = false;
     if (herr & 2) return fail(FWT_E_TIMEOUT, "deposit: bulk copy wait ran out");
     if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
-    if (!f64) FWT_TRY(defer_finish(c, rctx, D, npairs, c->defer_per_pair, launch));
+    if (!f64) FWT_TRY(defer_finish(c, rctx, D, npairs, c->defer_per_pair, ntiles, launch));
     return 0;
 }
 
@@ -1437,11 +1439,12 @@ int launch_scatter(Ctx *c, const CenterlineBatch &B)
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev);
     const int64_t nchunks = (B.npieces + kPChunk - 1) / kPChunk;
-    const unsigned grid = (unsigned)std::min<int64_t>((int64_t)sms * 3, (nchunks + kScatterWarps - 1) / kScatterWarps);
     unsigned long long *side = (unsigned long long *)c->b_side.p;
     DeferList D{};
     FWT_TRY(defer_list(c, B.npieces, c->defer_per_piece, D));
     auto launch = [&](const DeferList &L) -> int {
+        const int64_t nch = std::min<int64_t>(nchunks, L.w1) - L.w0;
+        const unsigned grid = (unsigned)std::min<int64_t>((int64_t)sms * 3, (nch + kScatterWarps - 1) / kScatterWarps);
         const int m = kt_begin(c, KT_DEPOSIT);
         if (general) {
             FWT_CUDA(cudaFuncSetAttribute(scatter_piece_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1468,7 +1471,7 @@ int launch_scatter(Ctx *c, const CenterlineBatch &B)
     FWT_CUDA(cudaStreamSynchronize(c->stream));
     if (herr & 64) return fail(FWT_E_STATE, "scatter: a chord box beyond the candidate codes or one period");
     if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
-    return defer_finish(c, rctx, D, B.npieces, c->defer_per_piece, launch);
+    return defer_finish(c, rctx, D, B.npieces, c->defer_per_piece, nchunks, launch);
 }
 
 }  // namespace fwt

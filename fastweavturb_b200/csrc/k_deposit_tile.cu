@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
 {
     extern __shared__ __align__(16) unsigned char dsm[];
     long long(*acc)[kAccN] = reinterpret_cast<long long(*)[kAccN]>(dsm);
-    const int tile = blockIdx.x;
+    const int tile = (int)D.w0 + blockIdx.x;
     const int64_t c0 = tile_off[tile], c1 = tile_off[tile + 1];
     // a tile that no record of this batch meets keeps its values: earlier batches wrote them,
     // or the field was cleared before the first
@@ -551,15 +551,16 @@ __global__ void side_fold_kernel(float *__restrict__ w, unsigned long long *__re
 int defer_list(Ctx *c, int64_t units, double rate, DeferList &D)
 {
     // 1.5 times the last launch's rate, between 1 Mi and 16 Mi pairs (256 MB) unless a larger
-    // list is already held; an overflow is refilled at its counted size (defer_finish)
+    // list is already held; an overflow is refilled in windows of work units (defer_finish)
     const double want = std::min(std::max(1.0 * (1 << 20), 1.5 * rate * (double)units), 1.0 * (1 << 24));
-    const unsigned long long cap = (unsigned long long)want;
+    const unsigned long long cap = std::min((unsigned long long)want, defer_max(c));
     FWT_TRY(buf_reserve(c, c->b_defer, 16 + sizeof(Deferred) * (size_t)cap));
     D.count = (unsigned long long *)c->b_defer.p;
     D.e = (Deferred *)((char *)c->b_defer.p + 16);
     D.cap = (c->b_defer.bytes - 16) / sizeof(Deferred);
     D.emit_only = 0;
-    D.pad = 0;
+    D.w0 = 0;
+    D.w1 = ~0u;
     FWT_CUDA(cudaMemsetAsync(D.count, 0, sizeof(unsigned long long), c->stream));
     return 0;
 }
@@ -568,7 +569,7 @@ int defer_grow(Ctx *c, unsigned long long n, DeferList &D)
 {
     // the list's old entries are rewritten by the refill pass: a fresh buffer will do
     buf_free(c, c->b_defer);
-    FWT_TRY(buf_reserve(c, c->b_defer, 16 + sizeof(Deferred) * (size_t)(n + n / 8)));
+    FWT_TRY(buf_reserve(c, c->b_defer, 16 + sizeof(Deferred) * (size_t)n));
     D.count = (unsigned long long *)c->b_defer.p;
     D.e = (Deferred *)((char *)c->b_defer.p + 16);
     D.cap = (c->b_defer.bytes - 16) / sizeof(Deferred);
@@ -708,10 +709,11 @@ int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     do {                                                                                                  \
         FWT_CUDA(cudaFuncSetAttribute(deposit_tile_kernel<G, A, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                       (int)kDepSmem));                                                    \
-        deposit_tile_kernel<G, A, F><<<(unsigned)ntiles, kDepThreads, kDepSmem, c->stream>>>(             \
+        deposit_tile_kernel<G, A, F><<<grid, kDepThreads, kDepSmem, c->stream>>>(                         \
             B.rec, N, ntx, nty, tz0, d_toff, d_list, scale, wx, wy, wz, d_err, rctx, L);                  \
         FWT_CUDA(cudaGetLastError());                                                                     \
     } while (0)
+        const unsigned grid = (unsigned)(std::min<int64_t>(ntiles, L.w1) - L.w0);
         const int m = kt_begin(c, KT_DEPOSIT);
         if (f64) {
             // the FP64 path evaluates every pair in FP64: the General distinction is only the FP32 one
@@ -736,7 +738,7 @@ int launch_tile(Ctx *c, const CenterlineBatch &B, int64_t *pairs_out)
     c->wmm_valid = false;
     if (herr & 2) return fail(FWT_E_TIMEOUT, "deposit: bulk copy wait ran out");
     if (herr & 4) return fail(FWT_E_RANGE, "deposit: contribution outside the fixed-point range");
-    if (!f64) FWT_TRY(defer_finish(c, rctx, D, npairs, c->defer_per_pair, launch));
+    if (!f64) FWT_TRY(defer_finish(c, rctx, D, npairs, c->defer_per_pair, ntiles, launch));
     return 0;
 }
 

@@ -349,11 +349,13 @@ constexpr uint32_t kDeferDecide = 1u << 31;
 constexpr size_t kSideStride = 4;
 
 struct DeferList {
-    Deferred *e;
-    unsigned long long *count;   // pairs pushed (may exceed cap)
-    unsigned long long cap;
-    int emit_only;               // 1: the refill pass after an overflow (no field update)
-    int pad;
+    Deferred *e = nullptr;
+    unsigned long long *count = nullptr;   // pairs pushed (may exceed cap)
+    unsigned long long cap = 0;
+    int emit_only = 0;                     // 1: a refill pass after an overflow (no field update)
+    // the refill pass's window of work units [w0, w1) (tiles, or chunks of pieces); the
+    // first pass covers every unit
+    uint32_t w0 = 0, w1 = ~0u;
 };
 
 // Append the lanes' flagged pairs (warp-uniform call).
@@ -383,32 +385,74 @@ int side_ensure(Ctx *c);
 
 // Evaluate the first n pairs of the list in FP64 into the side accumulator (k_deposit_tile.cu).
 int defer_apply(Ctx *c, const RedoCtx &R, const DeferList &D, unsigned long long n);
-// Make the list hold n pairs (n > its capacity) and reset its count.
+// Replace the list by one of n entries (its old entries are not kept) and reset its count.
 int defer_grow(Ctx *c, unsigned long long n, DeferList &D);
 void defer_rate(double &rate, unsigned long long n, int64_t units);
-
-// After a tile launch: read the list's count; if it overflowed, make room for the counted pairs
-// and refill the list through rescan(D) (the same launch in emit-only mode); then evaluate every
-// deferred pair in FP64 into the side accumulator.
-template <typename F>
-int defer_finish(Ctx *c, const RedoCtx &R, DeferList &D, int64_t units, double &rate, F &&rescan)
+// Entries of the largest list an overflow grows to (1 GiB, or the context's tuning): a launch
+// that defers more pairs refills its list in windows of work units.
+constexpr unsigned long long kDeferMaxEntries = 1ull << 26;
+inline unsigned long long defer_max(const Ctx *c)
 {
+    return c->defer_max_pairs >= 1.0 ? (unsigned long long)c->defer_max_pairs : kDeferMaxEntries;
+}
+
+// After a launch over `units` work units (the rate's denominator) of which `wunits` can be
+// windowed (tiles, or chunks of pieces): read the list's count and, when nothing overflowed,
+// evaluate every deferred pair in FP64 into the side accumulator.  After an overflow the list
+// is grown (up to kDeferMaxEntries) and refilled by rescan(D), the same launch in emit-only
+// mode over a window of units at a time; each window's pairs are evaluated before the next is
+// listed.  A unit's pairs are listed in the same order-independent way by every pass, so the
+// windows together hold each counted pair once.
+template <typename F>
+int defer_finish(Ctx *c, const RedoCtx &R, DeferList &D, int64_t units, double &rate, int64_t wunits, F &&rescan)
+{
+    auto read_count = [&](unsigned long long &n) -> int {
+        FWT_CUDA(cudaMemcpyAsync(&n, D.count, sizeof(n), cudaMemcpyDeviceToHost, c->stream));
+        FWT_CUDA(cudaStreamSynchronize(c->stream));
+        return 0;
+    };
     unsigned long long n = 0;
-    FWT_CUDA(cudaMemcpyAsync(&n, D.count, sizeof(n), cudaMemcpyDeviceToHost, c->stream));
-    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    FWT_TRY(read_count(n));
     defer_rate(rate, n, units);
     if (n == 0) return 0;
-    if (n > D.cap) {
-        FWT_TRY(defer_grow(c, n, D));
-        D.emit_only = 1;
-        FWT_TRY(rescan(D));
-        D.emit_only = 0;
-        unsigned long long n2 = 0;
-        FWT_CUDA(cudaMemcpyAsync(&n2, D.count, sizeof(n2), cudaMemcpyDeviceToHost, c->stream));
-        FWT_CUDA(cudaStreamSynchronize(c->stream));
-        if (n2 != n) return fail(FWT_E_STATE, "deferred pairs: the refill pass counted a different number");
+    if (n <= D.cap) return defer_apply(c, R, D, n);
+    const unsigned long long want = std::min(n + n / 8, defer_max(c));
+    if (want > D.cap) FWT_TRY(defer_grow(c, want, D));
+    D.emit_only = 1;
+    unsigned long long done = 0;
+    int64_t u = 0;
+    // window width in units, from the mean count per unit, for a list three quarters full
+    double width = std::max(1.0, (double)wunits * 0.75 * (double)D.cap / (double)n);
+    int rc = 0;
+    while (u < wunits && rc == 0) {
+        const int64_t w1 = std::min<int64_t>(wunits, u + (int64_t)width);
+        D.w0 = (uint32_t)u;
+        D.w1 = (uint32_t)w1;
+        FWT_CUDA(cudaMemsetAsync(D.count, 0, sizeof(unsigned long long), c->stream));
+        if ((rc = rescan(D)) != 0) break;
+        unsigned long long m = 0;
+        if ((rc = read_count(m)) != 0) break;
+        if (m > D.cap) {
+            if (w1 - u > 1) {   // narrower window: the counted pairs scaled to half the list
+                width = std::max(1.0, (double)(w1 - u) * 0.5 * (double)D.cap / (double)m);
+                continue;
+            }
+            // one unit holds more pairs than the list: make room for them and list it again
+            if ((rc = defer_grow(c, m + m / 8, D)) != 0) break;
+            continue;
+        }
+        if ((rc = defer_apply(c, R, D, m)) != 0) break;
+        done += m;
+        const double scaled = (double)(w1 - u) * 0.75 * (double)D.cap / (double)std::max(m, 1ull);
+        width = std::max(1.0, std::min(2.0 * (double)(w1 - u), scaled));
+        u = w1;
     }
-    return defer_apply(c, R, D, n);
+    D.emit_only = 0;
+    D.w0 = 0;
+    D.w1 = ~0u;
+    if (rc) return rc;
+    if (done != n) return fail(FWT_E_STATE, "deferred pairs: the refill passes counted a different number");
+    return 0;
 }
 
 // Shared kernels of the binning (defined in k_deposit_tile.cu).

@@ -246,6 +246,11 @@ int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
  * on the order); thicker piece lines go through the tiles.  0 switches it off, value < 0
  * restores the default, 5.  The field is the same either way to FP32 rounding. */
 #define FWT_TUNE_SCATTER_RT_CELLS 3
+/* FWT_TUNE_DEFER_MAX_PAIRS: the most entries (16 bytes each) the list of pairs an FP32 launch
+ * hands to FP64 grows to after an overflow; a launch that hands over more lists and evaluates
+ * them in windows of tiles (or of pieces) that fit.  value < 1 restores the default, 2^26
+ * (1 GiB).  The field is the same, bit for bit, whatever the limit. */
+#define FWT_TUNE_DEFER_MAX_PAIRS 4
 int fwt_set_tuning(fwt_ctx *ctx, int key, double value);
 
 /* Message of the last error on this thread. */

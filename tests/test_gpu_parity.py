@@ -232,3 +232,32 @@ def test_scatter_equals_tile_pieces(fwt, orc, sigma_ratio):
     vor, _ = orc.deposit(p, cl)
     assert rel_l2(fields[8.0], vor) <= TOL32
     assert rel_l2(fields[0.0], vor) <= TOL32
+
+
+@pytest.mark.parametrize("path", ["subsegment", "piece", "scatter"])
+def test_deferred_list_windows_are_exact(fwt, orc, path):
+    """The list of pairs handed from FP32 to FP64 limited to 16 entries: every launch overflows
+    it and lists its deferred pairs again in windows of tiles (or chunks of pieces), evaluating
+    one window at a time.  The FP64 contributions are int64 sums, so the field equals the one
+    built with the default list bit for bit, through each of the three deposition kernels."""
+    from fastweavturb_b200.configs import small
+    w = small(N=64, seed=11, nlev=2, tubes0=3, nodes0=128, sigma0=0.03)
+    w.sigma_ratio = 4.0
+    p, cl = oracle_inputs(orc, w)
+    piece, scatter = {"subsegment": (0.0, 0.0), "piece": (64.0, 0.0), "scatter": (64.0, 64.0)}[path]
+    fields, counts = {}, {}
+    for limit in (0, 16):
+        ctx = fwt.Context(gpu_params(fwt, w, precision=32, deposit_mode=0))
+        ctx.set_piece_radius_limit(piece)
+        ctx.set_scatter_radius_limit(scatter)
+        ctx.set_defer_limit(limit)
+        ctx.set_centerlines(cl.npoint, cl.xyz, p.sigma, p.Gamma, p.n_T)
+        ctx.deposit(1, w.ntubes)
+        fields[limit] = ctx.field(0).copy()
+        counts[limit] = ctx.counters()
+        ctx.close()
+    assert counts[16]["redone_fp64"] > 64
+    assert counts[0] == counts[16]
+    assert np.array_equal(fields[0], fields[16])
+    vor, _ = orc.deposit(p, cl)
+    assert rel_l2(fields[16], vor) <= TOL32
