@@ -121,15 +121,16 @@ __global__ void line_prep_kernel(const LineParam *__restrict__ lp, int nlines, c
 
 
 // ------------------------------------------------------------------ a3/a5: sections
-// |c' x c''| / |c'|^2 of the quintic cf ([coord][6], FP32) at z (tube.f90:633-647)
-__device__ __forceinline__ float turning_integrand(const float *cf, float z)
+// |c' x c''| / |c'|^2 at z of the quintic whose derivative coefficients are d1 ([coord][5]:
+// a1, 2 a2, 3 a3, 4 a4, 5 a5) and d2 ([coord][4]: 2 a2, 6 a3, 12 a4, 20 a5), FP32
+// (tube.f90:633-647), added to th
+__device__ __forceinline__ void turning_integrand(const float (&d1)[3][5], const float (&d2)[3][4], float z, float &th)
 {
     float dc[3], dd[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        const float *a = cf + 6 * d;
-        dc[d] = fmaf(fmaf(fmaf(fmaf(5.0f * a[5], z, 4.0f * a[4]), z, 3.0f * a[3]), z, 2.0f * a[2]), z, a[1]);
-        dd[d] = fmaf(fmaf(fmaf(20.0f * a[5], z, 12.0f * a[4]), z, 6.0f * a[3]), z, 2.0f * a[2]);
+        dc[d] = fmaf(fmaf(fmaf(fmaf(d1[d][4], z, d1[d][3]), z, d1[d][2]), z, d1[d][1]), z, d1[d][0]);
+        dd[d] = fmaf(fmaf(fmaf(d2[d][3], z, d2[d][2]), z, d2[d][1]), z, d2[d][0]);
     }
     const float x0 = dc[1] * dd[2] - dc[2] * dd[1];
     const float x1 = dc[2] * dd[0] - dc[0] * dd[2];
@@ -137,9 +138,10 @@ __device__ __forceinline__ float turning_integrand(const float *cf, float z)
     const float ndc2 = dc[0] * dc[0] + dc[1] * dc[1] + dc[2] * dc[2];
     // hardware square root and reciprocal (a few ulp): the sum only has to land within 1e-4 of
     // the reference's, and sections closer than that to a step of ceil() are redone in FP64
-    float nx;
+    float nx, rn;
     asm("sqrt.approx.f32 %0, %1;" : "=f"(nx) : "f"(x0 * x0 + x1 * x1 + x2 * x2));
-    return __fdividef(nx, ndc2);
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rn) : "f"(ndc2));
+    th = fmaf(nx, rn, th);
 }
 
 // Sections in three passes (n_sec + 1 slots per line; slot n_sec is the periodic copy): the
@@ -203,22 +205,28 @@ __global__ void section_kernel(int64_t nslots, int ntf_pre, const double *__rest
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= nslots) return;
-    // lane m < 18 loads coefficient m; every lane takes the FP32 copies by shuffles
+    // lane m < 18 loads coefficient m; every lane takes the FP32 derivative coefficients by
+    // shuffles, scaled once (1, 2, 3, 4, 5 for c' and 2, 6, 12, 20 for c'')
     const float mine = lane < 18 ? (float)coe[18 * warp + lane] : 0.0f;
-    float cf[18];
+    float d1[3][5], d2[3][4];
 #pragma unroll
-    for (int m = 0; m < 18; ++m) cf[m] = __shfl_sync(0xffffffffu, mine, m);
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+        for (int m = 1; m <= 5; ++m) d1[d][m - 1] = (float)m * __shfl_sync(0xffffffffu, mine, 6 * d + m);
+#pragma unroll
+        for (int m = 2; m <= 5; ++m) d2[d][m - 2] = (float)(m * (m - 1)) * __shfl_sync(0xffffffffu, mine, 6 * d + m);
+    }
     const float zstep = zstep_in[warp], z64 = 64.0f * zstep;
     float th0 = 0.0f, th1 = 0.0f;
     int tj = lane;
     float za = zstep * (float)lane, zb = zstep * (float)(lane + 32);
     for (; tj + 32 <= ntf_pre; tj += 64) {   // two independent samples per step
-        th0 += turning_integrand(cf, za);
-        th1 += turning_integrand(cf, zb);
+        turning_integrand(d1, d2, za, th0);
+        turning_integrand(d1, d2, zb, th1);
         za += z64;
         zb += z64;
     }
-    if (tj <= ntf_pre) th0 += turning_integrand(cf, za);
+    if (tj <= ntf_pre) turning_integrand(d1, d2, za, th0);
     const double sum = warp_sum((double)th0 + (double)th1);
     if (lane == 0) tsum_out[warp] = sum;
 }

@@ -124,9 +124,12 @@ int launch_walk(Ctx *c, const CenterlineBatch &B, unsigned long long *d_acc)
 
 static int64_t batch_node_cap(const Ctx *c)
 {
-    // sub-segment records are ~200 B and there are ~10-50 per node: keep a batch's
-    // set-up arrays within a few GB
-    return (int64_t)1 << 22;
+    // sub-segment records are ~200 B, with samples and tile lists ~300 B, and there are ~10-50
+    // per node: keep a batch's set-up arrays within a few GB, and under a memory cap within
+    // about half of it (24 KB per node)
+    int64_t cap = (int64_t)1 << 22;
+    if (c->p.mem_cap) cap = std::min(cap, std::max<int64_t>((int64_t)1 << 15, (int64_t)(c->p.mem_cap / 24576)));
+    return cap;
 }
 
 int deposit_lines(Ctx *c, int line_s, int line_e)

@@ -393,7 +393,10 @@ void defer_rate(double &rate, unsigned long long n, int64_t units);
 constexpr unsigned long long kDeferMaxEntries = 1ull << 26;
 inline unsigned long long defer_max(const Ctx *c)
 {
-    return c->defer_max_pairs >= 1.0 ? (unsigned long long)c->defer_max_pairs : kDeferMaxEntries;
+    if (c->defer_max_pairs >= 1.0) return (unsigned long long)c->defer_max_pairs;
+    // under a memory cap: a sixteenth of it
+    if (c->p.mem_cap) return std::max(1ull << 16, std::min(kDeferMaxEntries, (unsigned long long)(c->p.mem_cap / 256)));
+    return kDeferMaxEntries;
 }
 
 // After a launch over `units` work units (the rate's denominator) of which `wunits` can be

@@ -6,8 +6,9 @@ size, each with its own CUDA stream, so the FFT plans and device buffers of a si
 once and reused by every realisation of that size, and up to `workers` realisations are in
 flight at once (one host thread each; the library releases the interpreter during its calls):
 small fields, whose kernels fill a fraction of the GPU and whose phases end in short host
-synchronisations, overlap on the device.  Each realisation's centerlines are generated on the
-device, the field is built and its statistics stay on the device until read.
+synchronisations, overlap on the device.  The contexts share the device memory: each is capped
+at its share (plan), which sizes its batches of lines.  Each realisation's centerlines are
+generated on the device, the field is built and its statistics stay on the device until read.
 
 Autotuner: before the first realisation of a grid size, the deposition of a probe
 realisation is timed over the deposition kernels' selection limits, one after the other: the
@@ -41,11 +42,12 @@ RASTER_CANDIDATES = (0.0, 1.5, 2.5, 4.0)        # rasterised pieces radius limit
 
 
 class Ensemble:
-    def __init__(self, device=0, tune=True, Sp_order=6, workers=4):
+    def __init__(self, device=0, tune=True, Sp_order=6, workers=4, mem_cap=None):
         self.device = device
         self.tune = tune
         self.Sp_order = Sp_order
         self.workers = max(1, int(workers))
+        self.mem_cap = mem_cap     # device bytes per context, or per grid size (plan() sets them)
         self.ctx = {}
         self.tuned = {}
         self.tune_log = {}
@@ -58,7 +60,7 @@ class Ensemble:
             if key not in self.ctx:
                 self.ctx[key] = Context(Params(N=N, N_downsample=N, line_s=1, line_e=0, sigma_ratio=1.0,
                                                device=self.device, pdf_bins=201, Sp_order=self.Sp_order,
-                                               vorticity_output=0))
+                                               vorticity_output=0, mem_cap=self._cap(N)))
                 if N in self.tuned:
                     self._apply(self.ctx[key], self.tuned[N])
             return self.ctx[key]
@@ -117,15 +119,42 @@ class Ensemble:
 
     def slots_for(self, N):
         """Contexts kept for grid size N: every worker for small fields, fewer for large ones,
-        whose per-context buffers (records of up to 4 Mi nodes per batch, three N^3 fields)
-        run to gigabytes."""
-        cap = self.workers if N <= 96 else (4 if N <= 128 else 2)
+        which fill the GPU by themselves and whose buffers (tile lists, records, three N^3
+        fields) run to gigabytes."""
+        cap = self.workers if N <= 96 else (2 if N <= 128 else 1)
         return max(1, min(self.workers, cap))
+
+    def plan(self, members, total=None):
+        """Share the GPU's memory between the contexts the members will use: 80 % of the device
+        memory, 2 GB per context and the rest in proportion to N^3 (a context's fields, and
+        the tile lists of its thick tubes, grow with N^3).  Each context's share is its cap
+        (Params.mem_cap), which also bounds its batches of lines and its list of pairs handed to
+        FP64.  Without it every context would size its batch buffers for 4 Mi nodes (gigabytes
+        each) and sixteen contexts of five grid sizes would not fit.  Runs once, before the
+        first context is made; returns the caps by grid size."""
+        if self.mem_cap is not None:
+            return self.mem_cap
+        import torch
+        sizes = sorted({w.N for w in members} | {n for (n, _) in self.ctx})
+        slots = {N: self.slots_for(N) for N in sizes}
+        if total is None:
+            total = torch.cuda.mem_get_info(self.device)[1]
+        base = 2.0e9
+        spare = max(0.0, 0.8 * total - base * sum(slots.values()))
+        vol = sum(slots[N] * N ** 3 for N in sizes)
+        self.mem_cap = {N: int(base + spare * N ** 3 / vol) for N in sizes}
+        return self.mem_cap
+
+    def _cap(self, N):
+        if isinstance(self.mem_cap, dict):
+            return self.mem_cap.get(N, 0)
+        return int(self.mem_cap or 0)
 
     def run(self, members, stats=True):
         """Build every member, up to `workers` at once; returns (per-member statistics in
         member order, wall seconds of the build, Mpts/s = sum N^3 / wall)."""
         import torch
+        self.plan(members)
         for w in members:
             if self.tune and w.N not in self.tuned:
                 self.autotune(w)
@@ -198,6 +227,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
     members = cfg3_members(args.members)
     ens = Ensemble(workers=args.workers, tune=True)
+    ens.plan(members)
     ens.run(members[:min(4, len(members))], stats=False)     # warm: plans, buffers, autotuning
     _, t_conc, rate = ens.run(members, stats=False)
     # the same members one at a time (the sum of the single-field times)

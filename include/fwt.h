@@ -54,7 +54,9 @@ typedef struct {
     int Sp_order;       /* tube.f90:58 (default 10) */
     int pdf_bins;       /* tube.f90:129 bin_num (default 1000) */
     int vorticity_output; /* tube.f90:55 (default 1) */
-    size_t mem_cap;     /* bytes of device memory the context may hold (0 = no cap) */
+    size_t mem_cap;     /* bytes of device memory the context may hold (0 = no cap); a cap also
+                           bounds the lines' batches (mem_cap / 24576 nodes) and the list of
+                           pairs handed to FP64 (mem_cap / 256 entries) */
 } fwt_params;
 
 /* Fill *p with the reference defaults (the values of FBB_with_parameters.m:205-225 and
@@ -249,7 +251,8 @@ int fwt_counters(fwt_ctx *ctx, int64_t *c, int n);
 /* FWT_TUNE_DEFER_MAX_PAIRS: the most entries (16 bytes each) the list of pairs an FP32 launch
  * hands to FP64 grows to after an overflow; a launch that hands over more lists and evaluates
  * them in windows of tiles (or of pieces) that fit.  value < 1 restores the default, 2^26
- * (1 GiB).  The field is the same, bit for bit, whatever the limit. */
+ * (1 GiB), or mem_cap / 256 under a memory cap.  The field is the same, bit for bit, whatever
+ * the limit. */
 #define FWT_TUNE_DEFER_MAX_PAIRS 4
 int fwt_set_tuning(fwt_ctx *ctx, int key, double value);
 

@@ -38,9 +38,24 @@ def test_a_density_change_only_touches_the_end_of_a_level():
 def test_ensemble_context_caps_per_grid_size():
     ens = Ensemble(workers=8, tune=False)
     assert ens.slots_for(64) == 8 and ens.slots_for(96) == 8
-    assert ens.slots_for(128) == 4 and ens.slots_for(256) == 2
+    assert ens.slots_for(128) == 2 and ens.slots_for(256) == 1
     assert Ensemble(workers=1).slots_for(256) == 1
     assert ens.ctx == {}            # nothing is created before a run
+
+
+def test_ensemble_memory_plan_shares_the_device_by_volume():
+    from fastweavturb_b200.ensemble import cfg3_members
+    members = cfg3_members(64)
+    ens = Ensemble(workers=4, tune=False)
+    caps = ens.plan(members, total=180e9)
+    sizes = sorted({w.N for w in members})
+    assert sorted(caps) == sizes
+    # the contexts' caps fill 80 % of the device and grow with the grid size
+    used = sum(ens.slots_for(N) * caps[N] for N in sizes)
+    assert 0.79 * 180e9 <= used <= 0.8 * 180e9
+    assert all(caps[a] < caps[b] for a, b in zip(sizes, sizes[1:]))
+    assert caps[sizes[0]] >= 2e9 and ens._cap(sizes[-1]) == caps[sizes[-1]]
+    assert ens.plan(members, total=1.0) is caps     # planned once
 
 
 def test_draw_params_stay_in_the_box():
