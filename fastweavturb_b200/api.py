@@ -286,9 +286,16 @@ class Context:
         _check(library().fwt_sp(self._h, pmax, _ptr(r, ctypes.c_int), len(r), _ptr(out, ctypes.c_double)))
         return r, out.reshape(pmax, len(r))
 
-    def output_v(self):
+    def output_v(self, out=None):
+        """Downsampled |omega| and helicity of the normalised fields: (2, nd, nd, nd) [k, j, i]
+        (field_wh.dat).  `out`: a C-contiguous float32 array of 2 nd^3 elements to write into
+        (pinned host memory, e.g. a pinned torch tensor's numpy view, copies at the link's full
+        rate; a fresh numpy array goes through the driver's pageable staging)."""
         nd = self.params.N_downsample
-        out = np.zeros(2 * nd ** 3, dtype=np.float32)
+        if out is None:
+            out = np.zeros(2 * nd ** 3, dtype=np.float32)
+        elif out.dtype != np.float32 or out.size != 2 * nd ** 3 or not out.flags.c_contiguous:
+            raise ValueError("out: a C-contiguous float32 array of 2 * N_downsample^3 elements")
         _check(library().fwt_field_wh(self._h, _ptr(out, ctypes.c_float)))
         return out.reshape(2, nd, nd, nd)
 
