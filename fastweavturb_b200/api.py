@@ -54,7 +54,8 @@ class _Params(ctypes.Structure):
 
 EXPORTS = [
     "fwt_default_params", "fwt_create", "fwt_destroy", "fwt_load_inputs", "fwt_check_inputs", "fwt_set_centerlines",
-    "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart", "fwt_normalize", "fwt_spectrum",
+    "fwt_set_centerlines_async", "fwt_set_centerlines_device", "fwt_deposit", "fwt_filter", "fwt_biot_savart",
+    "fwt_normalize", "fwt_spectrum",
     "fwt_pdf", "fwt_pdf_noalloc", "fwt_sp", "fwt_sp_exponents", "fwt_field_wh", "fwt_field_uw", "fwt_field_wd",
     "fwt_set_outputs", "fwt_copy_field", "fwt_field_device", "fwt_vsf_deviation", "fwt_helicity",
     "fwt_isosurface", "fwt_set_slab", "fwt_biot_savart_block", "fwt_sp_block",
@@ -84,6 +85,8 @@ def library(path: str | None = None):
         "fwt_load_inputs": [vp, ctypes.c_char_p, ctypes.c_char_p],
         "fwt_check_inputs": [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(_Params), ctypes.POINTER(ip), i64p],
         "fwt_set_centerlines": [vp, ip, i64p, dp, dp, dp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
+        "fwt_set_centerlines_async": [vp, ip, i64p, dp, dp, dp, ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int)],
         "fwt_set_centerlines_device": [vp, ip, i64p, vp, vp, vp, dp, dp, ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int)],
         "fwt_deposit": [vp, ip, ip],
@@ -226,7 +229,10 @@ class Context:
     def load_inputs(self, centerline_path, params_path):
         _check(library().fwt_load_inputs(self._h, str(centerline_path).encode(), str(params_path).encode()))
 
-    def set_centerlines(self, npoint, xyz, sigma, Gamma, n_T, if_filter=None):
+    def set_centerlines(self, npoint, xyz, sigma, Gamma, n_T, if_filter=None, async_upload=False):
+        """Host centerlines: npoint per line, xyz (npointall, 3) FP64.  async_upload: the copy
+        runs behind the deposition (fwt_set_centerlines_async); the context keeps xyz alive
+        until the next deposition returns, and xyz must not change before then."""
         npoint = np.ascontiguousarray(npoint, dtype=np.int64)
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
         nl = len(npoint)
@@ -234,9 +240,10 @@ class Context:
         Gamma = np.ascontiguousarray(Gamma, dtype=np.float64)
         n_T = np.ascontiguousarray(n_T, dtype=np.int32)
         filt = np.ascontiguousarray(np.zeros(nl) if if_filter is None else if_filter, dtype=np.int32)
-        _check(library().fwt_set_centerlines(self._h, nl, _ptr(npoint, ctypes.c_int64), _ptr(xyz, ctypes.c_double),
-                                             _ptr(sigma, ctypes.c_double), _ptr(Gamma, ctypes.c_double),
-                                             _ptr(n_T, ctypes.c_int), _ptr(filt, ctypes.c_int)))
+        f = library().fwt_set_centerlines_async if async_upload else library().fwt_set_centerlines
+        self._upload = xyz if async_upload else None
+        _check(f(self._h, nl, _ptr(npoint, ctypes.c_int64), _ptr(xyz, ctypes.c_double), _ptr(sigma, ctypes.c_double),
+                 _ptr(Gamma, ctypes.c_double), _ptr(n_T, ctypes.c_int), _ptr(filt, ctypes.c_int)))
 
     def set_centerlines_device(self, npoint, dx, dy, dz, sigma, Gamma, n_T, if_filter=None):
         """dx, dy, dz: device pointers (int) to FP64 node coordinates on this context's GPU."""

@@ -169,6 +169,27 @@ struct PhaseTimer {
     }
 };
 
+int finish_upload(Ctx *c)
+{
+    if (!c->up_stream) return 0;
+    const cudaError_t e = cudaStreamSynchronize(c->up_stream);
+    for (auto &pe : c->up_events) cudaEventDestroy(pe.second);
+    c->up_events.clear();
+    if (e != cudaSuccess) return fail(FWT_E_CUDA, std::string("node upload: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+int wait_nodes(Ctx *c, int64_t upto)
+{
+    for (const auto &pe : c->up_events) {
+        if (pe.first >= upto) {
+            FWT_CUDA(cudaStreamWaitEvent(c->stream, pe.second, 0));
+            return 0;
+        }
+    }
+    return 0;
+}
+
 }  // namespace fwt
 
 using namespace fwt;
@@ -248,6 +269,8 @@ int fwt_destroy(fwt_ctx *h)
     if (!c) return 0;
     cudaSetDevice(c->dev);
     cudaStreamSynchronize(c->stream);
+    finish_upload(c);
+    if (c->up_stream) cudaStreamDestroy(c->up_stream);
     if (c->plans) {
         cufftDestroy(c->plan_r2c);
         cufftDestroy(c->plan_c2r);
@@ -292,35 +315,65 @@ static int set_lines_common(Ctx *c, int nline, const int64_t *npoint, const doub
     return 0;
 }
 
-int fwt_set_centerlines(fwt_ctx *h, int nline, const int64_t *npoint, const double *xyz, const double *sigma,
-                        const double *Gamma, const int *n_T, const int *if_filter)
+// The caller's row-major array in chunks of up to 32 Mi nodes (fast when it is pinned) through
+// a staging buffer (scratch[27]), each chunk made SoA on the device.  Synchronous: on the
+// context's stream, waited for.  Asynchronous: on the upload stream, one event per chunk, which
+// wait_nodes makes the context's stream wait for batch by batch.
+static int set_centerlines_host(Ctx *c, int nline, const int64_t *npoint, const double *xyz, const double *sigma,
+                                const double *Gamma, const int *n_T, const int *if_filter, bool async)
 {
-    Ctx *c = (Ctx *)h;
     if (!c || !xyz) return fail(FWT_E_ARG, "null argument");
     cudaSetDevice(c->dev);
+    FWT_TRY(finish_upload(c));   // an earlier upload still reads the staging buffer
     FWT_TRY(set_lines_common(c, nline, npoint, sigma, Gamma, n_T, if_filter));
     const int64_t n = c->node_off[nline];
-    // the caller's row-major array in chunks of up to 32 Mi nodes (fast when it is pinned)
-    // through a staging buffer (scratch[27]), each chunk made SoA on the device
     FWT_TRY(buf_reserve(c, c->b_nodes, sizeof(double) * 3 * (size_t)n));
     double *d = (double *)c->b_nodes.p;
     const int64_t chunk = std::min<int64_t>(n, (int64_t)1 << 25);
     FWT_TRY(buf_reserve(c, c->scratch[27], sizeof(double) * 3 * (size_t)std::max<int64_t>(chunk, 1)));
     double *stage = (double *)c->scratch[27].p;
+    cudaStream_t st = c->stream;
+    if (async) {
+        if (!c->up_stream) FWT_CUDA(cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking));
+        // the buffers may still be read by the context's earlier work
+        cudaEvent_t ready;
+        FWT_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+        FWT_CUDA(cudaEventRecord(ready, c->stream));
+        FWT_CUDA(cudaStreamWaitEvent(c->up_stream, ready, 0));
+        cudaEventDestroy(ready);
+        st = c->up_stream;
+    }
     for (int64_t o = 0; o < n; o += chunk) {
         const int64_t m = std::min(chunk, n - o);
-        FWT_CUDA(cudaMemcpyAsync(stage, xyz + 3 * o, sizeof(double) * 3 * (size_t)m, cudaMemcpyHostToDevice,
-                                 c->stream));
-        deinterleave_kernel<<<(unsigned)std::min<int64_t>((m + 255) / 256, 148 * 16), 256, 0, c->stream>>>(
-            stage, m, n, d + o);
+        FWT_CUDA(cudaMemcpyAsync(stage, xyz + 3 * o, sizeof(double) * 3 * (size_t)m, cudaMemcpyHostToDevice, st));
+        deinterleave_kernel<<<(unsigned)std::min<int64_t>((m + 255) / 256, 148 * 16), 256, 0, st>>>(stage, m, n,
+                                                                                                    d + o);
         c->launches += 1;
         FWT_CUDA(cudaGetLastError());
+        if (async) {
+            cudaEvent_t ev;
+            FWT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            FWT_CUDA(cudaEventRecord(ev, st));
+            c->up_events.emplace_back(o + m, ev);
+        }
     }
-    FWT_CUDA(cudaStreamSynchronize(c->stream));
+    if (!async) FWT_CUDA(cudaStreamSynchronize(c->stream));
     c->d_x = d;
     c->d_y = d + n;
     c->d_z = d + 2 * n;
     return 0;
+}
+
+int fwt_set_centerlines(fwt_ctx *h, int nline, const int64_t *npoint, const double *xyz, const double *sigma,
+                        const double *Gamma, const int *n_T, const int *if_filter)
+{
+    return set_centerlines_host((Ctx *)h, nline, npoint, xyz, sigma, Gamma, n_T, if_filter, false);
+}
+
+int fwt_set_centerlines_async(fwt_ctx *h, int nline, const int64_t *npoint, const double *xyz, const double *sigma,
+                              const double *Gamma, const int *n_T, const int *if_filter)
+{
+    return set_centerlines_host((Ctx *)h, nline, npoint, xyz, sigma, Gamma, n_T, if_filter, true);
 }
 
 int fwt_set_centerlines_device(fwt_ctx *h, int nline, const int64_t *npoint, const double *d_x, const double *d_y,
@@ -330,6 +383,7 @@ int fwt_set_centerlines_device(fwt_ctx *h, int nline, const int64_t *npoint, con
     Ctx *c = (Ctx *)h;
     if (!c || !d_x || !d_y || !d_z) return fail(FWT_E_ARG, "null argument");
     cudaSetDevice(c->dev);
+    FWT_TRY(finish_upload(c));
     FWT_TRY(set_lines_common(c, nline, npoint, sigma, Gamma, n_T, if_filter));
     c->d_x = d_x;
     c->d_y = d_y;

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/fwt.h"
@@ -79,6 +80,10 @@ struct Ctx {
     double raster_rt_cells = -1.0;  // tuning: radius limit of rasterised pieces in grid spacings (< 0: default)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // asynchronous node upload (fwt_set_centerlines_async): its stream, and per chunk the node
+    // count uploaded so far with the event that completes it
+    cudaStream_t up_stream = nullptr;
+    std::vector<std::pair<int64_t, cudaEvent_t>> up_events;
 
     // inputs (host)
     int nline = 0;
@@ -182,6 +187,11 @@ int stats_sp(Ctx *c, int pmax, const int *r, int nr, double *Sp);
 int stats_sp_block(Ctx *c, const void *u, int n0, int n1, int n2, int axis, double s, const int *r, int nr,
                    double *sums);
 int stats_field_wh(Ctx *c, float *host_out);
+// Make the context's stream wait until nodes [0, upto) of an asynchronous upload are on the
+// device (fwt_api.cu); nothing to do after a synchronous one.
+int wait_nodes(Ctx *c, int64_t upto);
+// Finish an asynchronous upload (before the nodes' buffers or the caller's array are reused).
+int finish_upload(Ctx *c);
 int stats_field_uw(Ctx *c, float *host_out);
 int stats_field_wd(Ctx *c, float *host_out);
 int stats_copy_field(Ctx *c, int which, int comp, double *host);

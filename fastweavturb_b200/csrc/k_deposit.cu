@@ -207,6 +207,8 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
             !tile_path ? BatchRecords::Walk : (thin(la) ? BatchRecords::Pieces : BatchRecords::SubSeg);
         if (std::getenv("FWT_SYNC_CHECK"))
             std::fprintf(stderr, "libfwt: batch lines %d..%d records %d\n", la + 1, lb, (int)mode);
+        // the batch's nodes, when an asynchronous upload is still bringing them
+        FWT_TRY(wait_nodes(c, c->node_off[lb]));
         CenterlineBatch B;
         B.raster = mode == BatchRecords::Pieces && rasterised(la);
         B.scatter = mode == BatchRecords::Pieces && scattered(la);
@@ -259,7 +261,8 @@ int deposit_lines(Ctx *c, int line_s, int line_e)
     FWT_CUDA(cudaStreamSynchronize(c->stream));
     c->counters[5] = (int64_t)(tile_path ? tally[1] : tally[0]);
     c->counters[6] = (int64_t)tally[2];
-    return 0;
+    // an asynchronous upload is complete once this call returns (its caller's array is free)
+    return finish_upload(c);
 }
 
 }  // namespace fwt

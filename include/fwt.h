@@ -87,6 +87,14 @@ int fwt_check_inputs(const char *centerline_path, const char *params_path, fwt_p
 int fwt_set_centerlines(fwt_ctx *ctx, int nline, const int64_t *npoint, const double *xyz,
                         const double *sigma, const double *Gamma, const int *n_T,
                         const int *if_filter);
+/* Same, with the copy asynchronous: the call returns once the upload is queued, and the
+ * deposition of each batch of lines waits only for that batch's nodes, so the transfer
+ * overlaps the work on the lines before them.  xyz must stay valid and unchanged until the
+ * next fwt_deposit / fwt_run returns (or fwt_destroy); pinned host memory copies at the link's
+ * full rate.  Results are those of fwt_set_centerlines. */
+int fwt_set_centerlines_async(fwt_ctx *ctx, int nline, const int64_t *npoint, const double *xyz,
+                              const double *sigma, const double *Gamma, const int *n_T,
+                              const int *if_filter);
 /* Same, with the node coordinates already on this context's device (x, y, z: npointall
  * doubles each).  The device arrays must stay valid until fwt_deposit returns. */
 int fwt_set_centerlines_device(fwt_ctx *ctx, int nline, const int64_t *npoint, const double *d_x,

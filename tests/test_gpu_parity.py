@@ -261,3 +261,30 @@ def test_deferred_list_windows_are_exact(fwt, orc, path):
     assert np.array_equal(fields[0], fields[16])
     vor, _ = orc.deposit(p, cl)
     assert rel_l2(fields[16], vor) <= TOL32
+
+
+def test_async_node_upload_equals_synchronous(fwt, orc):
+    """fwt_set_centerlines_async: the nodes' upload runs on its own stream and each batch of
+    lines waits for its own nodes.  With a memory cap that splits the 74 K nodes into three
+    batches, the field and the counters equal those of the synchronous upload bit for bit, and
+    a second deposition after an asynchronous upload into the same context does too."""
+    from fastweavturb_b200.configs import small
+    w = small(N=64, seed=7, nlev=3, tubes0=4, nodes0=256, sigma0=0.2)
+    p, cl = oracle_inputs(orc, w)
+    assert cl.xyz.size // 3 > 2 * 32768
+    out = {}
+    for mode in ("sync", "async", "async-again"):
+        if mode != "async-again":
+            ctx = fwt.Context(gpu_params(fwt, w, precision=32, deposit_mode=0, mem_cap=512 << 20))
+        ctx.set_centerlines(cl.npoint, cl.xyz.copy(), p.sigma, p.Gamma, p.n_T, async_upload=(mode != "sync"))
+        ctx.deposit(1, w.ntubes)
+        cnt = ctx.counters()
+        cnt.pop("launches")   # the context's running launch count
+        out[mode] = (ctx.field(0).copy(), cnt)
+        if mode == "sync":
+            ctx.close()
+    ctx.close()
+    for mode in ("async", "async-again"):
+        assert np.array_equal(out[mode][0], out["sync"][0])
+        assert out[mode][1] == out["sync"][1]
+    assert np.abs(out["sync"][0]).max() > 0
