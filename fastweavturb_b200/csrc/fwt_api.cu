@@ -275,6 +275,8 @@ int fwt_destroy(fwt_ctx *h)
         cufftDestroy(c->plan_r2c);
         cufftDestroy(c->plan_c2r);
     }
+    for (auto &p : c->fbb_plans) cufftDestroy(p.h);
+    c->fbb_plans.clear();
     buf_free(c, c->b_nodes);
     buf_free(c, c->b_w);
     buf_free(c, c->b_u);

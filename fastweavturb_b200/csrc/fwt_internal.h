@@ -105,6 +105,13 @@ struct Ctx {
     int u_out = 0, d_out = 0;
     DevBuf b_aux_spec, b_aux_real, b_aux_acc, b_aux_out;   // their buffers, made on first use
     cufftHandle plan_r2c = 0, plan_c2r = 0;
+    // the generator's plans, kept between calls (plan creation costs milliseconds and a device
+    // synchronisation): key n2 for the single circulant row (batch 0) or (n2, batch)
+    struct FftPlan {
+        int n2, batch;
+        cufftHandle h;
+    };
+    std::vector<FftPlan> fbb_plans;
     bool plans = false;
     size_t fft_ws_bytes = 0;
 

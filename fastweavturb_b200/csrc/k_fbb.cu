@@ -177,6 +177,28 @@ __global__ void fbb_bridge_kernel(uint64_t seed, int t0, int Np, int M, double H
     }
 }
 
+// A Z2Z plan of length n2 over `batch` contiguous rows, made once per context and shape (at
+// most eight are kept; the oldest is dropped).
+static int fbb_plan(Ctx *c, int n2, int batch, cufftHandle *out)
+{
+    for (const auto &p : c->fbb_plans) {
+        if (p.n2 == n2 && p.batch == batch) {
+            *out = p.h;
+            return 0;
+        }
+    }
+    if (c->fbb_plans.size() >= 8) {
+        cufftDestroy(c->fbb_plans.front().h);
+        c->fbb_plans.erase(c->fbb_plans.begin());
+    }
+    cufftHandle h = 0;
+    int n[1] = {n2};
+    FWT_CUFFT(cufftPlanMany(&h, 1, n, nullptr, 1, n2, nullptr, 1, n2, CUFFT_Z2Z, batch));
+    c->fbb_plans.push_back({n2, batch, h});
+    *out = h;
+    return 0;
+}
+
 int fbb_generate(Ctx *c, uint64_t seed, int nlev, const int *tubes, const int *nodes, const double *H,
                  const double *dB, double *d_x, double *d_y, double *d_z)
 {
@@ -194,7 +216,7 @@ int fbb_generate(Ctx *c, uint64_t seed, int nlev, const int *tubes, const int *n
         double *sq = (double *)(row + n2);
         fbb_row_kernel<<<(n2 + 255) / 256, 256, 0, c->stream>>>(M, H[lv], row);
         cufftHandle p1;
-        FWT_CUFFT(cufftPlan1d(&p1, n2, CUFFT_Z2Z, 1));
+        FWT_TRY(fbb_plan(c, n2, 1, &p1));
         FWT_CUFFT(cufftSetStream(p1, c->stream));
         FWT_CUFFT(cufftExecZ2Z(p1, row, row, CUFFT_FORWARD));
         fbb_sqrt_kernel<<<(n2 + 255) / 256, 256, 0, c->stream>>>(n2, row, sq);
@@ -202,7 +224,6 @@ int fbb_generate(Ctx *c, uint64_t seed, int nlev, const int *tubes, const int *n
         // batches of tubes: 3 complex rows of n2 per tube, ~1 GB per batch
         const int per = std::max(1, (int)std::min<int64_t>(T, ((int64_t)1 << 30) / ((int64_t)3 * n2 * 16)));
         cufftHandle pb = 0;
-        int pb_batch = -1;
         for (int tb = 0; tb < T; tb += per) {
             const int nt = std::min(per, T - tb), nb = 3 * nt;
             FWT_TRY(buf_reserve(c, c->scratch[3], sizeof(cufftDoubleComplex) * (size_t)nb * n2));
@@ -211,13 +232,8 @@ int fbb_generate(Ctx *c, uint64_t seed, int nlev, const int *tubes, const int *n
             double *fbm = (double *)c->scratch[4].p;
             const int64_t tot = (int64_t)nb * n2;
             fbb_fill_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(seed, t0 + tb, nb, n2, sq, Zb);
-            if (pb_batch != nb) {
-                if (pb) cufftDestroy(pb);
-                int n[1] = {n2};
-                FWT_CUFFT(cufftPlanMany(&pb, 1, n, nullptr, 1, n2, nullptr, 1, n2, CUFFT_Z2Z, nb));
-                FWT_CUFFT(cufftSetStream(pb, c->stream));
-                pb_batch = nb;
-            }
+            FWT_TRY(fbb_plan(c, n2, nb, &pb));
+            FWT_CUFFT(cufftSetStream(pb, c->stream));
             FWT_CUFFT(cufftExecZ2Z(pb, Zb, Zb, CUFFT_FORWARD));
             fbb_scan_kernel<<<nb, 256, 0, c->stream>>>(Zb, n2, M, fbm);
             fbb_bridge_kernel<<<nt, 256, 0, c->stream>>>(seed, t0 + tb, Np, M, H[lv], dB[lv], fbm, d_x, d_y, d_z,
@@ -225,12 +241,11 @@ int fbb_generate(Ctx *c, uint64_t seed, int nlev, const int *tubes, const int *n
             c->launches += 4;
             FWT_CUDA(cudaGetLastError());
         }
-        FWT_CUDA(cudaStreamSynchronize(c->stream));
-        if (pb) cufftDestroy(pb);
-        cufftDestroy(p1);
         node0 += (int64_t)T * Np;
         t0 += T;
     }
+    // the arrays are complete when the call returns
+    FWT_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
 }
 
