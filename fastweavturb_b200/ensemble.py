@@ -96,10 +96,7 @@ class Ensemble:
             return best
 
         def pick(kind, candidates, default):
-            # the default stays unless a candidate is at least 5 % faster: one probe realisation
-            # and millisecond timings do not separate closer settings
-            best = min(candidates, key=lambda v: times[(kind, v)])
-            return best if times[(kind, best)] < 0.95 * times[(kind, default)] else default
+            return self.pick(times, kind, candidates, default)
 
         times = {}
         ctx.set_raster_radius_limit(-1.0)
@@ -127,6 +124,14 @@ class Ensemble:
         self.tune_log[w.N] = times
         del keep
         return self.tuned[w.N]
+
+    @staticmethod
+    def pick(times, kind, candidates, default, margin=0.05):
+        """The setting of `kind` to keep from times[(kind, value)] (seconds): the fastest
+        candidate if it beats the default by at least `margin`, else the default (one probe
+        realisation and millisecond timings do not separate closer settings)."""
+        best = min(candidates, key=lambda v: times[(kind, v)])
+        return best if times[(kind, best)] < (1.0 - margin) * times[(kind, default)] else default
 
     def slots_for(self, N):
         """Contexts kept for grid size N: every worker for small fields, fewer for large ones,

@@ -46,6 +46,17 @@ module fwt_iface
          real(c_double) :: xyz(*), sigma(*), gamma(*)
          integer(c_int) :: n_t(*), if_filter(*)
       end function
+      ! the copy runs behind the deposition: xyz must stay allocated and unchanged until the
+      ! next fwt_deposit / fwt_run returns
+      integer(c_int) function fwt_set_centerlines_async(ctx, nline, npoint, xyz, sigma, gamma, n_t, if_filter) &
+         bind(C, name="fwt_set_centerlines_async")
+         import :: c_int, c_ptr, c_int64_t, c_double
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: nline
+         integer(c_int64_t) :: npoint(*)
+         real(c_double) :: xyz(*), sigma(*), gamma(*)
+         integer(c_int) :: n_t(*), if_filter(*)
+      end function
       integer(c_int) function fwt_deposit(ctx, line_s, line_e) bind(C, name="fwt_deposit")
          import :: c_int, c_ptr
          type(c_ptr), value :: ctx

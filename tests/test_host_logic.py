@@ -117,3 +117,13 @@ def test_write_ply_layout(tmp_path):
     assert np.array_equal(v, tris.reshape(6, 4))
     f = np.frombuffer(body[6 * 16:], dtype=[("n", "u1"), ("v", "<i4", (3,))])
     assert list(f["n"]) == [3, 3] and f["v"].tolist() == [[0, 1, 2], [3, 4, 5]]
+
+
+def test_autotuner_keeps_the_default_unless_clearly_faster():
+    t = {("raster", 0.0): 1.00, ("raster", 1.5): 0.97, ("raster", 2.5): 1.20, ("raster", 4.0): 0.99}
+    assert Ensemble.pick(t, "raster", (0.0, 1.5, 2.5, 4.0), 0.0) == 0.0      # 3 % is within the noise
+    t[("raster", 2.5)] = 0.90
+    assert Ensemble.pick(t, "raster", (0.0, 1.5, 2.5, 4.0), 0.0) == 2.5      # 10 % faster
+    t = {("piece", 8.0): 2.0, ("piece", 5.0): 1.0}
+    assert Ensemble.pick(t, "piece", (5.0, 8.0), 8.0) == 5.0
+    assert Ensemble.pick(t, "piece", (5.0, 8.0), 5.0) == 5.0                 # the default is the fastest
