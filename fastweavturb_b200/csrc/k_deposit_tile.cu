@@ -193,7 +193,7 @@ __device__ __forceinline__ void clip_box(const SegRec &R, uint32_t img, int N, i
     B.pe = plane_eps(R.off, ext, dx, R.dci);
 }
 
-// Warp-autonomous tile deposition.  Each warp claims chunks of kWarpChunk candidates of the
+// Warp-autonomous tile deposition.  Each warp claims chunks of up to kWarpChunk candidates of the
 // tile, stages their records in its own slice of shared memory with one bulk asynchronous
 // copy per record (cp.async.bulk, completion on the warp's mbarrier), flattens the chunk's
 // grid rows across its lanes, and adds into the CTA's fixed-point accumulators.  Only the
@@ -323,8 +323,8 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
     if (lane == 0) mbar_init(&S.bar);
     // chunks are handed out through a shared counter: a warp that finishes early takes the
     // next one, so the warps of a tile end close together at the epilogue's barrier
-    __shared__ int next_chunk;
-    if (threadIdx.x == 0) next_chunk = kDepWarps;
+    __shared__ int next_rec;
+    if (threadIdx.x == 0) next_rec = kDepWarps * kWarpChunk;
     if constexpr (F64)
         tile_acc_init_f64<Accumulate>(reinterpret_cast<double(*)[kAccN]>(acc), N, x0, y0, z0, zs, zlim, (const double *)wx,
                                       (const double *)wy, (const double *)wz);
@@ -333,16 +333,17 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
                                   (const float *)wz);
     __syncthreads();
 
-    const int nchunks = (int)((c1 - c0 + kWarpChunk - 1) / kWarpChunk);
+    const int nrec = (int)(c1 - c0);
     const float fscale = (float)scale;
     const float fmaxq = 4.0e18f;
     uint32_t phase = 0;
     bool failed = false;
     int qn = 0;   // queued points of this warp (warp-uniform)
     unsigned nacc = 0;   // pairs evaluated by this warp (warp-uniform)
-    for (int ch = warp; ch < nchunks && !failed;) {
-        const int64_t base = c0 + (int64_t)ch * kWarpChunk;
-        const int nc = (c1 - base < kWarpChunk) ? (int)(c1 - base) : kWarpChunk;
+    int csz = kWarpChunk;   // candidates in this warp's current chunk
+    for (int start = warp * kWarpChunk; start < nrec && !failed;) {
+        const int64_t base = c0 + start;
+        const int nc = min(csz, nrec - start);
         const uint32_t v = lane < nc ? __ldg(list + base + lane) : 0u;
         if (lane < nc) S.id[lane] = v;
         // stage the records: expect nc * sizeof(SegRec) bytes, then one bulk copy per record
@@ -438,9 +439,17 @@ __global__ void __launch_bounds__(kDepThreads, F64 ? 2 : 3) deposit_tile_kernel(
         }
         if (qn > 0) drain_queue<General, F64>(S, acc, lane, qn, qn, nacc, fscale, fmaxq, err, redo, D, x0, y0, z0);
         __syncwarp();   // the warp's stage is reused by its next chunk
-        int nxt = 0;
-        if (lane == 0) nxt = atomicAdd(&next_chunk, 1);
-        ch = __shfl_sync(0xffffffffu, nxt, 0);
+        // the next chunk, guided self-scheduling: kWarpChunk candidates while many remain,
+        // down to two near the end of the list, so that the warps reach the epilogue's
+        // barrier close together (a thick tube's candidates cost a whole tile each)
+        int nxt = 0, cs = 0;
+        if (lane == 0) {
+            const int rem = nrec - *(volatile int *)&next_rec;
+            cs = max(2, min(kWarpChunk, rem / (2 * kDepWarps)));
+            nxt = atomicAdd(&next_rec, cs);
+        }
+        start = __shfl_sync(0xffffffffu, nxt, 0);
+        csz = __shfl_sync(0xffffffffu, cs, 0);
     }
     if (failed && lane == 0) atomicOr(err, 2);
     if (lane == 0 && redo.tally && !D.emit_only) atomicAdd(redo.tally, (unsigned long long)nacc);
